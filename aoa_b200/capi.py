@@ -1,0 +1,95 @@
+"""ctypes binding of libaoa_b200.so (include/aoa_ckks.h).
+
+The library is the product: if it is missing or fails to load this module
+raises, there is no fallback path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libaoa_b200.so")
+
+c_int, c_long, c_size_t, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_size_t, ctypes.c_double
+c_u64, c_i64, c_void_p, c_char_p = ctypes.c_uint64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_char_p
+u64p = ctypes.POINTER(ctypes.c_uint64)
+i64p = ctypes.POINTER(ctypes.c_int64)
+f64p = ctypes.POINTER(ctypes.c_double)
+intp = ctypes.POINTER(ctypes.c_int)
+vpp = ctypes.POINTER(ctypes.c_void_p)
+
+AOA_OK = 0
+STATUS = {
+    1: "AOA_ERR_BAD_PARAM", 2: "AOA_ERR_LEVEL_EXHAUSTED", 3: "AOA_ERR_NO_KEY", 4: "AOA_ERR_OOM",
+    5: "AOA_ERR_CUDA", 6: "AOA_ERR_TIMEOUT", 7: "AOA_ERR_SLOT_MISMATCH", 8: "AOA_ERR_NOT_INITIALIZED",
+    9: "AOA_ERR_NO_DEVICE",
+}
+AOA_COEF, AOA_NTT = 1, 2
+
+
+class AoaError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("log_n", c_int), ("k", c_int), ("kl", c_int), ("primes", u64p),
+                ("generators", u64p), ("scale_bits", c_int), ("dnum", c_int)]
+
+
+# name -> (restype, argtypes); every function returns an aoa_status unless noted
+SIGNATURES = {
+    "aoa_last_error": (c_char_p, []),
+    "aoa_status_string": (c_char_p, [c_int]),
+    "aoa_engine_create": (c_int, [ctypes.POINTER(Params), vpp]),
+    "aoa_engine_destroy": (c_int, [c_void_p]),
+    "aoa_engine_info": (c_int, [c_void_p, intp, intp, intp, u64p]),
+    "aoa_ctx_create": (c_int, [c_void_p, c_void_p, vpp]),
+    "aoa_ctx_destroy": (c_int, [c_void_p]),
+    "aoa_ctx_sync": (c_int, [c_void_p]),
+    "aoa_ctx_stream": (c_int, [c_void_p, vpp]),
+    "aoa_device_alloc": (c_int, [c_void_p, c_size_t, vpp]),
+    "aoa_device_free": (c_int, [c_void_p, c_void_p]),
+    "aoa_memcpy_h2d": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
+    "aoa_memcpy_d2h": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
+    "aoa_memcpy_d2d": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
+    "aoa_ntt_fwd": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int]),
+    "aoa_ntt_inv": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library; raises if it is absent (build it with aoa_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libaoa_b200.so is not built (%s); run python -m aoa_b200.build" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols():
+    return list(SIGNATURES)
+
+
+def check(status):
+    if status != AOA_OK:
+        msg = load().aoa_last_error().decode()
+        raise AoaError(status, msg)
+
+
+def ptr(a):
+    """Host pointer of a C-contiguous numpy array."""
+    assert a.flags["C_CONTIGUOUS"]
+    return ctypes.c_void_p(a.ctypes.data)

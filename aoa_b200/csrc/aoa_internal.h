@@ -1,0 +1,95 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/aoa_ckks.h"
+#include "modarith.cuh"
+
+namespace aoa {
+
+struct AoaError : public std::runtime_error {
+  int status;
+  AoaError(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define AOA_CUDA(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      throw ::aoa::AoaError(AOA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define AOA_CHECK_LAUNCH()                                                                 \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess)                                                                 \
+      throw ::aoa::AoaError(AOA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct Tune {
+  long ntt_chunk_bytes = 48L << 20;   // per NTT launch pair: stays inside L2
+};
+
+// Device copy of the basis-conversion / rescale constants.
+struct RnsTables {
+  // ModUp at level l (fast_conv_Q_to_B, manager.cu:180-223):
+  //   modup_inv[l*k + i]          = (Q_l/q_i)^-1 mod q_i        (Shoup form)
+  //   modup_hat[(l*k + i)*kl + j] = (Q_l/q_i) mod b_j
+  ShoupW* modup_inv = nullptr;
+  uint64_t* modup_hat = nullptr;
+  // ModDown (fast_conv_B_to_Q, manager.cu:312-341):
+  //   moddown_inv[j]         = ((B/b_j) mod b_j)^-1            (Shoup form)
+  //   moddown_hat[j*k + i]   = (B/b_j) mod q_i
+  //   moddown_binv[i]        = (B mod q_i)^-1                 (Shoup form)
+  ShoupW* moddown_inv = nullptr;
+  uint64_t* moddown_hat = nullptr;
+  ShoupW* moddown_binv = nullptr;
+  // Rescale (ckks_rescale, manager.cu:90-118): resc_inv[l*k + i] = q_l^-1 mod q_i
+  ShoupW* resc_inv = nullptr;
+  // B mod q_i for rho (manager.cu:149-160), Shoup form; zero on B primes
+  ShoupW* bmodq = nullptr;
+};
+
+struct Engine {
+  int device = 0;
+  int log_n = 0, log_c = 0;
+  long N = 0;
+  int k = 0, kl = 0, nprimes = 0;
+  int scale_bits = 0;
+  bool lazy = false;          // every prime < 2^62: Harvey lazy butterflies
+  std::vector<uint64_t> primes, gens;
+  std::vector<PrimeConst> h_pc;
+  PrimeConst* d_pc = nullptr;
+  ShoupW* d_tw = nullptr;     // [nprimes][N]
+  ShoupW* d_itw = nullptr;    // [nprimes][N]
+  RnsTables rns;
+  Tune tune;
+  std::vector<void*> allocations;
+};
+
+struct Ctx {
+  Engine* E = nullptr;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+};
+
+// ntt.cu
+void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
+               long poly_stride, bool forward, cudaStream_t st);
+
+// host number theory (primes.cpp)
+uint64_t h_mulmod(uint64_t a, uint64_t b, uint64_t q);
+uint64_t h_powmod(uint64_t a, uint64_t e, uint64_t q);
+uint64_t h_invmod(uint64_t a, uint64_t q);
+bool h_is_prime(uint64_t n);
+uint64_t h_smallest_primitive_root(uint64_t q);
+uint64_t h_shoup_companion(uint64_t w, uint64_t q);
+int h_search_primes(int bits, uint64_t modulus, int count, uint64_t* out);
+
+}  // namespace aoa
