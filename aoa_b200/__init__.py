@@ -137,3 +137,128 @@ class DeviceArray:
             self.free()
         except Exception:
             pass
+
+
+class Ciphertext:
+    """cipher_t on the device: two polys of k limbs, level, slots, scale, domain."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        capi.check(capi.load().aoa_ct_create(ctx.handle, ctypes.byref(h)))
+        self.handle = h
+
+    @classmethod
+    def from_residues(cls, ctx, c0, c1, level=None, slots=0, scale=None, domain=AOA_COEF):
+        ct = cls(ctx)
+        ct.upload(c0, c1, domain)
+        E = ctx.engine
+        nl = np.asarray(c0).shape[0]
+        ct.set(level if level is not None else nl - 1, slots,
+               scale if scale is not None else (1 << E.scale_bits if E.scale_bits else 1), domain)
+        return ct
+
+    def upload(self, c0, c1, domain=AOA_COEF):
+        host = np.ascontiguousarray(np.stack([np.asarray(c0, dtype=np.uint64), np.asarray(c1, dtype=np.uint64)]))
+        capi.check(capi.load().aoa_ct_upload(self.ctx.handle, self.handle, capi.ptr(host), host.shape[1], domain))
+        self.ctx.sync()
+
+    def download(self, nlimbs=None, domain=AOA_COEF):
+        nlimbs = nlimbs or (self.level + 1)
+        out = np.empty((2, nlimbs, self.ctx.engine.N), dtype=np.uint64)
+        capi.check(capi.load().aoa_ct_download(self.ctx.handle, self.handle, capi.ptr(out), nlimbs, domain))
+        return out[0], out[1]
+
+    def set(self, level, slots, scale, domain):
+        capi.check(capi.load().aoa_ct_set(self.handle, level, slots, int(scale), domain))
+
+    def _get(self):
+        lv, sl, dm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        sc = ctypes.c_uint64()
+        capi.check(capi.load().aoa_ct_get(self.handle, ctypes.byref(lv), ctypes.byref(sl), ctypes.byref(sc),
+                                          ctypes.byref(dm)))
+        return lv.value, sl.value, sc.value, dm.value
+
+    level = property(lambda self: self._get()[0])
+    slots = property(lambda self: self._get()[1])
+    scale = property(lambda self: self._get()[2])
+    domain = property(lambda self: self._get()[3])
+
+    @property
+    def device_ptr(self):
+        p = ctypes.c_void_p()
+        capi.check(capi.load().aoa_ct_data(self.handle, ctypes.byref(p)))
+        return p
+
+    def close(self):
+        if getattr(self, "handle", None) and self.ctx.handle:
+            capi.load().aoa_ct_destroy(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SwitchKey:
+    """SwitchKey {b, a} over the QB basis (relinearisation, rotation or conjugation key)."""
+
+    def __init__(self, ctx, b, a, domain=AOA_NTT):
+        self.ctx = ctx
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        h = ctypes.c_void_p()
+        capi.check(capi.load().aoa_swk_create(ctx.handle, capi.ptr(b), capi.ptr(a), domain, ctypes.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None) and self.ctx.handle:
+            capi.load().aoa_swk_destroy(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _h(x):
+    return None if x is None else x.handle
+
+
+# ---- reference-named evaluation API (aoa-ntt include/newckks/ckks/ckks.h) -------
+
+def ckks_mul(ctx, c3, c1, c2, evk):
+    """HMult + relinearise + rescale into c3 (ckks_mul, ckks.cpp:334-347)."""
+    capi.check(capi.load().aoa_hmult_relin_rescale(ctx.handle, c3.handle, c1.handle, c2.handle, _h(evk)))
+
+
+def ckks_mul_without_rescale(ctx, c3, c1, c2, evk):
+    capi.check(capi.load().aoa_hmult(ctx.handle, c3.handle, c1.handle, c2.handle, _h(evk)))
+
+
+def ckks_rescale(ctx, c):
+    capi.check(capi.load().aoa_rescale(ctx.handle, c.handle))
+
+
+def ckks_add(ctx, c3, c1, c2):
+    capi.check(capi.load().aoa_add(ctx.handle, c3.handle, c1.handle, c2.handle))
+
+
+def ckks_sub(ctx, c3, c1, c2):
+    capi.check(capi.load().aoa_sub(ctx.handle, c3.handle, c1.handle, c2.handle))
+
+
+def ckks_rotate_left(ctx, c2, c1, steps, rtk):
+    capi.check(capi.load().aoa_rotate(ctx.handle, c2.handle, c1.handle, steps, _h(rtk)))
+
+
+def ckks_rotate_right(ctx, c2, c1, steps, rtk):
+    capi.check(capi.load().aoa_rotate(ctx.handle, c2.handle, c1.handle, -steps, _h(rtk)))
+
+
+def ckks_conjugate(ctx, c2, c1, cjk):
+    capi.check(capi.load().aoa_conjugate(ctx.handle, c2.handle, c1.handle, _h(cjk)))

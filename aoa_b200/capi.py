@@ -58,6 +58,25 @@ SIGNATURES = {
     "aoa_memcpy_d2d": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "aoa_ntt_fwd": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int]),
     "aoa_ntt_inv": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int]),
+    "aoa_modup": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "aoa_moddown": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "aoa_rescale_polys": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int]),
+    "aoa_ct_create": (c_int, [c_void_p, vpp]),
+    "aoa_ct_destroy": (c_int, [c_void_p, c_void_p]),
+    "aoa_ct_set": (c_int, [c_void_p, c_int, c_int, c_u64, c_int]),
+    "aoa_ct_get": (c_int, [c_void_p, intp, intp, u64p, intp]),
+    "aoa_ct_data": (c_int, [c_void_p, vpp]),
+    "aoa_ct_upload": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int]),
+    "aoa_ct_download": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int]),
+    "aoa_swk_create": (c_int, [c_void_p, c_void_p, c_void_p, c_int, vpp]),
+    "aoa_swk_destroy": (c_int, [c_void_p, c_void_p]),
+    "aoa_hmult": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_hmult_relin_rescale": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_rescale": (c_int, [c_void_p, c_void_p]),
+    "aoa_add": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_sub": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_rotate": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "aoa_conjugate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

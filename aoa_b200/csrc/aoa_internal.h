@@ -77,11 +77,54 @@ struct Ctx {
   Engine* E = nullptr;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  void* scratch = nullptr;      // key-switch workspace (stream-ordered allocation)
+  size_t scratch_bytes = 0;
 };
+
+// C-ABI error plumbing (engine.cu)
+int fail(int status, const std::string& msg);
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return AOA_OK;
+  } catch (const AoaError& e) {
+    return fail(e.status, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(AOA_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(AOA_ERR_BAD_PARAM, e.what());
+  }
+}
 
 // ntt.cu
 void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
                long poly_stride, bool forward, cudaStream_t st);
+
+// rns.cu
+void rns_init(Engine& E);
+void modup(const Engine& E, const uint64_t* in, long in_stride, uint64_t* out_b, long out_stride,
+           int npolys, int level, cudaStream_t st);
+void moddown(const Engine& E, const uint64_t* in_q, const uint64_t* in_b, long in_stride, uint64_t* out,
+             long out_stride, int npolys, int level, cudaStream_t st);
+void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int level, cudaStream_t st);
+
+// ops.cu  (op: 0 add, 1 sub, 2 mul, 3 neg)
+void ew_binary_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as, const uint64_t* b, long bs,
+                  int op, int prime0, int nlimbs, int npolys, cudaStream_t st);
+void ew_scalar_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as, const uint64_t* d_scalars,
+                  int op, int prime0, int nlimbs, int npolys, cudaStream_t st);
+void ew_muladd_op(const Engine& E, uint64_t* d, long ds, const uint64_t* a, long as, const uint64_t* b, long bs,
+                  const uint64_t* c, long cs, int prime0, int nlimbs, int npolys, cudaStream_t st);
+void tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
+               uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st);
+void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
+                      uint64_t* k1, int nq, cudaStream_t st);
+void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,
+                       int nlimbs, int npolys, cudaStream_t st);
+void automorph_ntt_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,
+                      int nlimbs, int npolys, cudaStream_t st);
 
 // host number theory (primes.cpp)
 uint64_t h_mulmod(uint64_t a, uint64_t b, uint64_t q);
@@ -93,3 +136,6 @@ uint64_t h_shoup_companion(uint64_t w, uint64_t q);
 int h_search_primes(int bits, uint64_t modulus, int count, uint64_t* out);
 
 }  // namespace aoa
+
+struct aoa_engine { aoa::Engine e; };
+struct aoa_ctx { aoa::Ctx c; };

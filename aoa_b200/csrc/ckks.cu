@@ -1,0 +1,391 @@
+// CKKS ciphertext objects and the key-switching operations (HMult +
+// relinearisation + rescale, rotation, conjugation, add/sub, rescale) behind
+// the C ABI.  Semantics follow the reference evaluator (aoa-ntt
+// src/ckks/ckks.cpp); residues of every output limb <= level are identical to
+// the reference's.  The pipeline differs: it is level aware (only limbs
+// 0..level and the kl special limbs are touched), keeps the transform-domain
+// d2 for the Q part of the extended key-switch input instead of transforming
+// it back and forth, and multiplies with the key in one kernel.
+#include <cstring>
+
+#include "aoa_internal.h"
+
+using namespace aoa;
+
+// Ciphertext (cipher_t, aoa-ntt include/newckks/ckks/cipher_t.h:17-22):
+// d = [c0 | c1], each k limbs of N words.
+struct aoa_ct {
+  uint64_t* d = nullptr;
+  int level = 0;
+  int slots = 0;
+  uint64_t scale = 0;
+  int domain = AOA_COEF;
+};
+
+// Switching key (SwitchKey, aoa-ntt include/newckks/defines.h:85-90):
+// d = [b | a], each k + kl limbs, transform domain.
+struct aoa_swk {
+  uint64_t* d = nullptr;
+};
+
+namespace aoa {
+
+// Workspace for one key switch / HMult at the engine's largest level:
+//   D   [3][k]       tensor outputs d0 d1 d2 (transform domain)
+//   T   [k]          coefficient-domain copy of the key-switch input
+//   UB  [kl]         ModUp output (B limbs)
+//   KS  [2][k + kl]  key products, then their inverse transforms
+//   R0  [k]          rotated c0
+struct Workspace {
+  uint64_t *D, *T, *UB, *KS, *R0;
+};
+
+size_t workspace_words(const Engine& E) {
+  return (size_t)E.N * (3 * E.k + E.k + std::max(E.kl, 1) + 2 * (E.k + E.kl) + E.k);
+}
+
+static Workspace carve(const Engine& E, uint64_t* p) {
+  const size_t limb = (size_t)E.N;
+  Workspace w;
+  w.D = p; p += 3 * E.k * limb;
+  w.T = p; p += E.k * limb;
+  w.UB = p; p += std::max(E.kl, 1) * limb;
+  w.KS = p; p += 2 * (E.k + E.kl) * limb;
+  w.R0 = p;
+  return w;
+}
+
+static Workspace get_ws(Ctx& C) {
+  const size_t need = workspace_words(*C.E) * sizeof(uint64_t);
+  if (C.scratch_bytes < need) {
+    if (C.scratch) AOA_CUDA(cudaFreeAsync(C.scratch, C.stream));
+    C.scratch = nullptr;
+    C.scratch_bytes = 0;
+    cudaError_t e = cudaMallocAsync(&C.scratch, need, C.stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw AoaError(AOA_ERR_OOM, "workspace allocation failed");
+    }
+    C.scratch_bytes = need;
+  }
+  return carve(*C.E, (uint64_t*)C.scratch);
+}
+
+static void to_domain(Ctx& C, aoa_ct* ct, int domain, int nlimbs) {
+  const Engine& E = *C.E;
+  if (ct->domain == domain) return;
+  ntt_batch(E, ct->d, 2, 0, nlimbs, E.k, domain == AOA_NTT, C.stream);
+  ct->domain = domain;
+}
+
+// Key switch of the coefficient-domain Q limbs 0..level at `x_coef`, whose
+// transform-domain image is `x_ntt` (may be null: computed here).  Writes the
+// two coefficient-domain results to out0 / out1 (limbs 0..level).
+static void keyswitch(Ctx& C, const Workspace& w, const uint64_t* x_coef, const uint64_t* x_ntt, const aoa_swk* key,
+                      int level, uint64_t* out0, uint64_t* out1, long out_stride) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  const int m = level + 1;
+  const long ks_stride = (long)(E.k + E.kl) * N;
+  // ModUp of the coefficient-domain input, then its B limbs to the transform domain
+  modup(E, x_coef, 0, w.UB, 0, 1, level, C.stream);
+  ntt_batch(E, w.UB, 1, E.k, E.kl, E.kl, true, C.stream);
+  if (!x_ntt) {
+    AOA_CUDA(cudaMemcpyAsync(w.KS, x_coef, (size_t)m * N * 8, cudaMemcpyDeviceToDevice, C.stream));
+    ntt_batch(E, w.KS, 1, 0, m, m, true, C.stream);
+    x_ntt = w.KS;
+  }
+  // products with the key over Q limbs 0..level and all B limbs:
+  // KS[0] = x * b, KS[1] = x * a, layout [2][m Q limbs | kl B limbs] (stride k + kl)
+  // (x_ntt may alias KS[0]'s Q limbs: keyswitch_mul reads x before writing k0)
+  keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + ks_stride, m, C.stream);
+  // back to coefficients: Q limbs under primes 0..level, B limbs under k..k+kl-1
+  ntt_batch(E, w.KS, 2, 0, m, E.k + E.kl, false, C.stream);
+  ntt_batch(E, w.KS + (long)m * N, 2, E.k, E.kl, E.k + E.kl, false, C.stream);
+  // ModDown both products
+  if (out1 == out0 + out_stride) {
+    moddown(E, w.KS, w.KS + (long)m * N, ks_stride, out0, out_stride, 2, level, C.stream);
+  } else {
+    moddown(E, w.KS, w.KS + (long)m * N, ks_stride, out0, 0, 1, level, C.stream);
+    moddown(E, w.KS + ks_stride, w.KS + ks_stride + (long)m * N, 0, out1, 0, 1, level, C.stream);
+  }
+}
+
+static uint64_t scale_after_mult(const Engine& E, uint64_t sa, uint64_t sb, int level) {
+  unsigned __int128 p = (unsigned __int128)sa * sb;            // ckks.cpp:328-330
+  return (uint64_t)(p / E.primes[level]);
+}
+
+// HMult + relinearisation (ckks_mul_without_rescale, ckks.cpp:273-332),
+// optionally followed by the rescale of ckks_mul (ckks.cpp:334-347).
+void hmult(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool do_rescale) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  if (a->level == 0 || b->level == 0)
+    throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
+  if (a->slots != b->slots) throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
+  if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
+  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
+  const int level = std::min(a->level, b->level);
+  const int m = level + 1;
+  const long half = (long)E.k * N;
+  Workspace w = get_ws(C);
+  // operands to the transform domain, in place (poly_mul does the same, poly_t.cpp:201-220)
+  to_domain(C, a, AOA_NTT, std::max(a->level, level) + 1);
+  if (b != a) to_domain(C, b, AOA_NTT, std::max(b->level, level) + 1);
+  uint64_t* D0 = w.D;
+  uint64_t* D1 = w.D + half;
+  uint64_t* D2 = w.D + 2 * half;
+  tensor_op(E, a->d, half, b->d, half, D0, D1, D2, m, C.stream);
+  // coefficient-domain d2 for ModUp
+  AOA_CUDA(cudaMemcpyAsync(w.T, D2, (size_t)m * N * 8, cudaMemcpyDeviceToDevice, C.stream));
+  ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  const uint64_t sa = a->scale, sb = b->scale;
+  const int slots = a->slots;
+  keyswitch(C, w, w.T, D2, evk, level, out->d, out->d + half, half);
+  // c = (d0, d1) in coefficients + key-switch output
+  ntt_batch(E, D0, 2, 0, m, E.k, false, C.stream);
+  ew_binary_op(E, out->d, half, out->d, half, D0, half, 0, 0, m, 2, C.stream);
+  out->level = level;
+  out->slots = slots;
+  out->scale = scale_after_mult(E, sa, sb, level);
+  out->domain = AOA_COEF;
+  if (do_rescale) {
+    rescale(E, out->d, half, 2, level, C.stream);
+    out->level = level - 1;
+  }
+}
+
+// Galois automorphism X -> X^g followed by the key switch with `key`
+// (ckks_rotate_left/right, ckks.cpp:953-1009; ckks_conjugate, ckks.cpp:1011-1040).
+void apply_galois(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* key) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  if (!key || !key->d) throw AoaError(AOA_ERR_NO_KEY, "missing switching key for this automorphism");
+  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
+  const int level = in->level, m = level + 1;
+  const long half = (long)E.k * N;
+  Workspace w = get_ws(C);
+  // the reference transforms the input to coefficients in place (encoder.cu:340)
+  to_domain(C, in, AOA_COEF, m);
+  automorph_coef_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
+  automorph_coef_op(E, w.T, in->d + half, 0, galois, m, 1, C.stream);
+  const int slots = in->slots;
+  const uint64_t scale = in->scale;
+  keyswitch(C, w, w.T, nullptr, key, level, out->d, out->d + half, half);
+  ew_binary_op(E, out->d, half, out->d, half, w.R0, 0, 0, 0, m, 1, C.stream);
+  out->level = level;
+  out->slots = slots;
+  out->scale = scale;
+  out->domain = AOA_COEF;
+}
+
+}  // namespace aoa
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int aoa_ct_create(aoa_ctx* c, aoa_ct** out) {
+  if (!c || !out) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    aoa_ct* ct = new aoa_ct();
+    cudaError_t e = cudaMallocAsync(&ct->d, (size_t)2 * E.k * E.N * 8, c->c.stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      delete ct;
+      throw AoaError(AOA_ERR_OOM, "ciphertext allocation failed");
+    }
+    AOA_CUDA(cudaMemsetAsync(ct->d, 0, (size_t)2 * E.k * E.N * 8, c->c.stream));
+    ct->level = E.k - 1;                                   // cipher_init (cipher_t.cpp:3-9)
+    ct->scale = E.scale_bits > 0 && E.scale_bits < 64 ? (1ull << E.scale_bits) : 1;
+    ct->slots = 0;
+    ct->domain = AOA_COEF;
+    *out = ct;
+  });
+}
+
+int aoa_ct_destroy(aoa_ctx* c, aoa_ct* ct) {
+  if (!ct) return AOA_OK;
+  if (!c) return fail(AOA_ERR_BAD_PARAM, "null context");
+  int st = guarded([&] { AOA_CUDA(cudaFreeAsync(ct->d, c->c.stream)); });
+  delete ct;
+  return st;
+}
+
+int aoa_ct_set(aoa_ct* ct, int level, int slots, uint64_t scale, int domain) {
+  if (!ct || (domain != AOA_COEF && domain != AOA_NTT)) return fail(AOA_ERR_BAD_PARAM, "bad argument");
+  ct->level = level; ct->slots = slots; ct->scale = scale; ct->domain = domain;
+  return AOA_OK;
+}
+
+int aoa_ct_get(const aoa_ct* ct, int* level, int* slots, uint64_t* scale, int* domain) {
+  if (!ct) return fail(AOA_ERR_BAD_PARAM, "null ciphertext");
+  if (level) *level = ct->level;
+  if (slots) *slots = ct->slots;
+  if (scale) *scale = ct->scale;
+  if (domain) *domain = ct->domain;
+  return AOA_OK;
+}
+
+int aoa_ct_data(aoa_ct* ct, uint64_t** d) {
+  if (!ct || !d) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  *d = ct->d;
+  return AOA_OK;
+}
+
+// host residues [2][nlimbs][N] (c0 then c1) in `domain`
+int aoa_ct_upload(aoa_ctx* c, aoa_ct* ct, const uint64_t* host, int nlimbs, int domain) {
+  if (!c || !ct || !host) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    if (nlimbs < 1 || nlimbs > E.k) throw AoaError(AOA_ERR_BAD_PARAM, "nlimbs out of range");
+    const size_t limb = (size_t)E.N * 8;
+    for (int p = 0; p < 2; p++)
+      AOA_CUDA(cudaMemcpyAsync(ct->d + (size_t)p * E.k * E.N, host + (size_t)p * nlimbs * E.N, nlimbs * limb,
+                               cudaMemcpyHostToDevice, c->c.stream));
+    ct->domain = domain;
+    ct->level = nlimbs - 1;
+  });
+}
+
+// download limbs 0..nlimbs-1 of both polys in `domain` (converts a copy)
+int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain) {
+  if (!c || !ct || !host) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    Ctx& C = c->c;
+    const Engine& E = *C.E;
+    if (nlimbs < 1 || nlimbs > E.k) throw AoaError(AOA_ERR_BAD_PARAM, "nlimbs out of range");
+    const size_t limb = (size_t)E.N * 8;
+    const uint64_t* src = ct->d;
+    uint64_t* tmp = nullptr;
+    if (domain != ct->domain) {
+      AOA_CUDA(cudaMallocAsync(&tmp, 2 * E.k * limb, C.stream));
+      AOA_CUDA(cudaMemcpyAsync(tmp, ct->d, 2 * E.k * limb, cudaMemcpyDeviceToDevice, C.stream));
+      ntt_batch(E, tmp, 2, 0, nlimbs, E.k, domain == AOA_NTT, C.stream);
+      src = tmp;
+    }
+    for (int p = 0; p < 2; p++)
+      AOA_CUDA(cudaMemcpyAsync(host + (size_t)p * nlimbs * E.N, src + (size_t)p * E.k * E.N, nlimbs * limb,
+                               cudaMemcpyDeviceToHost, C.stream));
+    if (tmp) AOA_CUDA(cudaFreeAsync(tmp, C.stream));
+    AOA_CUDA(cudaStreamSynchronize(C.stream));
+  });
+}
+
+// Switching key from host residues b, a ([k+kl][N] each) in `domain`.
+int aoa_swk_create(aoa_ctx* c, const uint64_t* host_b, const uint64_t* host_a, int domain, aoa_swk** out) {
+  if (!c || !host_b || !host_a || !out) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    Ctx& C = c->c;
+    const Engine& E = *C.E;
+    const size_t half = (size_t)E.nprimes * E.N;
+    aoa_swk* k = new aoa_swk();
+    if (cudaMallocAsync(&k->d, 2 * half * 8, C.stream) != cudaSuccess) {
+      cudaGetLastError();
+      delete k;
+      throw AoaError(AOA_ERR_OOM, "key allocation failed");
+    }
+    AOA_CUDA(cudaMemcpyAsync(k->d, host_b, half * 8, cudaMemcpyHostToDevice, C.stream));
+    AOA_CUDA(cudaMemcpyAsync(k->d + half, host_a, half * 8, cudaMemcpyHostToDevice, C.stream));
+    if (domain == AOA_COEF) ntt_batch(E, k->d, 2, 0, E.nprimes, E.nprimes, true, C.stream);
+    AOA_CUDA(cudaStreamSynchronize(C.stream));
+    *out = k;
+  });
+}
+
+int aoa_swk_destroy(aoa_ctx* c, aoa_swk* k) {
+  if (!k) return AOA_OK;
+  if (!c) return fail(AOA_ERR_BAD_PARAM, "null context");
+  int st = guarded([&] { AOA_CUDA(cudaFreeAsync(k->d, c->c.stream)); });
+  delete k;
+  return st;
+}
+
+int aoa_hmult(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
+  if (!c || !out || !a || !b) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { hmult(c->c, out, a, b, evk, false); });
+}
+
+int aoa_hmult_relin_rescale(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
+  if (!c || !out || !a || !b) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { hmult(c->c, out, a, b, evk, true); });
+}
+
+int aoa_rescale(aoa_ctx* c, aoa_ct* ct) {
+  if (!c || !ct) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    if (ct->level == 0)
+      throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
+    to_domain(c->c, ct, AOA_COEF, ct->level + 1);
+    rescale(*c->c.E, ct->d, (long)c->c.E->k * c->c.E->N, 2, ct->level, c->c.stream);
+    ct->level--;
+  });
+}
+
+// ckks_add / ckks_sub (ckks.cpp:240-271): level = min, scale and slots of a.
+static int add_sub(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, int op) {
+  if (!c || !out || !a || !b) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    Ctx& C = c->c;
+    const Engine& E = *C.E;
+    if (a->slots != b->slots) throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
+    const int level = std::min(a->level, b->level);
+    if (a->domain != b->domain) {       // mixed states: both to coefficients (poly_t.cpp:143-146)
+      to_domain(C, a, AOA_COEF, a->level + 1);
+      to_domain(C, b, AOA_COEF, b->level + 1);
+    }
+    const long half = (long)E.k * E.N;
+    ew_binary_op(E, out->d, half, a->d, half, b->d, half, op, 0, level + 1, 2, C.stream);
+    out->level = level;
+    out->slots = a->slots;
+    out->scale = a->scale;
+    out->domain = a->domain;
+  });
+}
+
+int aoa_add(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b) { return add_sub(c, out, a, b, 0); }
+int aoa_sub(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b) { return add_sub(c, out, a, b, 1); }
+
+// rotation by `steps` slots to the left with key rtk (ckks_rotate_left);
+// negative steps rotate right (rotate_slots_right = left by N/2 - r).
+int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk) {
+  if (!c || !out || !in) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    const long M = 2 * E.N;
+    long r = steps % (E.N / 2);
+    if (r < 0) r += E.N / 2;
+    const long g = (long)h_powmod(5, (uint64_t)r, (uint64_t)M);
+    apply_galois(c->c, out, in, g, rtk);
+  });
+}
+
+int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk) {
+  if (!c || !out || !in) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { apply_galois(c->c, out, in, 2 * c->c.E->N - 1, cjk); });
+}
+
+// Standalone basis conversions on device buffers (coefficient domain):
+// ModUp reads Q limbs 0..level of `in_q` ([k][N]) and writes kl limbs to `out_b`;
+// ModDown reads a QB poly ([k + kl][N], B limbs at offset k) and writes limbs
+// 0..level of `out_q`.
+int aoa_modup(aoa_ctx* c, const uint64_t* in_q, uint64_t* out_b, int level) {
+  if (!c || !in_q || !out_b) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { modup(*c->c.E, in_q, 0, out_b, 0, 1, level, c->c.stream); });
+}
+
+int aoa_moddown(aoa_ctx* c, const uint64_t* in_qb, uint64_t* out_q, int level) {
+  if (!c || !in_qb || !out_q) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    moddown(E, in_qb, in_qb + (long)E.k * E.N, 0, out_q, 0, 1, level, c->c.stream);
+  });
+}
+
+int aoa_rescale_polys(aoa_ctx* c, uint64_t* d, int npolys, int poly_stride, int level) {
+  if (!c || !d) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { rescale(*c->c.E, d, (long)poly_stride * c->c.E->N, npolys, level, c->c.stream); });
+}
+
+}  // extern "C"

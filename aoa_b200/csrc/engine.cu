@@ -17,20 +17,6 @@ int fail(int status, const std::string& msg) {
   return status;
 }
 
-template <class F>
-int guarded(F&& f) {
-  try {
-    f();
-    return AOA_OK;
-  } catch (const AoaError& e) {
-    return fail(e.status, e.what());
-  } catch (const std::bad_alloc&) {
-    return fail(AOA_ERR_OOM, "host allocation failed");
-  } catch (const std::exception& e) {
-    return fail(AOA_ERR_BAD_PARAM, e.what());
-  }
-}
-
 static long bitrev(uint32_t x, int bits) {
   uint32_t r = 0;
   for (int i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
@@ -156,9 +142,6 @@ static void build_rns_tables(Engine& E) {
 
 using namespace aoa;
 
-struct aoa_engine { Engine e; };
-struct aoa_ctx { Ctx c; };
-
 extern "C" {
 
 const char* aoa_last_error(void) { return g_last_error.c_str(); }
@@ -213,6 +196,7 @@ int aoa_engine_create(const aoa_params* p, aoa_engine** out) {
       E.gens[i] = p->generators ? p->generators[i] : h_smallest_primitive_root(E.primes[i]);
     build_prime_tables(E);
     build_rns_tables(E);
+    rns_init(E);
     AOA_CUDA(cudaDeviceSynchronize());
   });
   if (st != AOA_OK) {
@@ -263,6 +247,7 @@ int aoa_ctx_create(aoa_engine* e, void* stream, aoa_ctx** out) {
 int aoa_ctx_destroy(aoa_ctx* h) {
   if (!h) return AOA_OK;
   int st = guarded([&] {
+    if (h->c.scratch) AOA_CUDA(cudaFreeAsync(h->c.scratch, h->c.stream));
     AOA_CUDA(cudaStreamSynchronize(h->c.stream));
     if (h->c.own_stream) AOA_CUDA(cudaStreamDestroy(h->c.stream));
   });

@@ -1,0 +1,159 @@
+// RNS basis conversion (ModUp / ModDown) and rescale, sm_100a CUDA cores.
+//
+// Both conversions are small dense modular matrix products per coefficient:
+//   ModUp   (fast_conv_Q_to_B_opt, aoa-ntt src/cuda/manager.cu:180-223)
+//     B_j = sum_{i<=l} [x_i (Q_l/q_i)^-1]_{q_i} * [(Q_l/q_i)]_{b_j}   mod b_j
+//   ModDown (fast_conv_B_to_Q, manager.cu:312-341)
+//     out_i = (x_i - sum_j [x_j (B/b_j)^-1]_{b_j} * [(B/b_j)]_{q_i}) * B^-1 mod q_i
+// The reference reduces after every term (mulmod + addmod per term); here the
+// products accumulate exactly in 128 bits and each output is reduced once
+// (sum of <= 64 products of two < 2^63 values stays below 2^128).  The exact
+// residues are identical.  One thread owns one coefficient and keeps up to
+// 32 accumulators in registers; the constant matrix slice sits in shared
+// memory and is read as a warp broadcast.
+#include "aoa_internal.h"
+
+namespace aoa {
+
+constexpr int kConvOut = 32;     // outputs per pass (register accumulators)
+constexpr int kConvThreads = 128;
+
+// in:  nin limbs at `in` (stride N), under primes in_prime0 + i
+// out: nout limbs at `out` (stride N), under primes out_prime0 + j
+// zc[i]  : Shoup constant applied to input limb i before the product
+// mat    : [nin][mat_ld] matrix, entry (i, j) = multiplier of z_i for output j
+// post   : 0 = out_j = acc_j mod p_j (ModUp)
+//          1 = out_j = (x_j - acc_j mod p_j) * post_c[j]  with x_j = sub_src limb j (ModDown)
+struct ConvArgs {
+  const uint64_t* in;
+  uint64_t* out;
+  const uint64_t* sub_src;
+  long in_poly_stride, out_poly_stride, sub_poly_stride;   // in elements
+  int nin, nout, mat_ld;
+  int in_prime0, out_prime0;
+  const ShoupW* zc;
+  const uint64_t* mat;
+  const ShoupW* post_c;
+  const PrimeConst* pc;
+  int log_n;
+  int post;
+};
+
+__global__ void __launch_bounds__(kConvThreads)
+basis_convert(ConvArgs a, int out_first) {
+  extern __shared__ uint64_t smat[];    // [nin][kConvOut]
+  const int nout = min(kConvOut, a.nout - out_first);
+  for (int e = threadIdx.x; e < a.nin * kConvOut; e += blockDim.x) {
+    const int i = e / kConvOut, j = e % kConvOut;
+    smat[e] = j < nout ? a.mat[(long)i * a.mat_ld + out_first + j] : 0;
+  }
+  __syncthreads();
+  const long N = 1L << a.log_n;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t* in = a.in + blockIdx.y * a.in_poly_stride + c;
+  uint64_t lo[kConvOut], hi[kConvOut];
+#pragma unroll
+  for (int j = 0; j < kConvOut; j++) lo[j] = hi[j] = 0;
+  for (int i = 0; i < a.nin; i++) {
+    const uint64_t qi = a.pc[a.in_prime0 + i].q;
+    const ShoupW zc = a.zc[i];
+    const uint64_t z = shoup(in[(long)i * N], zc, qi);
+    const uint64_t* row = smat + i * kConvOut;
+#pragma unroll
+    for (int j = 0; j < kConvOut; j++) mac128(lo[j], hi[j], z, row[j]);
+  }
+  uint64_t* out = a.out + blockIdx.y * a.out_poly_stride + c;
+#pragma unroll
+  for (int j = 0; j < kConvOut; j++) {
+    if (j < nout) {
+      const int jj = out_first + j;
+      const PrimeConst& P = a.pc[a.out_prime0 + jj];
+      uint64_t r = reduce128(lo[j], hi[j], P);
+      if (a.post) {
+        const uint64_t x = a.sub_src[blockIdx.y * a.sub_poly_stride + (long)jj * N + c];
+        r = shoup(sub_mod(x, r, P.q), a.post_c[jj], P.q);
+      }
+      out[(long)jj * N] = r;
+    }
+  }
+}
+
+static void run_convert(const Engine& E, ConvArgs a, int npolys, cudaStream_t st) {
+  const long N = E.N;
+  if (N % kConvThreads) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: N too small");
+  const size_t smem = (size_t)a.nin * kConvOut * sizeof(uint64_t);
+  if (smem > 200 * 1024) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: too many input limbs");
+  dim3 grid(N / kConvThreads, npolys);
+  for (int j0 = 0; j0 < a.nout; j0 += kConvOut)
+    basis_convert<<<grid, kConvThreads, smem, st>>>(a, j0);
+  AOA_CHECK_LAUNCH();
+}
+
+// Once per engine (per device): opt in to the dynamic shared memory the
+// conversion kernel needs, and check the 128-bit accumulation bound.
+void rns_init(Engine& E) {
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  auto bits = [](uint64_t x) { int b = 0; while (x) { b++; x >>= 1; } return b; };
+  uint64_t mq = 0, mb = 0;
+  for (int i = 0; i < E.k; i++) mq = std::max(mq, E.primes[i]);
+  for (int j = 0; j < E.kl; j++) mb = std::max(mb, E.primes[E.k + j]);
+  const int terms = std::max(E.k, E.kl);
+  if (E.kl && bits(mq) + bits(mb) + bits((uint64_t)terms) > 128)
+    throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: prime sizes overflow the 128-bit accumulator");
+}
+
+// ModUp: Q limbs 0..level of `in` (coefficient domain) -> kl B limbs of `out_b`.
+void modup(const Engine& E, const uint64_t* in, long in_stride, uint64_t* out_b, long out_stride,
+           int npolys, int level, cudaStream_t st) {
+  if (E.kl == 0) return;
+  if (level < 0 || level >= E.k) throw AoaError(AOA_ERR_BAD_PARAM, "modup: bad level");
+  ConvArgs a{};
+  a.in = in; a.out = out_b; a.sub_src = nullptr;
+  a.in_poly_stride = in_stride; a.out_poly_stride = out_stride;
+  a.nin = level + 1; a.nout = E.kl; a.mat_ld = E.kl;
+  a.in_prime0 = 0; a.out_prime0 = E.k;
+  a.zc = E.rns.modup_inv + (long)level * E.k;
+  a.mat = E.rns.modup_hat + (long)level * E.k * E.kl;
+  a.post_c = nullptr; a.pc = E.d_pc; a.log_n = E.log_n; a.post = 0;
+  run_convert(E, a, npolys, st);
+}
+
+// ModDown: `in` holds Q limbs 0..level at in_q and kl B limbs at in_b
+// (coefficient domain) -> limbs 0..level of `out`.
+void moddown(const Engine& E, const uint64_t* in_q, const uint64_t* in_b, long in_stride, uint64_t* out,
+             long out_stride, int npolys, int level, cudaStream_t st) {
+  if (level < 0 || level >= E.k) throw AoaError(AOA_ERR_BAD_PARAM, "moddown: bad level");
+  ConvArgs a{};
+  a.in = in_b; a.out = out; a.sub_src = in_q;
+  a.in_poly_stride = in_stride; a.out_poly_stride = out_stride; a.sub_poly_stride = in_stride;
+  a.nin = E.kl; a.nout = level + 1; a.mat_ld = E.k;
+  a.in_prime0 = E.k; a.out_prime0 = 0;
+  a.zc = E.rns.moddown_inv;
+  a.mat = E.rns.moddown_hat;
+  a.post_c = E.rns.moddown_binv; a.pc = E.d_pc; a.log_n = E.log_n; a.post = 1;
+  run_convert(E, a, npolys, st);
+}
+
+// Rescale by q_level (ckks_rescale, manager.cu:90-118): for i < level,
+// c_i <- (c_i - [c_level]_{q_i}) * q_level^-1 mod q_i, floor semantics, on
+// npolys polys (stride poly_stride) in place, coefficient domain.
+__global__ void rescale_kernel(uint64_t* d, long poly_stride, int level, const ShoupW* inv,
+                               const PrimeConst* pc, int log_n) {
+  const long N = 1L << log_n;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  uint64_t* p = d + blockIdx.z * poly_stride;
+  const PrimeConst& P = pc[i];
+  const uint64_t top = shoup(p[(long)level * N + c], 1, P.one_sh, P.q);   // [c_level]_{q_i}
+  p[(long)i * N + c] = shoup(sub_mod(p[(long)i * N + c], top, P.q), inv[i], P.q);
+}
+
+void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int level, cudaStream_t st) {
+  if (level < 1 || level >= E.k) throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "rescale: level must be >= 1");
+  dim3 grid(E.N / 256, level, npolys);
+  rescale_kernel<<<grid, 256, 0, st>>>(d, poly_stride, level, E.rns.resc_inv + (long)level * E.k, E.d_pc,
+                                       E.log_n);
+  AOA_CHECK_LAUNCH();
+}
+
+}  // namespace aoa

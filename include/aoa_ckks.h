@@ -95,6 +95,60 @@ int aoa_memcpy_d2d(aoa_ctx* c, void* dst, const void* src, size_t bytes);
 int aoa_ntt_fwd(aoa_ctx* c, uint64_t* d_data, int npolys, int first_prime, int nlimbs, int poly_stride);
 int aoa_ntt_inv(aoa_ctx* c, uint64_t* d_data, int npolys, int first_prime, int nlimbs, int poly_stride);
 
+/* --- RNS basis conversion and rescale on device buffers (coefficient domain).
+ *     aoa_modup replaces CUDAManager::execute_modup / fast_conv_Q_to_B_opt
+ *     (src/cuda/manager.cu:180-249): reads Q limbs 0..level of in_q ([k][N]),
+ *     writes the kl special limbs to out_b ([kl][N]).
+ *     aoa_moddown replaces execute_moddown / fast_conv_B_to_Q
+ *     (manager.cu:312-367): reads a QB poly ([k+kl][N]), writes limbs 0..level
+ *     of out_q ([k][N]).
+ *     aoa_rescale_polys replaces execute_rescale / ckks_rescale
+ *     (manager.cu:90-139) on npolys polys of poly_stride limbs, in place.     */
+int aoa_modup(aoa_ctx* c, const uint64_t* in_q, uint64_t* out_b, int level);
+int aoa_moddown(aoa_ctx* c, const uint64_t* in_qb, uint64_t* out_q, int level);
+int aoa_rescale_polys(aoa_ctx* c, uint64_t* d, int npolys, int poly_stride, int level);
+
+/* --- ciphertexts: replace cipher_t / cipher_init / cipher_free
+ *     (include/newckks/ckks/cipher_t.h:17-48, src/ckks/cipher_t.cpp:3-34).
+ *     A ciphertext holds two polys of k limbs on the device; create sets
+ *     level = k-1 and scale = 2^scale_bits like cipher_init.                  */
+typedef struct aoa_ct aoa_ct;
+int aoa_ct_create(aoa_ctx* c, aoa_ct** out);
+int aoa_ct_destroy(aoa_ctx* c, aoa_ct* ct);
+int aoa_ct_set(aoa_ct* ct, int level, int slots, uint64_t scale, int domain);
+int aoa_ct_get(const aoa_ct* ct, int* level, int* slots, uint64_t* scale, int* domain);
+int aoa_ct_data(aoa_ct* ct, uint64_t** device_ptr);          /* [2][k][N] */
+/* host residues [2][nlimbs][N] (c0 then c1); upload sets level = nlimbs-1.
+ * download converts a device copy to `domain` (poly_copy_to_host INTTs,
+ * poly_t.cpp:74-100) and synchronises the stream.                           */
+int aoa_ct_upload(aoa_ctx* c, aoa_ct* ct, const uint64_t* host, int nlimbs, int domain);
+int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain);
+
+/* --- switching keys: SwitchKey {a, b} over QB (include/newckks/defines.h:85-101,
+ *     src/ckks/ckkskeys.cpp:101-191).  host_b / host_a: [k+kl][N] residues.   */
+typedef struct aoa_swk aoa_swk;
+int aoa_swk_create(aoa_ctx* c, const uint64_t* host_b, const uint64_t* host_a, int domain, aoa_swk** out);
+int aoa_swk_destroy(aoa_ctx* c, aoa_swk* k);
+
+/* --- CKKS evaluation (src/ckks/ckks.cpp; include/newckks/ckks/ckks.h:23-319).
+ *     Outputs may alias inputs.  Like the reference, operands are brought to
+ *     the domain an operation needs in place.                                 */
+/* ckks_mul_without_rescale (ckks.cpp:273-332): out level = min level, scale =
+ * floor(sa*sb/q_level), coefficient domain.                                  */
+int aoa_hmult(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
+/* ckks_mul (ckks.cpp:334-347): HMult + relinearise + rescale.                */
+int aoa_hmult_relin_rescale(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
+/* ckks_rescale (ckks.cpp:220-230) */
+int aoa_rescale(aoa_ctx* c, aoa_ct* ct);
+/* ckks_add / ckks_sub (ckks.cpp:232-271) */
+int aoa_add(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b);
+int aoa_sub(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b);
+/* ckks_rotate_left (steps > 0) / ckks_rotate_right (steps < 0, i.e. left by
+ * N/2 - |steps|) with the matching key (ckks.cpp:953-1009).                  */
+int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk);
+/* ckks_conjugate (ckks.cpp:1011-1040) */
+int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -348,10 +348,12 @@ static void ntt_tables(Ctx& C, Prime& P) {
   uint64_t ipsi = oc_invmod(psi, q);
   uint64_t invN = oc_invmod((uint64_t)N % q, q);
   P.nthroot.resize(N); P.invnthroot.resize(N);
+  uint64_t pw = 1, ipw = 1;                 // psi^c and psi^-c by running products
   for (int c = 0; c < N; c++) {
-    P.nthroot[c] = oc_powmod(psi, c, q);
-    P.invnthroot[c] = C.hier ? oc_powmod(ipsi, c, q)
-                             : oc_mulmod_exact(oc_powmod(ipsi, c, q), invN, q);  // ntt.cu:714-720
+    P.nthroot[c] = pw;
+    P.invnthroot[c] = C.hier ? ipw : oc_mulmod_exact(ipw, invN, q);   // ntt.cu:714-720
+    pw = oc_mulmod_exact(pw, psi, q);
+    ipw = oc_mulmod_exact(ipw, ipsi, q);
   }
   if (C.hier) {
     compute_gjk(P, C.Na, P.gjk_a, P.invgjk_a);
@@ -362,9 +364,15 @@ static void ntt_tables(Ctx& C, Prime& P) {
     uint64_t gi = oc_invmod(g, q);
     uint64_t invNN = oc_invmod((uint64_t)(Na * Nb) % q, q);
     P.gN.resize(N); P.ginvN.resize(N);
-    for (int c = 0; c < N; c++) {
-      P.gN[c] = oc_powmod(g, (uint64_t)(c / Nb) * bitrev(c % Nb, lb), q);
-      P.ginvN[c] = oc_mulmod_exact(oc_powmod(gi, (uint64_t)bitrev(c / Na, lb) * (c % Na), q), invNN, q);
+    // gN[c] = g^((c / Nb) * bitrev(c % Nb)): running product down each column
+    for (int col = 0; col < Nb; col++) {
+      uint64_t step = oc_powmod(g, bitrev(col, lb), q), cur = 1;
+      for (int r = 0; r < Na; r++) { P.gN[(size_t)r * Nb + col] = cur; cur = oc_mulmod_exact(cur, step, q); }
+    }
+    // ginvN[c] = g^-(bitrev(c / Na) * (c % Na)) / N: running product along each row
+    for (int u = 0; u < Nb; u++) {
+      uint64_t step = oc_powmod(gi, bitrev(u, lb), q), cur = invNN;
+      for (int v = 0; v < Na; v++) { P.ginvN[(size_t)u * Na + v] = cur; cur = oc_mulmod_exact(cur, step, q); }
     }
   } else {
     compute_gjk(P, N, P.gjk_a, P.invgjk_a);

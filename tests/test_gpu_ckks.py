@@ -1,0 +1,212 @@
+"""GPU parity of the CKKS hot path against the CPU oracle, through the C ABI.
+
+Every residue of every live output limb must be bit-exact.  Inputs are seeded
+synthetic ciphertexts / keys (tests/ckks_inputs.py)."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import Oracle, reference_prime_set, ST_COEF, ST_NTT
+from tests.ckks_inputs import make_keys, encrypt_values, uniform_residues
+from tests.gpu_util import require_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(log_n, Q, B, scale_bits=0):
+    import aoa_b200
+    E = aoa_b200.Engine(log_n, Q, B, scale_bits=scale_bits)
+    ctx = aoa_b200.Context(E)
+    return aoa_b200, E, ctx, Oracle(1 << log_n, Q, B)
+
+
+def _sets(ref_table):
+    q55, b55 = reference_prime_set(ref_table, 4, 4, 55)
+    p60 = oracle.gen_ntt_primes(60, 1 << 17, 11)
+    return {"ref55": (q55, b55), "p60": (p60[:5], p60[5:])}
+
+
+@pytest.mark.parametrize("pset", ["ref55", "p60"])
+def test_modup_moddown_rescale(ref_table, pset):
+    require_gpu()
+    Q, B = _sets(ref_table)[pset]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    rng = np.random.default_rng(3)
+    N, k, kl = E.N, E.k, E.kl
+    xq = uniform_residues(rng, Q, N)
+    xb = uniform_residues(rng, B, N)
+    dq = ctx.upload(xq)
+    dqb = ctx.upload(np.concatenate([xq, xb]))
+    for level in range(k):
+        out_b = ctx.alloc((kl, N))
+        aoa.capi.check(aoa.capi.load().aoa_modup(ctx.handle, dq.ptr, out_b.ptr, level))
+        assert np.array_equal(out_b.numpy(), o.modup(xq, level)), "modup level %d" % level
+        out_q = ctx.alloc((k, N))
+        aoa.capi.check(aoa.capi.load().aoa_moddown(ctx.handle, dqb.ptr, out_q.ptr, level))
+        assert np.array_equal(out_q.numpy()[: level + 1], o.moddown(np.concatenate([xq, xb]), level)[: level + 1])
+    for level in range(1, k):
+        d = ctx.upload(np.stack([xq, xq[::-1].copy()]))
+        aoa.capi.check(aoa.capi.load().aoa_rescale_polys(ctx.handle, d.ptr, 2, k, level))
+        got = d.numpy()
+        w0, w1 = o.rescale(xq, xq[::-1].copy(), level)
+        assert np.array_equal(got[0, :level], w0[:level]) and np.array_equal(got[1, :level], w1[:level])
+
+
+def _rand_ct(rng, primes, N, nlimbs):
+    return uniform_residues(rng, primes[:nlimbs], N), uniform_residues(rng, primes[:nlimbs], N)
+
+
+@pytest.mark.parametrize("pset,log_n", [("ref55", 12), ("p60", 12), ("p60", 13)])
+@pytest.mark.parametrize("in_domain", ["coef", "ntt"])
+def test_hmult_relin_rescale_bit_exact(ref_table, pset, log_n, in_domain):
+    require_gpu()
+    Q, B = _sets(ref_table)[pset]
+    aoa, E, ctx, o = _setup(log_n, Q, B)
+    keys = make_keys(o, seed=21)
+    evk = aoa.SwitchKey(ctx, keys["evk"][0], keys["evk"][1], domain=aoa.AOA_NTT)
+    rng = np.random.default_rng(log_n)
+    N, k = E.N, E.k
+    a0, a1 = _rand_ct(rng, Q, N, k)
+    b0, b1 = _rand_ct(rng, Q, N, k)
+    dom = aoa.AOA_COEF if in_domain == "coef" else aoa.AOA_NTT
+    st = ST_COEF if in_domain == "coef" else ST_NTT
+    sa, sb = 1 << 40, (1 << 40) + 12345
+    ca = aoa.Ciphertext.from_residues(ctx, a0, a1, slots=N // 2, scale=sa, domain=dom)
+    cb = aoa.Ciphertext.from_residues(ctx, b0, b1, slots=N // 2, scale=sb, domain=dom)
+    for level in (k - 1, 2):
+        ca.set(level, N // 2, sa, ca.domain)
+        cb.set(level, N // 2, sb, cb.domain)
+        out = aoa.Ciphertext(ctx)
+        aoa.ckks_mul(ctx, out, ca, cb, evk)
+        # the oracle is not level aware: hand it the live limbs and stale zeros above
+        pad = lambda x: np.concatenate([x[: level + 1], np.zeros((k - level - 1, N), dtype=np.uint64)])
+        A = [pad(v) for v in (ca.download(domain=aoa.AOA_COEF if st == ST_COEF else aoa.AOA_NTT, nlimbs=k))]
+        Bc = [pad(v) for v in (cb.download(domain=aoa.AOA_COEF if st == ST_COEF else aoa.AOA_NTT, nlimbs=k))]
+        w0, w1, wsc = o.hmult(A, Bc, keys["evk"], level, sa, sb, rescale=True, a_state=st, b_state=st)
+        g0, g1 = out.download(nlimbs=level)
+        assert out.level == level - 1 and out.scale == wsc
+        assert np.array_equal(g0, w0[:level]) and np.array_equal(g1, w1[:level])
+
+
+def test_hmult_without_rescale_and_aliasing(ref_table):
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=4)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(8)
+    N, k = E.N, E.k
+    a0, a1 = _rand_ct(rng, Q, N, k)
+    ca = aoa.Ciphertext.from_residues(ctx, a0, a1, slots=4, scale=1 << 30)
+    w0, w1, wsc = o.hmult((a0, a1), (a0, a1), keys["evk"], k - 1, 1 << 30, 1 << 30, rescale=False)
+    aoa.ckks_mul_without_rescale(ctx, ca, ca, ca, evk)       # out aliases both inputs
+    g0, g1 = ca.download(nlimbs=k)
+    assert np.array_equal(g0, w0) and np.array_equal(g1, w1) and ca.scale == wsc
+
+
+@pytest.mark.parametrize("pset", ["ref55", "p60"])
+def test_rotate_conjugate_bit_exact(ref_table, pset):
+    require_gpu()
+    Q, B = _sets(ref_table)[pset]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=9, rotations=(1, 2, 64), conjugation=True)
+    rng = np.random.default_rng(1)
+    N, k = E.N, E.k
+    c0, c1 = _rand_ct(rng, Q, N, k)
+    for r in (1, 2, 64):
+        rtk = aoa.SwitchKey(ctx, *keys["rtk"][r])
+        ct = aoa.Ciphertext.from_residues(ctx, c0, c1, slots=N // 2)
+        out = aoa.Ciphertext(ctx)
+        aoa.ckks_rotate_left(ctx, out, ct, r, rtk)
+        w0, w1 = o.rotate_left((c0, c1), r, keys["rtk"][r], k - 1, state=ST_COEF)
+        g0, g1 = out.download(nlimbs=k)
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1), r
+    cjk = aoa.SwitchKey(ctx, *keys["cjk"])
+    ct = aoa.Ciphertext.from_residues(ctx, c0, c1, slots=N // 2)
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_conjugate(ctx, out, ct, cjk)
+    w0, w1 = o.conjugate((c0, c1), keys["cjk"], k - 1, state=ST_COEF)
+    g0, g1 = out.download(nlimbs=k)
+    assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+
+
+def test_add_sub_mixed_domains(ref_table):
+    require_gpu()
+    Q, B = _sets(ref_table)["ref55"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    rng = np.random.default_rng(2)
+    N, k = E.N, E.k
+    a = _rand_ct(rng, Q, N, k)
+    b = _rand_ct(rng, Q, N, k)
+    for sub in (False, True):
+        ca = aoa.Ciphertext.from_residues(ctx, *a, domain=aoa.AOA_NTT)
+        cb = aoa.Ciphertext.from_residues(ctx, *b, domain=aoa.AOA_COEF)
+        out = aoa.Ciphertext(ctx)
+        (aoa.ckks_sub if sub else aoa.ckks_add)(ctx, out, ca, cb)
+        w0, w1, st = o.add(a, b, subtract=sub, a_state=ST_NTT, b_state=ST_COEF)
+        assert st == ST_COEF and out.domain == aoa.AOA_COEF
+        g0, g1 = out.download(nlimbs=k, domain=aoa.AOA_COEF)
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+
+
+def test_error_statuses(ref_table):
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    rng = np.random.default_rng(0)
+    a = _rand_ct(rng, Q, E.N, E.k)
+    ca = aoa.Ciphertext.from_residues(ctx, *a, slots=8)
+    cb = aoa.Ciphertext.from_residues(ctx, *a, slots=16)
+    out = aoa.Ciphertext(ctx)
+    keys = make_keys(o, seed=1)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    with pytest.raises(aoa.AoaError) as ei:
+        aoa.ckks_mul(ctx, out, ca, cb, evk)
+    assert ei.value.name == "AOA_ERR_SLOT_MISMATCH"
+    with pytest.raises(aoa.AoaError) as ei:
+        aoa.ckks_mul(ctx, out, ca, ca, None)
+    assert ei.value.name == "AOA_ERR_NO_KEY"
+    ca.set(0, 8, 1 << 20, aoa.AOA_COEF)
+    with pytest.raises(aoa.AoaError) as ei:
+        aoa.ckks_mul(ctx, out, ca, ca, evk)
+    assert ei.value.name == "AOA_ERR_LEVEL_EXHAUSTED"
+    with pytest.raises(aoa.AoaError) as ei:
+        aoa.ckks_rescale(ctx, ca)
+    assert ei.value.name == "AOA_ERR_LEVEL_EXHAUSTED"
+    with pytest.raises(aoa.AoaError) as ei:
+        aoa.ckks_rotate_left(ctx, out, cb, 1, None)
+    assert ei.value.name == "AOA_ERR_NO_KEY"
+
+
+def test_encrypted_hmult_decodes_full_size():
+    """N = 2^16, 30 x 60-bit Q primes, 31 special primes, scale 2^50: the
+    decrypted product matches the FP64 cleartext product (size-independent
+    property at the benchmark's full size)."""
+    require_gpu()
+    import aoa_b200 as aoa
+    ps = oracle.gen_ntt_primes(60, 1 << 17, 61)
+    Q, B = ps[:30], ps[30:]
+    log_n = 16
+    E = aoa.Engine(log_n, Q, B, scale_bits=50)
+    ctx = aoa.Context(E)
+    o = Oracle(1 << log_n, Q, B)
+    keys = make_keys(o, seed=2)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(1)
+    slots = 1 << 15
+    r1, t1 = np.sqrt(rng.uniform(0, 1, slots)), rng.uniform(0, 2 * np.pi, slots)
+    r2, t2 = np.sqrt(rng.uniform(0, 1, slots)), rng.uniform(0, 2 * np.pi, slots)
+    v1, v2 = r1 * np.exp(1j * t1), r2 * np.exp(1j * t2)
+    scale = 1 << 50
+    c1 = encrypt_values(o, keys, v1, scale, seed=3)
+    c2 = encrypt_values(o, keys, v2, scale, seed=4)
+    g1 = aoa.Ciphertext.from_residues(ctx, *c1, slots=slots, scale=scale, domain=aoa.AOA_NTT)
+    g2 = aoa.Ciphertext.from_residues(ctx, *c2, slots=slots, scale=scale, domain=aoa.AOA_NTT)
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_mul(ctx, out, g1, g2, evk)
+    d0, d1 = out.download(nlimbs=out.level + 1)
+    pad = lambda x: np.concatenate([x, np.zeros((30 - x.shape[0], 1 << log_n), dtype=np.uint64)])
+    m = o.decrypt((pad(d0), pad(d1)), keys["s"][:30], state=ST_COEF)
+    got = o.decode(m[0], slots, out.scale)
+    err = np.abs(got - v1 * v2)
+    assert err.max() < 2.0 ** -20, err.max()
