@@ -262,3 +262,33 @@ def ckks_rotate_right(ctx, c2, c1, steps, rtk):
 
 def ckks_conjugate(ctx, c2, c1, cjk):
     capi.check(capi.load().aoa_conjugate(ctx.handle, c2.handle, c1.handle, _h(cjk)))
+
+
+class PinnedArray:
+    """Page-locked host array (aoa_host_alloc) viewed as numpy."""
+
+    def __init__(self, shape, dtype=np.uint64):
+        self.shape, self.dtype = tuple(shape), np.dtype(dtype)
+        nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        h = ctypes.c_void_p()
+        capi.check(capi.load().aoa_host_alloc(max(nbytes, 8), ctypes.byref(h)))
+        self.ptr = h
+        buf = (ctypes.c_char * max(nbytes, 8)).from_address(h.value)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=int(np.prod(self.shape))).reshape(self.shape)
+
+    def free(self):
+        if getattr(self, "ptr", None) is not None:
+            self.array = None
+            capi.load().aoa_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def kernel_launches():
+    """Kernels launched by libaoa_b200.so so far in this process."""
+    return int(capi.load().aoa_kernel_launches())

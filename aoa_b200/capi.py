@@ -44,6 +44,9 @@ class Params(ctypes.Structure):
 SIGNATURES = {
     "aoa_last_error": (c_char_p, []),
     "aoa_status_string": (c_char_p, [c_int]),
+    "aoa_kernel_launches": (c_long, []),
+    "aoa_search_primes": (c_int, [c_int, c_u64, c_int, u64p]),
+    "aoa_primitive_root": (c_u64, [c_u64]),
     "aoa_engine_create": (c_int, [ctypes.POINTER(Params), vpp]),
     "aoa_engine_destroy": (c_int, [c_void_p]),
     "aoa_engine_info": (c_int, [c_void_p, intp, intp, intp, u64p]),
@@ -53,6 +56,8 @@ SIGNATURES = {
     "aoa_ctx_stream": (c_int, [c_void_p, vpp]),
     "aoa_device_alloc": (c_int, [c_void_p, c_size_t, vpp]),
     "aoa_device_free": (c_int, [c_void_p, c_void_p]),
+    "aoa_host_alloc": (c_int, [c_size_t, vpp]),
+    "aoa_host_free": (c_int, [c_void_p]),
     "aoa_memcpy_h2d": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "aoa_memcpy_d2h": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "aoa_memcpy_d2d": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),

@@ -81,6 +81,9 @@ struct Ctx {
   size_t scratch_bytes = 0;
 };
 
+// count of kernel launches issued by this library (engine.cu)
+void note_launch();
+
 // C-ABI error plumbing (engine.cu)
 int fail(int status, const std::string& msg);
 

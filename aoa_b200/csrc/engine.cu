@@ -1,6 +1,7 @@
 // Engine set-up (prime tables, transform twiddles, RNS constants) and the core
 // of the C ABI declared in include/aoa_ckks.h.
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #ifdef _OPENMP
 #include <omp.h>
@@ -11,6 +12,9 @@
 namespace aoa {
 
 static thread_local std::string g_last_error;
+static std::atomic<long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int fail(int status, const std::string& msg) {
   g_last_error = msg;
@@ -146,6 +150,8 @@ extern "C" {
 
 const char* aoa_last_error(void) { return g_last_error.c_str(); }
 
+long aoa_kernel_launches(void) { return g_launches.load(); }
+
 const char* aoa_status_string(int s) {
   switch (s) {
     case AOA_OK: return "ok";
@@ -280,6 +286,28 @@ int aoa_device_alloc(aoa_ctx* h, size_t bytes, void** out) {
 int aoa_device_free(aoa_ctx* h, void* p) {
   if (!h) return fail(AOA_ERR_BAD_PARAM, "null context");
   return guarded([&] { AOA_CUDA(cudaFreeAsync(p, h->c.stream)); });
+}
+
+int aoa_search_primes(int bits, uint64_t modulus, int count, uint64_t* out) {
+  if (!out || count < 0) return fail(AOA_ERR_BAD_PARAM, "bad argument");
+  return h_search_primes(bits, modulus, count, out);
+}
+
+uint64_t aoa_primitive_root(uint64_t q) { return h_is_prime(q) ? h_smallest_primitive_root(q) : 0; }
+
+int aoa_host_alloc(size_t bytes, void** out) {
+  if (!out) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw AoaError(AOA_ERR_OOM, std::string("pinned host allocation failed: ") + cudaGetErrorString(e));
+    }
+  });
+}
+
+int aoa_host_free(void* p) {
+  return guarded([&] { AOA_CUDA(cudaFreeHost(p)); });
 }
 
 int aoa_memcpy_h2d(aoa_ctx* h, void* dst, const void* src, size_t n) {

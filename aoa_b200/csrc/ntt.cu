@@ -347,6 +347,7 @@ static void launch_cols(const NttBatch& b, int nlimbs, int npolys, bool fwd, cud
   dim3 grid(C / W, nlimbs, npolys);
   if (fwd) ntt_fwd_cols<LOG_R, W, LAZY><<<grid, T * W, 0, st>>>(b);
   else ntt_inv_cols<LOG_R, W, LAZY><<<grid, T * W, 0, st>>>(b);
+  note_launch();
 }
 
 template <int LOG_C, bool LAZY>
@@ -358,6 +359,7 @@ static void launch_rows(const NttBatch& b, int nlimbs, int npolys, bool fwd, cud
   dim3 grid(R / ROWS, nlimbs, npolys);
   if (fwd) ntt_fwd_rows<LOG_C, ROWS, LAZY><<<grid, T * ROWS, 0, st>>>(b);
   else ntt_inv_rows<LOG_C, ROWS, LAZY><<<grid, T * ROWS, 0, st>>>(b);
+  note_launch();
 }
 
 template <bool LAZY>

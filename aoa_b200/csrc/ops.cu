@@ -131,7 +131,7 @@ void ew_binary_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long
                   int op, int prime0, int nlimbs, int npolys, cudaStream_t st) {
   if (nlimbs <= 0 || npolys <= 0) return;
   ew_binary<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(Limbs{c, cs}, CLimbs{a, as}, CLimbs{b, bs}, op, prime0,
-                                                        E.d_pc, E.log_n);
+                                                        E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
@@ -139,7 +139,7 @@ void ew_scalar_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long
                   int op, int prime0, int nlimbs, int npolys, cudaStream_t st) {
   if (nlimbs <= 0 || npolys <= 0) return;
   ew_scalar<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(Limbs{c, cs}, CLimbs{a, as}, d_scalars, op, prime0,
-                                                        E.d_pc, E.log_n);
+                                                        E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
@@ -147,32 +147,32 @@ void ew_muladd_op(const Engine& E, uint64_t* d, long ds, const uint64_t* a, long
                   const uint64_t* c, long cs, int prime0, int nlimbs, int npolys, cudaStream_t st) {
   if (nlimbs <= 0 || npolys <= 0) return;
   ew_muladd<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(Limbs{d, ds}, CLimbs{a, as}, CLimbs{b, bs},
-                                                        CLimbs{c, cs}, prime0, E.d_pc, E.log_n);
+                                                        CLimbs{c, cs}, prime0, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
 void tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
                uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st) {
-  hmult_tensor<<<ew_grid(E, nlimbs, 1), 256, 0, st>>>(a, b, a_half, b_half, d0, d1, d2, E.d_pc, E.log_n);
+  hmult_tensor<<<ew_grid(E, nlimbs, 1), 256, 0, st>>>(a, b, a_half, b_half, d0, d1, d2, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
 void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
                       uint64_t* k1, int nq, cudaStream_t st) {
   const long half = (long)E.nprimes * E.N;
-  keyswitch_mul<<<ew_grid(E, nq + E.kl, 1), 256, 0, st>>>(xq, xb, key, half, k0, k1, nq, E.k, E.d_pc, E.log_n);
+  keyswitch_mul<<<ew_grid(E, nq + E.kl, 1), 256, 0, st>>>(xq, xb, key, half, k0, k1, nq, E.k, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
 void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,
                        int nlimbs, int npolys, cudaStream_t st) {
-  automorph_coef<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(out, in, poly_stride, galois, E.d_pc, E.log_n);
+  automorph_coef<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(out, in, poly_stride, galois, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
 void automorph_ntt_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,
                       int nlimbs, int npolys, cudaStream_t st) {
-  automorph_ntt<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(out, in, poly_stride, galois, E.log_n);
+  automorph_ntt<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(out, in, poly_stride, galois, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 

@@ -15,8 +15,11 @@
 
 namespace aoa {
 
-constexpr int kConvOut = 32;     // outputs per pass (register accumulators)
-constexpr int kConvThreads = 128;
+constexpr int kConvOut = 32;     // outputs per launch: kConvHalves groups of kConvAcc
+constexpr int kConvAcc = 16;     // register accumulators per thread
+constexpr int kConvHalves = kConvOut / kConvAcc;
+constexpr int kConvCoefs = 128;  // coefficients per CTA
+constexpr int kConvThreads = kConvCoefs * kConvHalves;
 
 // in:  nin limbs at `in` (stride N), under primes in_prime0 + i
 // out: nout limbs at `out` (stride N), under primes out_prime0 + j
@@ -39,7 +42,7 @@ struct ConvArgs {
   int post;
 };
 
-__global__ void __launch_bounds__(kConvThreads)
+__global__ void __launch_bounds__(kConvThreads, 3)
 basis_convert(ConvArgs a, int out_first) {
   extern __shared__ uint64_t smat[];    // [nin][kConvOut]
   const int nout = min(kConvOut, a.nout - out_first);
@@ -49,26 +52,30 @@ basis_convert(ConvArgs a, int out_first) {
   }
   __syncthreads();
   const long N = 1L << a.log_n;
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int half = threadIdx.x / kConvCoefs;          // which kConvAcc outputs of this launch
+  const long c = (long)blockIdx.x * kConvCoefs + (threadIdx.x % kConvCoefs);
   const uint64_t* in = a.in + blockIdx.y * a.in_poly_stride + c;
-  uint64_t lo[kConvOut], hi[kConvOut];
+  uint64_t lo[kConvAcc], hi[kConvAcc];
 #pragma unroll
-  for (int j = 0; j < kConvOut; j++) lo[j] = hi[j] = 0;
+  for (int j = 0; j < kConvAcc; j++) lo[j] = hi[j] = 0;
+  uint64_t x_next = in[0];
   for (int i = 0; i < a.nin; i++) {
+    const uint64_t x = x_next;
+    if (i + 1 < a.nin) x_next = in[(long)(i + 1) * N];     // prefetch the next input limb
     const uint64_t qi = a.pc[a.in_prime0 + i].q;
-    const ShoupW zc = a.zc[i];
-    const uint64_t z = shoup(in[(long)i * N], zc, qi);
-    const uint64_t* row = smat + i * kConvOut;
+    const uint64_t z = shoup(x, a.zc[i], qi);
+    const uint64_t* row = smat + i * kConvOut + half * kConvAcc;
 #pragma unroll
-    for (int j = 0; j < kConvOut; j++) mac128(lo[j], hi[j], z, row[j]);
+    for (int j = 0; j < kConvAcc; j++) mac128(lo[j], hi[j], z, row[j]);
   }
   uint64_t* out = a.out + blockIdx.y * a.out_poly_stride + c;
 #pragma unroll
-  for (int j = 0; j < kConvOut; j++) {
+  for (int jl = 0; jl < kConvAcc; jl++) {
+    const int j = half * kConvAcc + jl;
     if (j < nout) {
       const int jj = out_first + j;
       const PrimeConst& P = a.pc[a.out_prime0 + jj];
-      uint64_t r = reduce128(lo[j], hi[j], P);
+      uint64_t r = reduce128(lo[jl], hi[jl], P);
       if (a.post) {
         const uint64_t x = a.sub_src[blockIdx.y * a.sub_poly_stride + (long)jj * N + c];
         r = shoup(sub_mod(x, r, P.q), a.post_c[jj], P.q);
@@ -80,12 +87,14 @@ basis_convert(ConvArgs a, int out_first) {
 
 static void run_convert(const Engine& E, ConvArgs a, int npolys, cudaStream_t st) {
   const long N = E.N;
-  if (N % kConvThreads) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: N too small");
+  if (N % kConvCoefs) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: N too small");
   const size_t smem = (size_t)a.nin * kConvOut * sizeof(uint64_t);
   if (smem > 200 * 1024) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: too many input limbs");
-  dim3 grid(N / kConvThreads, npolys);
-  for (int j0 = 0; j0 < a.nout; j0 += kConvOut)
+  dim3 grid(N / kConvCoefs, npolys);
+  for (int j0 = 0; j0 < a.nout; j0 += kConvOut) {
     basis_convert<<<grid, kConvThreads, smem, st>>>(a, j0);
+    note_launch();
+  }
   AOA_CHECK_LAUNCH();
 }
 
@@ -152,7 +161,7 @@ void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int lev
   if (level < 1 || level >= E.k) throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "rescale: level must be >= 1");
   dim3 grid(E.N / 256, level, npolys);
   rescale_kernel<<<grid, 256, 0, st>>>(d, poly_stride, level, E.rns.resc_inv + (long)level * E.k, E.d_pc,
-                                       E.log_n);
+                                       E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 

@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark: batched HMult + relinearise + rescale at N = 2^16, L = 30.
+
+Workload (one "step"): B independent ckks_mul calls (HMult + relinearisation
+with the dnum = 1 evaluation key + rescale) on ciphertext pairs at level 29
+(30 live 60-bit Q primes, q = 1 mod 2^17, 31 special 60-bit primes, scale
+2^50).  Inputs are seeded uniform residues in the coefficient domain (the
+state a previous rescale leaves them in), so every call also runs the forward
+transforms of its operands.  Each pair occupies 60 MiB; a step touches far
+more than the 126 MB L2, so no L2 flush is needed between steps.
+
+Prints one JSON line (rank 0).  --impl reference times the CPU restatement of
+the reference algorithm (oracle/) on the host cores instead.
+Multi-GPU (torchrun): replicas only — each rank runs its own batch, no
+collective on the data path; value = all ranks' ops / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LOG_N, K, KL, SCALE_BITS = 16, 30, 31, 50
+METRIC = "Batched HMult+relin+rescale/s at N=2^16 L=30"
+UNIT = "HMult/s"
+
+
+def primes():
+    from aoa_b200 import params
+    return params.ntt_primes(60, 2 << LOG_N, K + KL)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.proc, self.path = index, None, None
+
+    def start(self):
+        try:
+            self.path = "/tmp/aoa_clocks_%d.csv" % os.getpid()
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference path (oracle/), all host threads."""
+    if rank != 0:
+        return
+    import oracle
+    from oracle import Oracle
+    threads = os.cpu_count() or 1
+    oracle.lib().oc_set_threads(threads)
+    ps = primes()
+    o = Oracle(1 << LOG_N, ps[:K], ps[K:])
+    rng = np.random.default_rng(1)
+    N = 1 << LOG_N
+    rr = lambda qs: np.array([rng.integers(0, q, N, dtype=np.uint64) for q in qs], dtype=np.uint64)
+    a, b = (rr(ps[:K]), rr(ps[:K])), (rr(ps[:K]), rr(ps[:K]))
+    evk = (rr(ps), rr(ps))
+    for _ in range(args.warmup):
+        o.hmult(a, b, evk, K - 1, 1 << SCALE_BITS, 1 << SCALE_BITS)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.hmult(a, b, evk, K - 1, 1 << SCALE_BITS, 1 << SCALE_BITS)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic",
+            "config": {"workload": "hmult_relin_rescale", "log_n": LOG_N, "q_limbs": K, "special_limbs": KL,
+                       "dnum": 1, "level": K - 1, "prime_bits": 60, "batch": 1},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "1 HMult+relin+rescale per step (reference op sequence, oracle/ckks_oracle.cpp)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def profile_case(args, aoa, ctx, rr, ps):
+    """Small fixed cases for ncu: `ntt` = forward + inverse over args.polys
+    polys of 30 limbs (args.polys * 15 MiB); `hmult` = 2 HMult+relin+rescale."""
+    N = 1 << LOG_N
+    if args.profile_case == "ntt":
+        buf = ctx.alloc((args.polys, K, N))
+        xs = rr(ps[:K])
+        for p in range(args.polys):
+            aoa.capi.check(aoa.capi.load().aoa_memcpy_h2d(ctx.handle, buf.offset(p * K * N), aoa.capi.ptr(xs),
+                                                          xs.nbytes))
+        for _ in range(2):
+            ctx.ntt_fwd(buf, args.polys, 0, K)
+            ctx.ntt_inv(buf, args.polys, 0, K)
+        ctx.sync()
+        assert np.array_equal(buf.numpy()[0], xs), "inverse(forward(x)) != x"
+    else:
+        evk = aoa.SwitchKey(ctx, rr(ps), rr(ps))
+        a = aoa.Ciphertext.from_residues(ctx, rr(ps[:K]), rr(ps[:K]), slots=N // 2, scale=1 << SCALE_BITS)
+        b = aoa.Ciphertext.from_residues(ctx, rr(ps[:K]), rr(ps[:K]), slots=N // 2, scale=1 << SCALE_BITS)
+        o = aoa.Ciphertext(ctx)
+        for _ in range(2):
+            a.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+            b.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+            aoa.ckks_mul(ctx, o, a, b, evk)
+        ctx.sync()
+    print("profile case done")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--impl", default="aoa", choices=["aoa", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["ntt", "hmult"],
+                    help="run a small fixed case for ncu captures (no timing, no JSON)")
+    ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    import aoa_b200 as aoa
+
+    ps = primes()
+    E = aoa.Engine(LOG_N, ps[:K], ps[K:], scale_bits=SCALE_BITS)
+    ctx = aoa.Context(E)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    N = 1 << LOG_N
+    B = args.batch
+    rng = np.random.default_rng(1000 + rank)
+    rr = lambda qs: np.array([rng.integers(0, q, N, dtype=np.uint64) for q in qs], dtype=np.uint64)
+    if args.profile_case:
+        profile_case(args, aoa, ctx, rr, ps)
+        return
+    evk = aoa.SwitchKey(ctx, rr(ps), rr(ps))
+    host_in = [(rr(ps[:K]), rr(ps[:K]), rr(ps[:K]), rr(ps[:K])) for _ in range(B)]
+    cts = [(aoa.Ciphertext.from_residues(ctx, x[0], x[1], slots=N // 2, scale=1 << SCALE_BITS),
+            aoa.Ciphertext.from_residues(ctx, x[2], x[3], slots=N // 2, scale=1 << SCALE_BITS)) for x in host_in]
+    outs = [aoa.Ciphertext(ctx) for _ in range(B)]
+
+    def step():
+        for (a, b), o in zip(cts, outs):
+            a.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+            b.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+            aoa.ckks_mul(ctx, o, a, b, evk)
+
+    def barrier():
+        torch.cuda.synchronize()
+        ctx.sync()
+        if pg:
+            pg.barrier()
+
+    def maxt(ms):
+        if not pg:
+            return ms
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident throughput -------------------------------------------
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = aoa.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
+    launches = aoa.kernel_launches() - l0
+    clk = clocks.stop()
+    ms = maxt(e0.elapsed_time(e1))
+    ms_step = ms / args.steps
+    value = world * B * args.steps / (ms / 1000.0)
+
+    # ---- per-call latency (plain per-call path, one op at a time) -------------
+    lat = []
+    (a0, b0), o0 = cts[0], outs[0]
+    for _ in range(max(20, args.steps)):
+        a0.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+        b0.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        aoa.ckks_mul(ctx, o0, a0, b0, evk)
+        s1.record(stream)
+        s1.synchronize()
+        lat.append(s0.elapsed_time(s1))
+    lat = np.array(lat)
+
+    # ---- NTT roofline (forward transform over 64 polys x 30 limbs) ----------------
+    npolys = 64
+    buf = ctx.alloc((npolys, K, N))
+    xs = rr(ps[:K])
+    for p in range(npolys):
+        aoa.capi.check(aoa.capi.load().aoa_memcpy_h2d(ctx.handle, buf.offset(p * K * N), aoa.capi.ptr(xs), xs.nbytes))
+    for _ in range(3):
+        ctx.ntt_fwd(buf, npolys, 0, K)
+        ctx.ntt_inv(buf, npolys, 0, K)
+    barrier()
+    reps = 5
+    t0, t1, t2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    t0.record(stream)
+    for _ in range(reps):
+        ctx.ntt_fwd(buf, npolys, 0, K)
+    t1.record(stream)
+    for _ in range(reps):
+        ctx.ntt_inv(buf, npolys, 0, K)
+    t2.record(stream)
+    barrier()
+    fwd_ms = t0.elapsed_time(t1) / reps
+    inv_ms = t1.elapsed_time(t2) / reps
+    algo_bytes = 16 * npolys * K * N          # read + write every coefficient once
+    achieved = algo_bytes / (fwd_ms / 1000.0) / 1e9
+    peak, peak_src = measured_peaks()
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tj = json.load(f)
+        if "ntt_fwd_bytes_per_coef" in tj:
+            traffic = tj["ntt_fwd_bytes_per_coef"] * npolys * K * N
+    del buf
+
+    # ---- end to end through the C ABI with host buffers -----------------------------
+    pin_in = [aoa.PinnedArray((2, K, N)) for _ in range(2 * B)]
+    for i, x in enumerate(host_in):
+        pin_in[2 * i].array[0], pin_in[2 * i].array[1] = x[0], x[1]
+        pin_in[2 * i + 1].array[0], pin_in[2 * i + 1].array[1] = x[2], x[3]
+    pin_out = [aoa.PinnedArray((2, K - 1, N)) for _ in range(B)]
+    lib = aoa.capi.load()
+
+    def e2e_step():
+        for i, ((a, b), o) in enumerate(zip(cts, outs)):
+            aoa.capi.check(lib.aoa_ct_upload(ctx.handle, a.handle, pin_in[2 * i].ptr, K, aoa.AOA_COEF))
+            aoa.capi.check(lib.aoa_ct_upload(ctx.handle, b.handle, pin_in[2 * i + 1].ptr, K, aoa.AOA_COEF))
+            a.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+            b.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+            aoa.ckks_mul(ctx, o, a, b, evk)
+            aoa.capi.check(lib.aoa_ct_download(ctx.handle, o.handle, pin_out[i].ptr, K - 1, aoa.AOA_COEF))
+
+    e2e_step()
+    barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, args.steps // 2)
+    q0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    q1.record(stream)
+    barrier()
+    e2e_ms = maxt(q0.elapsed_time(q1))
+    e2e_value = world * B * e2e_steps / (e2e_ms / 1000.0)
+    h2d = B * 2 * 2 * K * N * 8
+    d2h = B * 2 * (K - 1) * N * 8
+
+    # ---- CPU baseline (rank 0, N = 1): the oracle's reference op sequence ------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        from oracle import Oracle
+        threads = os.cpu_count() or 1
+        oracle.lib().oc_set_threads(threads)
+        o = Oracle(N, ps[:K], ps[K:])
+        x = host_in[0]
+        ek = (rr(ps), rr(ps))
+        o.hmult((x[0], x[1]), (x[2], x[3]), ek, K - 1, 1 << SCALE_BITS, 1 << SCALE_BITS)   # warm
+        n_cpu, tc = 0, time.perf_counter()
+        while n_cpu < 2 or time.perf_counter() - tc < 10.0:
+            o.hmult((x[0], x[1]), (x[2], x[3]), ek, K - 1, 1 << SCALE_BITS, 1 << SCALE_BITS)
+            n_cpu += 1
+            if n_cpu >= 20:
+                break
+        tc = time.perf_counter() - tc
+        cpu = {"value": n_cpu / tc, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "%d HMult+relin+rescale on the same N=2^16, k=30, kl=31 workload "
+                         "(reference op sequence, oracle/ckks_oracle.cpp, OpenMP)" % n_cpu}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "hmult_relin_rescale", "log_n": LOG_N, "q_limbs": K, "special_limbs": KL,
+                       "dnum": 1, "level": K - 1, "prime_bits": 60, "scale_bits": SCALE_BITS,
+                       "batch_per_gpu": B, "input_domain": "coefficient", "parallelism": "replicas",
+                       "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % B},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "single_op_ops_per_s": float(1000.0 / np.mean(lat))},
+            "ntt": {"fwd_ms": fwd_ms, "inv_ms": inv_ms, "polys": npolys, "limbs": K,
+                    "fwd_gbs": achieved, "inv_gbs": algo_bytes / (inv_ms / 1000.0) / 1e9,
+                    "hbm_frac": achieved / peak},
+            "roofline": {"kernel": "ntt forward (column + row kernel pair), N=2^16", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_src, "algorithmic_bytes": algo_bytes, "traffic": traffic},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -63,6 +63,21 @@ typedef struct {
 /* Last error message of this thread ("" if none). */
 const char* aoa_last_error(void);
 const char* aoa_status_string(int status);
+/* Number of CUDA kernels this library has launched in this process (all
+ * contexts); benchmarks difference it around a timed region.  No reference
+ * counterpart (the reference has no launch accounting).                     */
+long aoa_kernel_launches(void);
+
+/* --- prime selection (host only, no device needed).  The reference picks its
+ *     primes from fixed tables (src/cuda/htrans/coprimes.cu, selected by
+ *     fill_ckks_coprimes_bucket, src/cuda/manager.cu:426-464) and their
+ *     primitive roots from the PROOTS table.  aoa_search_primes returns the
+ *     `count` largest primes of exactly `bits` bits with q = 1 mod `modulus`
+ *     (descending; the count found is the return value, negative on error);
+ *     aoa_primitive_root returns the smallest primitive root of prime q (the
+ *     rule the reference's PROOTS entries follow), 0 if q is not prime.       */
+int aoa_search_primes(int bits, uint64_t modulus, int count, uint64_t* out);
+uint64_t aoa_primitive_root(uint64_t q);
 
 /* --- engine: replaces CUDAManager::init / destroy
  *     (aoa-ntt include/newckks/cuda/manager.h:52-80, src/cuda/manager.cu:762-821)
@@ -84,6 +99,9 @@ int aoa_ctx_stream(aoa_ctx* c, void** stream_out);
  *     poly_copy_to_host, src/arithmetic/poly_t.cpp:10-100).                    */
 int aoa_device_alloc(aoa_ctx* c, size_t bytes, void** out);
 int aoa_device_free(aoa_ctx* c, void* p);
+/* page-locked host memory, so host<->device copies run asynchronously */
+int aoa_host_alloc(size_t bytes, void** out);
+int aoa_host_free(void* p);
 int aoa_memcpy_h2d(aoa_ctx* c, void* dst, const void* src, size_t bytes);
 int aoa_memcpy_d2h(aoa_ctx* c, void* dst, const void* src, size_t bytes);
 int aoa_memcpy_d2d(aoa_ctx* c, void* dst, const void* src, size_t bytes);
