@@ -32,8 +32,11 @@ struct AoaError : public std::runtime_error {
       throw ::aoa::AoaError(AOA_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
   } while (0)
 
+constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration limit
+
 struct Tune {
   long ntt_chunk_bytes = 48L << 20;   // per NTT launch pair: stays inside L2
+  int ntt_polys_per_cta = 8;          // polys a transform CTA streams through its buffers
 };
 
 // Device copy of the basis-conversion / rescale constants.
@@ -70,6 +73,9 @@ struct Engine {
   ShoupW* d_itw = nullptr;    // [nprimes][N]
   RnsTables rns;
   Tune tune;
+  // Device error word: kernels OR in kErr* bits instead of trapping (a bounded
+  // wait that expired, ...); aoa_ctx_sync reads and clears it.
+  unsigned* d_err = nullptr;
   std::vector<void*> allocations;
 };
 
@@ -102,6 +108,7 @@ int guarded(F&& f) {
 }
 
 // ntt.cu
+void ntt_init(Engine& E);
 void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
                long poly_stride, bool forward, cudaStream_t st);
 

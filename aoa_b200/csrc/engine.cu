@@ -81,6 +81,7 @@ static void build_prime_tables(Engine& E) {
   E.d_pc = dev_upload(E, E.h_pc);
   E.d_tw = dev_upload(E, tw);
   E.d_itw = dev_upload(E, itw);
+  E.d_err = dev_upload(E, std::vector<unsigned>(1, 0u));
 }
 
 // Basis-conversion and rescale constants (manager.cu:566-759).
@@ -203,6 +204,7 @@ int aoa_engine_create(const aoa_params* p, aoa_engine** out) {
     build_prime_tables(E);
     build_rns_tables(E);
     rns_init(E);
+    ntt_init(E);
     AOA_CUDA(cudaDeviceSynchronize());
   });
   if (st != AOA_OK) {
@@ -263,7 +265,16 @@ int aoa_ctx_destroy(aoa_ctx* h) {
 
 int aoa_ctx_sync(aoa_ctx* h) {
   if (!h) return fail(AOA_ERR_BAD_PARAM, "null context");
-  return guarded([&] { AOA_CUDA(cudaStreamSynchronize(h->c.stream)); });
+  return guarded([&] {
+    AOA_CUDA(cudaStreamSynchronize(h->c.stream));
+    unsigned err = 0;
+    AOA_CUDA(cudaMemcpy(&err, h->c.E->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+    if (err) {
+      AOA_CUDA(cudaMemset(h->c.E->d_err, 0, sizeof(unsigned)));
+      throw AoaError(AOA_ERR_TIMEOUT, "a device-side bounded wait expired (error bits 0x" + std::to_string(err) +
+                                          "); the affected results are invalid");
+    }
+  });
 }
 
 int aoa_ctx_stream(aoa_ctx* h, void** s) {

@@ -89,11 +89,26 @@ AOA_HD uint64_t reduce128(uint64_t lo, uint64_t hi, const PrimeConst& P) {
   return add_mod(h, l, P.q);
 }
 
-// 128-bit multiply-accumulate: (hi:lo) += a * b
+// 128-bit multiply-accumulate: (hi:lo) += a * b, as three 32-bit carry chains
+// over the four partial products (a0 b0 + a1 b1 2^64, then a0 b1 2^32, a1 b0 2^32).
 AOA_HD void mac128(uint64_t& lo, uint64_t& hi, uint64_t a, uint64_t b) {
 #ifdef __CUDA_ARCH__
-  uint64_t pl = a * b, ph = __umul64hi(a, b);
-  asm("add.cc.u64 %0, %0, %2;\n\taddc.u64 %1, %1, %3;" : "+l"(lo), "+l"(hi) : "l"(pl), "l"(ph));
+  uint32_t r0 = (uint32_t)lo, r1 = (uint32_t)(lo >> 32), r2 = (uint32_t)hi, r3 = (uint32_t)(hi >> 32);
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  asm("mad.lo.cc.u32 %0, %4, %6, %0;\n\t"
+      "madc.hi.cc.u32 %1, %4, %6, %1;\n\t"
+      "madc.lo.cc.u32 %2, %5, %7, %2;\n\t"
+      "madc.hi.u32 %3, %5, %7, %3;\n\t"
+      "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+      "madc.hi.cc.u32 %2, %4, %7, %2;\n\t"
+      "addc.u32 %3, %3, 0;\n\t"
+      "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "addc.u32 %3, %3, 0;"
+      : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  lo = ((uint64_t)r1 << 32) | r0;
+  hi = ((uint64_t)r3 << 32) | r2;
 #else
   unsigned __int128 s = ((unsigned __int128)hi << 64 | lo) + (unsigned __int128)a * b;
   lo = (uint64_t)s; hi = (uint64_t)(s >> 64);

@@ -110,13 +110,11 @@ __device__ __forceinline__ void fwd_high(uint64_t (&v)[Sub<LOG_S>::E], const Sho
   for (int i = D::HI - 1; i >= 0; i--) {
     const int span = 1 << i;
 #pragma unroll
-    for (int g = 0; g < (1 << (D::HI - 1 - i)); g++) {
+    for (int h = 0; h < D::E; h++) {
+      if (h & span) continue;
+      const int g = h >> (i + 1);
       const ShoupW w = tw[(K << (D::HI - 1 - i)) + g];
-#pragma unroll
-      for (int o = 0; o < span; o++) {
-        const int h = (g << (i + 1)) + o;
         Bf<LAZY>::ct(v[h], v[h + span], w, q);
-      }
     }
   }
 }
@@ -129,13 +127,11 @@ __device__ __forceinline__ void fwd_low(uint64_t (&u)[Sub<LOG_S>::L], const Shou
   for (int i = D::LO - 1; i >= 0; i--) {
     const int span = 1 << i;
 #pragma unroll
-    for (int g = 0; g < (1 << (D::LO - 1 - i)); g++) {
+    for (int l = 0; l < D::L; l++) {
+      if (l & span) continue;
+      const int g = l >> (i + 1);
       const ShoupW w = tw[(K << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + g];
-#pragma unroll
-      for (int o = 0; o < span; o++) {
-        const int l = (g << (i + 1)) + o;
         Bf<LAZY>::ct(u[l], u[l + span], w, q);
-      }
     }
   }
 }
@@ -150,13 +146,11 @@ __device__ __forceinline__ void inv_low(uint64_t (&u)[Sub<LOG_S>::L], const Shou
   for (int i = 0; i < D::LO; i++) {
     const int span = 1 << i;
 #pragma unroll
-    for (int g = 0; g < (1 << (D::LO - 1 - i)); g++) {
+    for (int l = 0; l < D::L; l++) {
+      if (l & span) continue;
+      const int g = l >> (i + 1);
       const ShoupW w = itw[(K << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + g];
-#pragma unroll
-      for (int o = 0; o < span; o++) {
-        const int l = (g << (i + 1)) + o;
         Bf<LAZY>::gs(u[l], u[l + span], w, q);
-      }
     }
   }
 }
@@ -170,92 +164,242 @@ __device__ __forceinline__ void inv_high(uint64_t (&v)[Sub<LOG_S>::E], const Sho
   for (int i = 0; i < D::HI; i++) {
     const int span = 1 << i;
 #pragma unroll
-    for (int g = 0; g < (1 << (D::HI - 1 - i)); g++) {
+    for (int h = 0; h < D::E; h++) {
+      if (h & span) continue;
+      const int g = h >> (i + 1);
       const ShoupW w = itw[(K << (D::HI - 1 - i)) + g];
-#pragma unroll
-      for (int o = 0; o < span; o++) {
-        const int h = (g << (i + 1)) + o;
         if (LAST && i == D::HI - 1) Bf<LAZY>::gs_last(v[h], v[h + span], ninv, ninv_w1, q);
         else Bf<LAZY>::gs(v[h], v[h + span], w, q);
-      }
     }
   }
 }
 
+// ---- register-twiddle variants of the low-digit rounds ------------------------
+// Row kernels keep each thread's low-digit twiddles in registers for all the
+// polys a CTA processes: list order is stage-major (j = 2^(LO-1-i) - 1 + g).
+
+template <int LOG_S>
+__device__ __forceinline__ void load_low_tw(ShoupW (&w)[Sub<LOG_S>::G][Sub<LOG_S>::L - 1],
+                                            const ShoupW* __restrict__ tw, uint32_t K, int t) {
+  using D = Sub<LOG_S>;
+#pragma unroll
+  for (int gg = 0; gg < D::G; gg++) {
+    const uint32_t hi = t * D::G + gg;
+#pragma unroll
+    for (int j = 0; j < D::L - 1; j++) {
+      // entry j belongs to the stage with 2^lvl twiddles (lvl = LO-1-i), group g
+      const int lvl = 31 - __clz(j + 1);
+      const int g = j + 1 - (1 << lvl);
+      w[gg][j] = tw[(K << (LOG_S - D::LO + lvl)) + (hi << lvl) + g];
+    }
+  }
+}
+
+template <int LOG_S, bool LAZY>
+__device__ __forceinline__ void fwd_low_r(uint64_t (&u)[Sub<LOG_S>::L], const ShoupW (&w)[Sub<LOG_S>::L - 1],
+                                          uint64_t q) {
+  using D = Sub<LOG_S>;
+#pragma unroll
+  for (int i = D::LO - 1; i >= 0; i--) {
+    const int span = 1 << i;
+#pragma unroll
+    for (int l = 0; l < D::L; l++) {
+      if (l & span) continue;
+      const int g = l >> (i + 1);
+      const ShoupW tw = w[(1 << (D::LO - 1 - i)) - 1 + g];
+        Bf<LAZY>::ct(u[l], u[l + span], tw, q);
+    }
+  }
+}
+
+template <int LOG_S, bool LAZY>
+__device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const ShoupW (&w)[Sub<LOG_S>::L - 1],
+                                          uint64_t q) {
+  using D = Sub<LOG_S>;
+#pragma unroll
+  for (int i = 0; i < D::LO; i++) {
+    const int span = 1 << i;
+#pragma unroll
+    for (int l = 0; l < D::L; l++) {
+      if (l & span) continue;
+      const int g = l >> (i + 1);
+      const ShoupW tw = w[(1 << (D::LO - 1 - i)) - 1 + g];
+        Bf<LAZY>::gs(u[l], u[l + span], tw, q);
+    }
+  }
+}
+
+// ---- asynchronous bulk copies (TMA engine) and mbarriers --------------------------
+
+constexpr int kSpinLimit = 1 << 20;     // bounded mbarrier waits
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)), "r"(bytes)
+               : "memory");
+}
+
+// global -> shared bulk copy; bytes % 16 == 0, both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mb) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(mb))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* mb, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(mb)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for phase `parity` of the barrier; gives up after kSpinLimit tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
+  for (int i = 0; i < kSpinLimit; i++)
+    if (mbar_try_wait(mb, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // ---- kernels ---------------------------------------------------------------
 // Batch addressing: limb (poly p, limb l) lives at data + (p*poly_stride + l)*N
-// and uses prime first_prime + l.  grid = (tiles per limb, nlimbs, npolys).
+// and uses prime first_prime + l.  grid = (tiles per limb, nlimbs, poly groups);
+// a CTA transforms the same tile of the same limb for polys_per_cta polys,
+// streaming them through two shared-memory buffers filled by bulk copies.
 
 struct NttBatch {
   uint64_t* data;
   const ShoupW* tw;        // [nprimes][N] forward twiddles (psi^bitrev)
   const ShoupW* itw;       // [nprimes][N] inverse twiddles
   const PrimeConst* pc;    // [nprimes]
+  unsigned* err;           // device error word
   int log_n, log_r, log_c; // N = R * C
   int first_prime;
   long poly_stride;        // limbs between consecutive polys
+  int npolys, polys_per_cta;
 };
 
-template <int LOG_R, int W, bool LAZY>
-__global__ void __launch_bounds__(Sub<LOG_R>::T * W)
-ntt_fwd_cols(NttBatch b) {
-  using D = Sub<LOG_R>;
-  __shared__ uint64_t sm[D::S][W];
-  const int w = threadIdx.x % W, t = threadIdx.x / W;
-  const int prime = b.first_prime + blockIdx.y;
-  const long N = 1L << b.log_n, C = 1L << b.log_c;
-  const uint64_t q = b.pc[prime].q;
-  uint64_t* x = b.data + ((long)blockIdx.z * b.poly_stride + blockIdx.y) * N + (long)blockIdx.x * W + w;
-  const ShoupW* tw = b.tw + (long)prime * N;
-  uint64_t v[D::E];
-#pragma unroll
-  for (int h = 0; h < D::E; h++) v[h] = x[(long)((h << D::LO) + t) * C];
-  fwd_high<LOG_R, LAZY>(v, tw, 1, q);
-#pragma unroll
-  for (int h = 0; h < D::E; h++) sm[(h << D::LO) + t][w] = v[h];
-  __syncthreads();
-#pragma unroll
-  for (int g = 0; g < D::G; g++) {
-    const int hi = t * D::G + g;
-    uint64_t u[D::L];
-#pragma unroll
-    for (int l = 0; l < D::L; l++) u[l] = sm[(hi << D::LO) + l][w];
-    fwd_low<LOG_R, LAZY>(u, tw, 1, hi, q);
-#pragma unroll
-    for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
-  }
+// Shared-memory budget of the kernels below (dynamic part).
+template <int LOG_S>
+constexpr int tile_words() { return Sub<LOG_S>::PER_CTA * Sub<LOG_S>::S; }
+
+template <int LOG_R>
+constexpr size_t cols_smem() { return 2 * tile_words<LOG_R>() * 8 + (size_t)Sub<LOG_R>::S * sizeof(ShoupW); }
+
+template <int LOG_C>
+constexpr size_t rows_smem() {
+  return 2 * tile_words<LOG_C>() * 8 + (size_t)Sub<LOG_C>::PER_CTA * (Sub<LOG_C>::E - 1) * sizeof(ShoupW);
 }
 
-template <int LOG_R, int W, bool LAZY>
-__global__ void __launch_bounds__(Sub<LOG_R>::T * W)
-ntt_inv_cols(NttBatch b) {
+// Column pass.  Tile = S rows x W columns of one limb; the load is S bulk copies
+// of W*8 bytes (one per row) issued by warp 0.
+template <int LOG_R, bool LAZY, bool FWD>
+__global__ void __launch_bounds__(Sub<LOG_R>::T * Sub<LOG_R>::PER_CTA, 3)
+ntt_cols(NttBatch b) {
   using D = Sub<LOG_R>;
-  __shared__ uint64_t sm[D::S][W];
+  constexpr int W = D::PER_CTA;
+  constexpr int TILE = D::S * W;
+  extern __shared__ __align__(128) uint64_t dyn[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  uint64_t* bufs = dyn;                                   // [2][S][W]
+  ShoupW* tws = (ShoupW*)(dyn + 2 * TILE);                 // [S]: twiddles 0..S-1 (K = 1)
   const int w = threadIdx.x % W, t = threadIdx.x / W;
-  const int prime = b.first_prime + blockIdx.y;
+  const int limb = blockIdx.y, prime = b.first_prime + limb;
   const long N = 1L << b.log_n, C = 1L << b.log_c;
   const PrimeConst& P = b.pc[prime];
   const uint64_t q = P.q;
-  const ShoupW ninv{P.ninv, P.ninv_sh}, ninv_w1{P.ninv_w1, P.ninv_w1_sh};
-  uint64_t* x = b.data + ((long)blockIdx.z * b.poly_stride + blockIdx.y) * N + (long)blockIdx.x * W + w;
-  const ShoupW* itw = b.itw + (long)prime * N;
-#pragma unroll
-  for (int g = 0; g < D::G; g++) {
-    const int hi = t * D::G + g;
-    uint64_t u[D::L];
-#pragma unroll
-    for (int l = 0; l < D::L; l++) u[l] = x[(long)((hi << D::LO) + l) * C];
-    inv_low<LOG_R, LAZY>(u, itw, 1, hi, q);
-#pragma unroll
-    for (int l = 0; l < D::L; l++) sm[(hi << D::LO) + l][w] = u[l];
+  const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
+  const int p0 = blockIdx.z * b.polys_per_cta;
+  const int p1 = min(b.npolys, p0 + b.polys_per_cta);
+  for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[e] = tw[e];
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    mbar_init_fence();
   }
   __syncthreads();
-  uint64_t v[D::E];
+  auto tile_src = [&](int p) -> uint64_t* {
+    return b.data + ((long)p * b.poly_stride + limb) * N + (long)blockIdx.x * W;
+  };
+  auto issue = [&](int p, int bi) {        // warp 0: S row segments of W words
+    if (threadIdx.x < 32) {
+      if (threadIdx.x == 0) mbar_expect_tx(&mbar[bi], TILE * 8);
+      __syncwarp();
+      const uint64_t* src = tile_src(p);
+      for (int r = threadIdx.x; r < D::S; r += 32)
+        bulk_g2s(bufs + bi * TILE + r * W, src + r * C, W * 8, &mbar[bi]);
+    }
+  };
+  if (p0 < p1) issue(p0, 0);
+  for (int p = p0; p < p1; p++) {
+    const int it = p - p0, bi = it & 1;
+    if (p + 1 < p1) issue(p + 1, bi ^ 1);
+    const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
+      if (p + 1 < p1) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);   // drain the copy in flight
+      return;
+    }
+    uint64_t(*sm)[W] = (uint64_t(*)[W])(bufs + bi * TILE);
+    uint64_t* x = tile_src(p) + w;
+    if (FWD) {
+      uint64_t v[D::E];
 #pragma unroll
-  for (int h = 0; h < D::E; h++) v[h] = sm[(h << D::LO) + t][w];
-  inv_high<LOG_R, LAZY, true>(v, itw, 1, q, ninv, ninv_w1);
+      for (int h = 0; h < D::E; h++) v[h] = sm[(h << D::LO) + t][w];
+      fwd_high<LOG_R, LAZY>(v, tws, 1, q);
 #pragma unroll
-  for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];
+      for (int h = 0; h < D::E; h++) sm[(h << D::LO) + t][w] = v[h];
+      __syncthreads();
+#pragma unroll
+      for (int g = 0; g < D::G; g++) {
+        const int hi = t * D::G + g;
+        uint64_t u[D::L];
+#pragma unroll
+        for (int l = 0; l < D::L; l++) u[l] = sm[(hi << D::LO) + l][w];
+        fwd_low<LOG_R, LAZY>(u, tws, 1, hi, q);
+#pragma unroll
+        for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
+      }
+    } else {
+      const ShoupW ninv{P.ninv, P.ninv_sh}, ninv_w1{P.ninv_w1, P.ninv_w1_sh};
+#pragma unroll
+      for (int g = 0; g < D::G; g++) {
+        const int hi = t * D::G + g;
+        uint64_t u[D::L];
+#pragma unroll
+        for (int l = 0; l < D::L; l++) u[l] = sm[(hi << D::LO) + l][w];
+        inv_low<LOG_R, LAZY>(u, tws, 1, hi, q);
+#pragma unroll
+        for (int l = 0; l < D::L; l++) sm[(hi << D::LO) + l][w] = u[l];
+      }
+      __syncthreads();
+      uint64_t v[D::E];
+#pragma unroll
+      for (int h = 0; h < D::E; h++) v[h] = sm[(h << D::LO) + t][w];
+      inv_high<LOG_R, LAZY, true>(v, tws, 1, q, ninv, ninv_w1);
+#pragma unroll
+      for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];
+    }
+    // generic-proxy accesses of buffer bi end here; the next bulk copy into it
+    // (issued in the next iteration) is an async-proxy write
+    fence_proxy_async();
+    __syncthreads();
+  }
 }
 
 // swizzled position inside one row of shared memory
@@ -264,153 +408,236 @@ __device__ __forceinline__ int swz(int hi, int lo) {
   return (hi << Sub<LOG_S>::LO) + (lo ^ (hi & (Sub<LOG_S>::L - 1)));
 }
 
-template <int LOG_C, int ROWS, bool LAZY>
-__global__ void __launch_bounds__(Sub<LOG_C>::T * ROWS)
-ntt_fwd_rows(NttBatch b) {
+// Row pass.  Tile = ROWS contiguous rows of one limb: one bulk copy.
+template <int LOG_C, bool LAZY, bool FWD>
+__global__ void __launch_bounds__(Sub<LOG_C>::T * Sub<LOG_C>::PER_CTA, 2)
+ntt_rows(NttBatch b) {
   using D = Sub<LOG_C>;
-  __shared__ uint64_t sm[ROWS][D::S];
+  constexpr int ROWS = D::PER_CTA;
+  constexpr int TILE = ROWS * D::S;
+  constexpr int NT1 = D::E - 1;                           // high-digit twiddles per row
+  extern __shared__ __align__(128) uint64_t dyn[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  uint64_t* bufs = dyn;                                   // [2][ROWS][S]
+  ShoupW* tw1 = (ShoupW*)(dyn + 2 * TILE);                 // [ROWS][NT1]
   const int t = threadIdx.x % D::T, rho = threadIdx.x / D::T;
-  const int prime = b.first_prime + blockIdx.y;
+  const int limb = blockIdx.y, prime = b.first_prime + limb;
   const long N = 1L << b.log_n;
-  const uint32_t row = blockIdx.x * ROWS + rho;
+  const uint32_t row0 = blockIdx.x * ROWS;
+  const uint32_t Kbase = (1u << b.log_r) + row0;
   const uint64_t q = b.pc[prime].q;
-  uint64_t* x = b.data + ((long)blockIdx.z * b.poly_stride + blockIdx.y) * N + ((long)row << LOG_C);
-  const ShoupW* tw = b.tw + (long)prime * N;
-  const uint32_t K = (1u << b.log_r) + row;
-  uint64_t* s = sm[rho];
-  uint64_t v[D::E];
-#pragma unroll
-  for (int h = 0; h < D::E; h++) v[h] = x[(h << D::LO) + t];
-  fwd_high<LOG_C, LAZY>(v, tw, K, q);
-#pragma unroll
-  for (int h = 0; h < D::E; h++) s[swz<LOG_C>(h, t)] = v[h];
-  __syncwarp();
-#pragma unroll
-  for (int g = 0; g < D::G; g++) {
-    const int hi = t * D::G + g;
-    uint64_t u[D::L];
-#pragma unroll
-    for (int l = 0; l < D::L; l++) u[l] = s[swz<LOG_C>(hi, l)];
-    fwd_low<LOG_C, LAZY>(u, tw, K, hi, q);
-#pragma unroll
-    for (int l = 0; l < D::L; l++) s[swz<LOG_C>(hi, l)] = u[l];
+  const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
+  const int p0 = blockIdx.z * b.polys_per_cta;
+  const int p1 = min(b.npolys, p0 + b.polys_per_cta);
+  for (int e = threadIdx.x; e < ROWS * NT1; e += blockDim.x) {
+    const int r = e / NT1, j = e % NT1;
+    const int lvl = 31 - __clz(j + 1);                    // stage level: 2^lvl twiddles
+    const int g = j + 1 - (1 << lvl);
+    tw1[e] = tw[((Kbase + r) << lvl) + g];
   }
-  __syncwarp();
-#pragma unroll
-  for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = Bf<LAZY>::fwd_out(s[swz<LOG_C>(h, t)], q);
-}
-
-template <int LOG_C, int ROWS, bool LAZY>
-__global__ void __launch_bounds__(Sub<LOG_C>::T * ROWS)
-ntt_inv_rows(NttBatch b) {
-  using D = Sub<LOG_C>;
-  __shared__ uint64_t sm[ROWS][D::S];
-  const int t = threadIdx.x % D::T, rho = threadIdx.x / D::T;
-  const int prime = b.first_prime + blockIdx.y;
-  const long N = 1L << b.log_n;
-  const uint32_t row = blockIdx.x * ROWS + rho;
-  const uint64_t q = b.pc[prime].q;
-  uint64_t* x = b.data + ((long)blockIdx.z * b.poly_stride + blockIdx.y) * N + ((long)row << LOG_C);
-  const ShoupW* itw = b.itw + (long)prime * N;
-  const uint32_t K = (1u << b.log_r) + row;
-  uint64_t* s = sm[rho];
-#pragma unroll
-  for (int h = 0; h < D::E; h++) s[swz<LOG_C>(h, t)] = x[(h << D::LO) + t];
-  __syncwarp();
-#pragma unroll
-  for (int g = 0; g < D::G; g++) {
-    const int hi = t * D::G + g;
-    uint64_t u[D::L];
-#pragma unroll
-    for (int l = 0; l < D::L; l++) u[l] = s[swz<LOG_C>(hi, l)];
-    inv_low<LOG_C, LAZY>(u, itw, K, hi, q);
-#pragma unroll
-    for (int l = 0; l < D::L; l++) s[swz<LOG_C>(hi, l)] = u[l];
+  ShoupW w2[D::G][D::L - 1];
+  load_low_tw<LOG_C>(w2, tw, Kbase + rho, t);
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    mbar_init_fence();
   }
-  __syncwarp();
-  uint64_t v[D::E];
+  __syncthreads();
+  auto tile_src = [&](int p) -> uint64_t* {
+    return b.data + ((long)p * b.poly_stride + limb) * N + ((long)row0 << LOG_C);
+  };
+  auto issue = [&](int p, int bi) {
+    mbar_expect_tx(&mbar[bi], TILE * 8);
+    bulk_g2s(bufs + bi * TILE, tile_src(p), TILE * 8, &mbar[bi]);
+  };
+  if (threadIdx.x == 0 && p0 < p1) issue(p0, 0);
+  const ShoupW* t1 = tw1 + rho * NT1;
+  for (int p = p0; p < p1; p++) {
+    const int it = p - p0, bi = it & 1;
+    if (threadIdx.x == 0 && p + 1 < p1) issue(p + 1, bi ^ 1);
+    const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
+      if (p + 1 < p1) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);
+      return;
+    }
+    uint64_t* s = bufs + bi * TILE + rho * D::S;
+    uint64_t* x = tile_src(p) + rho * D::S;
+    uint64_t v[D::E];
+    if (FWD) {
 #pragma unroll
-  for (int h = 0; h < D::E; h++) v[h] = s[swz<LOG_C>(h, t)];
-  inv_high<LOG_C, LAZY, false>(v, itw, K, q, ShoupW{0, 0}, ShoupW{0, 0});
+      for (int h = 0; h < D::E; h++) v[h] = s[(h << D::LO) + t];
+      // high-digit stages: twiddle (K << (HI-1-i)) + g sits at t1[2^(HI-1-i) - 1 + g]
 #pragma unroll
-  for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = v[h];
+      for (int i = D::HI - 1; i >= 0; i--) {
+        const int span = 1 << i;
+#pragma unroll
+        for (int h = 0; h < D::E; h++) {
+          if (h & span) continue;
+          const int g = h >> (i + 1);
+          const ShoupW wv = t1[(1 << (D::HI - 1 - i)) - 1 + g];
+            Bf<LAZY>::ct(v[h], v[h + span], wv, q);
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < D::E; h++) s[swz<LOG_C>(h, t)] = v[h];
+      __syncwarp();
+#pragma unroll
+      for (int gg = 0; gg < D::G; gg++) {
+        const int hi = t * D::G + gg;
+        uint64_t u[D::L];
+#pragma unroll
+        for (int l = 0; l < D::L; l++) u[l] = s[swz<LOG_C>(hi, l)];
+        fwd_low_r<LOG_C, LAZY>(u, w2[gg], q);
+#pragma unroll
+        for (int l = 0; l < D::L; l++) s[swz<LOG_C>(hi, l)] = u[l];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = Bf<LAZY>::fwd_out(s[swz<LOG_C>(h, t)], q);
+    } else {
+#pragma unroll
+      for (int h = 0; h < D::E; h++) v[h] = s[(h << D::LO) + t];
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < D::E; h++) s[swz<LOG_C>(h, t)] = v[h];
+      __syncwarp();
+#pragma unroll
+      for (int gg = 0; gg < D::G; gg++) {
+        const int hi = t * D::G + gg;
+        uint64_t u[D::L];
+#pragma unroll
+        for (int l = 0; l < D::L; l++) u[l] = s[swz<LOG_C>(hi, l)];
+        inv_low_r<LOG_C, LAZY>(u, w2[gg], q);
+#pragma unroll
+        for (int l = 0; l < D::L; l++) s[swz<LOG_C>(hi, l)] = u[l];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < D::E; h++) v[h] = s[swz<LOG_C>(h, t)];
+#pragma unroll
+      for (int i = 0; i < D::HI; i++) {
+        const int span = 1 << i;
+#pragma unroll
+        for (int h = 0; h < D::E; h++) {
+          if (h & span) continue;
+          const int g = h >> (i + 1);
+          const ShoupW wv = t1[(1 << (D::HI - 1 - i)) - 1 + g];
+            Bf<LAZY>::gs(v[h], v[h + span], wv, q);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = v[h];
+    }
+    fence_proxy_async();
+    __syncthreads();
+  }
 }
 
 // ---- host launchers ----------------------------------------------------------
 
 template <int LOG_R, bool LAZY>
-static void launch_cols(const NttBatch& b, int nlimbs, int npolys, bool fwd, cudaStream_t st) {
+static void launch_cols(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
   constexpr int T = Sub<LOG_R>::T;
-  constexpr int W = Sub<LOG_R>::PER_CTA;        // columns per CTA
+  constexpr int W = Sub<LOG_R>::PER_CTA;
   const int C = 1 << b.log_c;
   if (C % W) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: column tile does not divide C");
-  dim3 grid(C / W, nlimbs, npolys);
-  if (fwd) ntt_fwd_cols<LOG_R, W, LAZY><<<grid, T * W, 0, st>>>(b);
-  else ntt_inv_cols<LOG_R, W, LAZY><<<grid, T * W, 0, st>>>(b);
+  dim3 grid(C / W, nlimbs, groups);
+  constexpr size_t smem = cols_smem<LOG_R>();
+  if (fwd) ntt_cols<LOG_R, LAZY, true><<<grid, T * W, smem, st>>>(b);
+  else ntt_cols<LOG_R, LAZY, false><<<grid, T * W, smem, st>>>(b);
   note_launch();
 }
 
 template <int LOG_C, bool LAZY>
-static void launch_rows(const NttBatch& b, int nlimbs, int npolys, bool fwd, cudaStream_t st) {
+static void launch_rows(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
   constexpr int T = Sub<LOG_C>::T;
   constexpr int ROWS = Sub<LOG_C>::PER_CTA;
   const int R = 1 << b.log_r;
   if (R % ROWS) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: row tile does not divide R");
-  dim3 grid(R / ROWS, nlimbs, npolys);
-  if (fwd) ntt_fwd_rows<LOG_C, ROWS, LAZY><<<grid, T * ROWS, 0, st>>>(b);
-  else ntt_inv_rows<LOG_C, ROWS, LAZY><<<grid, T * ROWS, 0, st>>>(b);
+  dim3 grid(R / ROWS, nlimbs, groups);
+  constexpr size_t smem = rows_smem<LOG_C>();
+  if (fwd) ntt_rows<LOG_C, LAZY, true><<<grid, T * ROWS, smem, st>>>(b);
+  else ntt_rows<LOG_C, LAZY, false><<<grid, T * ROWS, smem, st>>>(b);
   note_launch();
 }
 
+#define AOA_NTT_SIZES(X) X(5) X(6) X(7) X(8) X(9) X(10)
+
 template <bool LAZY>
-static void run_cols(const NttBatch& b, int nlimbs, int npolys, bool fwd, cudaStream_t st) {
+static void run_cols(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
   switch (b.log_r) {
-    case 5: launch_cols<5, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 6: launch_cols<6, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 7: launch_cols<7, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 8: launch_cols<8, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 9: launch_cols<9, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 10: launch_cols<10, LAZY>(b, nlimbs, npolys, fwd, st); break;
+#define AOA_CASE(s) \
+  case s: launch_cols<s, LAZY>(b, nlimbs, groups, fwd, st); break;
+    AOA_NTT_SIZES(AOA_CASE)
+#undef AOA_CASE
     default: throw AoaError(AOA_ERR_BAD_PARAM, "ntt: unsupported column size");
   }
 }
 
 template <bool LAZY>
-static void run_rows(const NttBatch& b, int nlimbs, int npolys, bool fwd, cudaStream_t st) {
+static void run_rows(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
   switch (b.log_c) {
-    case 5: launch_rows<5, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 6: launch_rows<6, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 7: launch_rows<7, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 8: launch_rows<8, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 9: launch_rows<9, LAZY>(b, nlimbs, npolys, fwd, st); break;
-    case 10: launch_rows<10, LAZY>(b, nlimbs, npolys, fwd, st); break;
+#define AOA_CASE(s) \
+  case s: launch_rows<s, LAZY>(b, nlimbs, groups, fwd, st); break;
+    AOA_NTT_SIZES(AOA_CASE)
+#undef AOA_CASE
     default: throw AoaError(AOA_ERR_BAD_PARAM, "ntt: unsupported row size");
   }
 }
 
+template <class K>
+static void allow_smem(K kernel, size_t bytes) {
+  AOA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// Once per engine: opt every transform kernel in to its dynamic shared memory.
+void ntt_init(Engine&) {
+#define AOA_ALLOW(s)                                                         \
+  allow_smem(ntt_cols<s, true, true>, cols_smem<s>());                       \
+  allow_smem(ntt_cols<s, true, false>, cols_smem<s>());                      \
+  allow_smem(ntt_cols<s, false, true>, cols_smem<s>());                      \
+  allow_smem(ntt_cols<s, false, false>, cols_smem<s>());                     \
+  allow_smem(ntt_rows<s, true, true>, rows_smem<s>());                       \
+  allow_smem(ntt_rows<s, true, false>, rows_smem<s>());                      \
+  allow_smem(ntt_rows<s, false, true>, rows_smem<s>());                      \
+  allow_smem(ntt_rows<s, false, false>, rows_smem<s>());
+  AOA_NTT_SIZES(AOA_ALLOW)
+#undef AOA_ALLOW
+}
+
 // Transform limbs [0, nlimbs) of npolys polys (layout [npolys][poly_stride][N]),
 // limb l under prime first_prime + l.  Work is split into chunks of whole polys
-// whose total size stays within the L2 budget, column and row pass per chunk.
+// whose total size stays within the L2 budget, column and row pass per chunk;
+// inside a pass each CTA streams up to polys_per_cta polys of one limb tile.
 void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
                long poly_stride, bool forward, cudaStream_t st) {
   if (npolys <= 0 || nlimbs <= 0) return;
   if (first_prime < 0 || first_prime + nlimbs > E.nprimes)
     throw AoaError(AOA_ERR_BAD_PARAM, "ntt: prime range out of bounds");
   NttBatch b;
-  b.tw = E.d_tw; b.itw = E.d_itw; b.pc = E.d_pc;
+  b.tw = E.d_tw; b.itw = E.d_itw; b.pc = E.d_pc; b.err = E.d_err;
   b.log_n = E.log_n; b.log_c = E.log_c; b.log_r = E.log_n - E.log_c;
   b.first_prime = first_prime; b.poly_stride = poly_stride;
   const long limb_bytes = (8L << E.log_n);
-  long chunk = std::max(1L, E.tune.ntt_chunk_bytes / (limb_bytes * nlimbs));
-  for (long p0 = 0; p0 < npolys; p0 += chunk) {
-    int np = (int)std::min<long>(chunk, npolys - p0);
-    b.data = data + p0 * poly_stride * (1L << E.log_n);
+  const long chunk = std::max(1L, E.tune.ntt_chunk_bytes / (limb_bytes * nlimbs));
+  // CTAs per pass ~ tiles * nlimbs * groups; keep a few waves of 148 SMs
+  const int tiles = 16;
+  for (long c0 = 0; c0 < npolys; c0 += chunk) {
+    const int np = (int)std::min<long>(chunk, npolys - c0);
+    int per = std::max(1, std::min(np, (int)((long)np * tiles * nlimbs / 1200)));
+    per = std::min(per, E.tune.ntt_polys_per_cta);
+    b.npolys = np;
+    b.polys_per_cta = per;
+    const int groups = (np + per - 1) / per;
+    b.data = data + c0 * poly_stride * (1L << E.log_n);
     if (E.lazy) {
-      if (forward) { run_cols<true>(b, nlimbs, np, true, st); run_rows<true>(b, nlimbs, np, true, st); }
-      else { run_rows<true>(b, nlimbs, np, false, st); run_cols<true>(b, nlimbs, np, false, st); }
+      if (forward) { run_cols<true>(b, nlimbs, groups, true, st); run_rows<true>(b, nlimbs, groups, true, st); }
+      else { run_rows<true>(b, nlimbs, groups, false, st); run_cols<true>(b, nlimbs, groups, false, st); }
     } else {
-      if (forward) { run_cols<false>(b, nlimbs, np, true, st); run_rows<false>(b, nlimbs, np, true, st); }
-      else { run_rows<false>(b, nlimbs, np, false, st); run_cols<false>(b, nlimbs, np, false, st); }
+      if (forward) { run_cols<false>(b, nlimbs, groups, true, st); run_rows<false>(b, nlimbs, groups, true, st); }
+      else { run_rows<false>(b, nlimbs, groups, false, st); run_cols<false>(b, nlimbs, groups, false, st); }
     }
   }
   AOA_CHECK_LAUNCH();
