@@ -42,7 +42,7 @@ struct ConvArgs {
   int post;
 };
 
-__global__ void __launch_bounds__(kConvThreads, 3)
+__global__ void __launch_bounds__(kConvThreads, 2)
 basis_convert(ConvArgs a, int out_first) {
   extern __shared__ uint64_t smat[];    // [nin][kConvOut]
   const int nout = min(kConvOut, a.nout - out_first);
