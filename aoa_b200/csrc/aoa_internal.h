@@ -36,7 +36,7 @@ constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration
 
 struct Tune {
   long ntt_chunk_bytes = 48L << 20;   // per NTT launch pair: stays inside L2
-  int ntt_polys_per_cta = 8;          // polys a transform CTA streams through its buffers
+  double ntt_waves = 1.0;             // transform CTAs per pass, in resident waves
 };
 
 // Device copy of the basis-conversion / rescale constants.
@@ -60,7 +60,7 @@ struct RnsTables {
 };
 
 struct Engine {
-  int device = 0;
+  int device = 0, num_sms = 148;
   int log_n = 0, log_c = 0;
   long N = 0;
   int k = 0, kl = 0, nprimes = 0;

@@ -99,12 +99,31 @@ struct Bf<true> {
   }
 };
 
+// ---- explicit shared-memory accessors --------------------------------------------
+// (ld.shared / st.shared: keeps every on-chip access on the short-latency path)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t lds64(uint32_t a) {
+  uint64_t v;
+  asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void sts64(uint32_t a, uint64_t v) {
+  asm volatile("st.shared.u64 [%0], %1;" ::"r"(a), "l"(v));
+}
+__device__ __forceinline__ ShoupW ldsw(uint32_t a) {
+  ShoupW w;
+  asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(w.w), "=l"(w.wp) : "r"(a));
+  return w;
+}
+
 // ---- forward (Cooley-Tukey, merged twist) ---------------------------------
-// twiddle index for local half-span 2^j and local group g: K * S/2^(j+1) + g
+// twiddle index for local half-span 2^j and local group g: K * S/2^(j+1) + g;
+// here K = 1 and the twiddles 0..S-1 of the prime sit in shared memory at tw.
 
 template <int LOG_S, bool LAZY>
-__device__ __forceinline__ void fwd_high(uint64_t (&v)[Sub<LOG_S>::E], const ShoupW* __restrict__ tw,
-                                         uint32_t K, uint64_t q) {
+__device__ __forceinline__ void fwd_high_s(uint64_t (&v)[Sub<LOG_S>::E], uint32_t tw, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
   for (int i = D::HI - 1; i >= 0; i--) {
@@ -112,16 +131,14 @@ __device__ __forceinline__ void fwd_high(uint64_t (&v)[Sub<LOG_S>::E], const Sho
 #pragma unroll
     for (int h = 0; h < D::E; h++) {
       if (h & span) continue;
-      const int g = h >> (i + 1);
-      const ShoupW w = tw[(K << (D::HI - 1 - i)) + g];
-        Bf<LAZY>::ct(v[h], v[h + span], w, q);
+      const ShoupW w = ldsw(tw + 16 * ((1 << (D::HI - 1 - i)) + (h >> (i + 1))));
+      Bf<LAZY>::ct(v[h], v[h + span], w, q);
     }
   }
 }
 
 template <int LOG_S, bool LAZY>
-__device__ __forceinline__ void fwd_low(uint64_t (&u)[Sub<LOG_S>::L], const ShoupW* __restrict__ tw,
-                                        uint32_t K, uint32_t hi, uint64_t q) {
+__device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t tw, uint32_t hi, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
   for (int i = D::LO - 1; i >= 0; i--) {
@@ -129,9 +146,8 @@ __device__ __forceinline__ void fwd_low(uint64_t (&u)[Sub<LOG_S>::L], const Shou
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      const int g = l >> (i + 1);
-      const ShoupW w = tw[(K << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + g];
-        Bf<LAZY>::ct(u[l], u[l + span], w, q);
+      const ShoupW w = ldsw(tw + 16 * ((1 << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + (l >> (i + 1))));
+      Bf<LAZY>::ct(u[l], u[l + span], w, q);
     }
   }
 }
@@ -139,8 +155,7 @@ __device__ __forceinline__ void fwd_low(uint64_t (&u)[Sub<LOG_S>::L], const Shou
 // ---- inverse (Gentleman-Sande) -------------------------------------------
 
 template <int LOG_S, bool LAZY>
-__device__ __forceinline__ void inv_low(uint64_t (&u)[Sub<LOG_S>::L], const ShoupW* __restrict__ itw,
-                                        uint32_t K, uint32_t hi, uint64_t q) {
+__device__ __forceinline__ void inv_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t itw, uint32_t hi, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
   for (int i = 0; i < D::LO; i++) {
@@ -148,17 +163,17 @@ __device__ __forceinline__ void inv_low(uint64_t (&u)[Sub<LOG_S>::L], const Shou
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      const int g = l >> (i + 1);
-      const ShoupW w = itw[(K << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + g];
-        Bf<LAZY>::gs(u[l], u[l + span], w, q);
+      const ShoupW w = ldsw(itw + 16 * ((1 << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + (l >> (i + 1))));
+      Bf<LAZY>::gs(u[l], u[l + span], w, q);
     }
   }
 }
 
-// LAST: this round holds the transform's final stage (half-span N/2): scale by N^-1.
-template <int LOG_S, bool LAZY, bool LAST>
-__device__ __forceinline__ void inv_high(uint64_t (&v)[Sub<LOG_S>::E], const ShoupW* __restrict__ itw,
-                                         uint32_t K, uint64_t q, ShoupW ninv, ShoupW ninv_w1) {
+// the column pass's high digit holds the transform's final stage (half-span
+// N/2): scale by N^-1 there
+template <int LOG_S, bool LAZY>
+__device__ __forceinline__ void inv_high_s(uint64_t (&v)[Sub<LOG_S>::E], uint32_t itw, uint64_t q, ShoupW ninv,
+                                           ShoupW ninv_w1) {
   using D = Sub<LOG_S>;
 #pragma unroll
   for (int i = 0; i < D::HI; i++) {
@@ -166,17 +181,19 @@ __device__ __forceinline__ void inv_high(uint64_t (&v)[Sub<LOG_S>::E], const Sho
 #pragma unroll
     for (int h = 0; h < D::E; h++) {
       if (h & span) continue;
-      const int g = h >> (i + 1);
-      const ShoupW w = itw[(K << (D::HI - 1 - i)) + g];
-        if (LAST && i == D::HI - 1) Bf<LAZY>::gs_last(v[h], v[h + span], ninv, ninv_w1, q);
-        else Bf<LAZY>::gs(v[h], v[h + span], w, q);
+      if (i == D::HI - 1) {
+        Bf<LAZY>::gs_last(v[h], v[h + span], ninv, ninv_w1, q);
+      } else {
+        const ShoupW w = ldsw(itw + 16 * ((1 << (D::HI - 1 - i)) + (h >> (i + 1))));
+        Bf<LAZY>::gs(v[h], v[h + span], w, q);
+      }
     }
   }
 }
 
-// ---- register-twiddle variants of the low-digit rounds ------------------------
-// Row kernels keep each thread's low-digit twiddles in registers for all the
-// polys a CTA processes: list order is stage-major (j = 2^(LO-1-i) - 1 + g).
+// ---- row-pass twiddles ---------------------------------------------------------
+// High digit: per row, at row_tw[2^(HI-1-i) - 1 + g] (shared memory).
+// Low digit: per thread in registers, list order j = 2^(LO-1-i) - 1 + g.
 
 template <int LOG_S>
 __device__ __forceinline__ void load_low_tw(ShoupW (&w)[Sub<LOG_S>::G][Sub<LOG_S>::L - 1],
@@ -187,8 +204,7 @@ __device__ __forceinline__ void load_low_tw(ShoupW (&w)[Sub<LOG_S>::G][Sub<LOG_S
     const uint32_t hi = t * D::G + gg;
 #pragma unroll
     for (int j = 0; j < D::L - 1; j++) {
-      // entry j belongs to the stage with 2^lvl twiddles (lvl = LO-1-i), group g
-      const int lvl = 31 - __clz(j + 1);
+      const int lvl = 31 - __clz(j + 1);       // entry j: stage with 2^lvl twiddles, group g
       const int g = j + 1 - (1 << lvl);
       w[gg][j] = tw[(K << (LOG_S - D::LO + lvl)) + (hi << lvl) + g];
     }
@@ -205,9 +221,7 @@ __device__ __forceinline__ void fwd_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      const int g = l >> (i + 1);
-      const ShoupW tw = w[(1 << (D::LO - 1 - i)) - 1 + g];
-        Bf<LAZY>::ct(u[l], u[l + span], tw, q);
+      Bf<LAZY>::ct(u[l], u[l + span], w[(1 << (D::LO - 1 - i)) - 1 + (l >> (i + 1))], q);
     }
   }
 }
@@ -222,9 +236,7 @@ __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      const int g = l >> (i + 1);
-      const ShoupW tw = w[(1 << (D::LO - 1 - i)) - 1 + g];
-        Bf<LAZY>::gs(u[l], u[l + span], tw, q);
+      Bf<LAZY>::gs(u[l], u[l + span], w[(1 << (D::LO - 1 - i)) - 1 + (l >> (i + 1))], q);
     }
   }
 }
@@ -232,8 +244,6 @@ __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
 // ---- asynchronous bulk copies (TMA engine) and mbarriers --------------------------
 
 constexpr int kSpinLimit = 1 << 20;     // bounded mbarrier waits
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count) : "memory");
@@ -249,10 +259,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, unsigned bytes) {
 }
 
 // global -> shared bulk copy; bytes % 16 == 0, both addresses 16-byte aligned
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mb) {
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, unsigned bytes, uint64_t* mb) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
       "l"(src), "r"(bytes), "r"(smem_u32(mb))
       : "memory");
 }
@@ -277,10 +286,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // ---- kernels ---------------------------------------------------------------
-// Batch addressing: limb (poly p, limb l) lives at data + (p*poly_stride + l)*N
-// and uses prime first_prime + l.  grid = (tiles per limb, nlimbs, poly groups);
-// a CTA transforms the same tile of the same limb for polys_per_cta polys,
-// streaming them through two shared-memory buffers filled by bulk copies.
+// Work items: limb l of poly p (item j = l * npolys + p) lives at
+// data + (p * poly_stride + l) * N under prime first_prime + l.  grid =
+// (tiles per limb, G): CTA (x, y) handles tile x of items y, y + G, ... and
+// streams them through two shared-memory buffers filled by bulk copies, so the
+// next item's tile arrives while the current one is transformed.  Twiddles are
+// reloaded only when the limb changes.
 
 struct NttBatch {
   uint64_t* data;
@@ -291,10 +302,9 @@ struct NttBatch {
   int log_n, log_r, log_c; // N = R * C
   int first_prime;
   long poly_stride;        // limbs between consecutive polys
-  int npolys, polys_per_cta;
+  int npolys, nitems;      // nitems = nlimbs * npolys
 };
 
-// Shared-memory budget of the kernels below (dynamic part).
 template <int LOG_S>
 constexpr int tile_words() { return Sub<LOG_S>::PER_CTA * Sub<LOG_S>::S; }
 
@@ -306,8 +316,8 @@ constexpr size_t rows_smem() {
   return 2 * tile_words<LOG_C>() * 8 + (size_t)Sub<LOG_C>::PER_CTA * (Sub<LOG_C>::E - 1) * sizeof(ShoupW);
 }
 
-// Column pass.  Tile = S rows x W columns of one limb; the load is S bulk copies
-// of W*8 bytes (one per row) issued by warp 0.
+// Column pass.  Tile = S rows x W columns of one limb; its load is S bulk copies
+// of W*8 bytes (one per row) issued by warp 0.  Shared layout [S][W].
 template <int LOG_R, bool LAZY, bool FWD>
 __global__ void __launch_bounds__(Sub<LOG_R>::T * Sub<LOG_R>::PER_CTA, 3)
 ntt_cols(NttBatch b) {
@@ -316,62 +326,67 @@ ntt_cols(NttBatch b) {
   constexpr int TILE = D::S * W;
   extern __shared__ __align__(128) uint64_t dyn[];
   __shared__ __align__(8) uint64_t mbar[2];
-  uint64_t* bufs = dyn;                                   // [2][S][W]
-  ShoupW* tws = (ShoupW*)(dyn + 2 * TILE);                 // [S]: twiddles 0..S-1 (K = 1)
+  const uint32_t sbuf = smem_u32(dyn);                          // [2][S][W] words
+  const uint32_t stw = smem_u32(dyn + 2 * TILE);                // [S] ShoupW
+  ShoupW* tws = (ShoupW*)(dyn + 2 * TILE);
   const int w = threadIdx.x % W, t = threadIdx.x / W;
-  const int limb = blockIdx.y, prime = b.first_prime + limb;
   const long N = 1L << b.log_n, C = 1L << b.log_c;
-  const PrimeConst& P = b.pc[prime];
-  const uint64_t q = P.q;
-  const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
-  const int p0 = blockIdx.z * b.polys_per_cta;
-  const int p1 = min(b.npolys, p0 + b.polys_per_cta);
-  for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[e] = tw[e];
+  const int G = gridDim.y;
   if (threadIdx.x == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     mbar_init_fence();
   }
   __syncthreads();
-  auto tile_src = [&](int p) -> uint64_t* {
+  auto src_of = [&](int j) -> const uint64_t* {
+    const int limb = j / b.npolys, p = j % b.npolys;
     return b.data + ((long)p * b.poly_stride + limb) * N + (long)blockIdx.x * W;
   };
-  auto issue = [&](int p, int bi) {        // warp 0: S row segments of W words
+  auto issue = [&](int j, int bi) {        // warp 0: S row segments of W words
     if (threadIdx.x < 32) {
       if (threadIdx.x == 0) mbar_expect_tx(&mbar[bi], TILE * 8);
       __syncwarp();
-      const uint64_t* src = tile_src(p);
+      const uint64_t* src = src_of(j);
       for (int r = threadIdx.x; r < D::S; r += 32)
-        bulk_g2s(bufs + bi * TILE + r * W, src + r * C, W * 8, &mbar[bi]);
+        bulk_g2s(sbuf + (bi * TILE + r * W) * 8, src + r * C, W * 8, &mbar[bi]);
     }
   };
-  if (p0 < p1) issue(p0, 0);
-  for (int p = p0; p < p1; p++) {
-    const int it = p - p0, bi = it & 1;
-    if (p + 1 < p1) issue(p + 1, bi ^ 1);
+  int cur_limb = -1;
+  if ((int)blockIdx.y < b.nitems) issue(blockIdx.y, 0);
+  for (int j = blockIdx.y, it = 0; j < b.nitems; j += G, it++) {
+    const int bi = it & 1;
+    const int limb = j / b.npolys, prime = b.first_prime + limb;
+    if (j + G < b.nitems) issue(j + G, bi ^ 1);
+    if (limb != cur_limb) {                // previous users of tws passed the barrier below
+      const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
+      for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[e] = tw[e];
+      cur_limb = limb;
+    }
     const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
-      if (p + 1 < p1) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);   // drain the copy in flight
+      if (j + G < b.nitems) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);   // drain the copy in flight
       return;
     }
-    uint64_t(*sm)[W] = (uint64_t(*)[W])(bufs + bi * TILE);
-    uint64_t* x = tile_src(p) + w;
+    const PrimeConst& P = b.pc[prime];
+    const uint64_t q = P.q;
+    const uint32_t sm = sbuf + bi * TILE * 8 + w * 8;            // + row * W * 8
+    uint64_t* x = const_cast<uint64_t*>(src_of(j)) + w;
     if (FWD) {
       uint64_t v[D::E];
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = sm[(h << D::LO) + t][w];
-      fwd_high<LOG_R, LAZY>(v, tws, 1, q);
+      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + ((h << D::LO) + t) * W * 8);
+      fwd_high_s<LOG_R, LAZY>(v, stw, q);
 #pragma unroll
-      for (int h = 0; h < D::E; h++) sm[(h << D::LO) + t][w] = v[h];
+      for (int h = 0; h < D::E; h++) sts64(sm + ((h << D::LO) + t) * W * 8, v[h]);
       __syncthreads();
 #pragma unroll
       for (int g = 0; g < D::G; g++) {
         const int hi = t * D::G + g;
         uint64_t u[D::L];
 #pragma unroll
-        for (int l = 0; l < D::L; l++) u[l] = sm[(hi << D::LO) + l][w];
-        fwd_low<LOG_R, LAZY>(u, tws, 1, hi, q);
+        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + ((hi << D::LO) + l) * W * 8);
+        fwd_low_s<LOG_R, LAZY>(u, stw, hi, q);
 #pragma unroll
         for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
       }
@@ -382,16 +397,16 @@ ntt_cols(NttBatch b) {
         const int hi = t * D::G + g;
         uint64_t u[D::L];
 #pragma unroll
-        for (int l = 0; l < D::L; l++) u[l] = sm[(hi << D::LO) + l][w];
-        inv_low<LOG_R, LAZY>(u, tws, 1, hi, q);
+        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + ((hi << D::LO) + l) * W * 8);
+        inv_low_s<LOG_R, LAZY>(u, stw, hi, q);
 #pragma unroll
-        for (int l = 0; l < D::L; l++) sm[(hi << D::LO) + l][w] = u[l];
+        for (int l = 0; l < D::L; l++) sts64(sm + ((hi << D::LO) + l) * W * 8, u[l]);
       }
       __syncthreads();
       uint64_t v[D::E];
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = sm[(h << D::LO) + t][w];
-      inv_high<LOG_R, LAZY, true>(v, tws, 1, q, ninv, ninv_w1);
+      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + ((h << D::LO) + t) * W * 8);
+      inv_high_s<LOG_R, LAZY>(v, stw, q, ninv, ninv_w1);
 #pragma unroll
       for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];
     }
@@ -402,7 +417,7 @@ ntt_cols(NttBatch b) {
   }
 }
 
-// swizzled position inside one row of shared memory
+// swizzled word offset inside one row of shared memory
 template <int LOG_S>
 __device__ __forceinline__ int swz(int hi, int lo) {
   return (hi << Sub<LOG_S>::LO) + (lo ^ (hi & (Sub<LOG_S>::L - 1)));
@@ -418,113 +433,115 @@ ntt_rows(NttBatch b) {
   constexpr int NT1 = D::E - 1;                           // high-digit twiddles per row
   extern __shared__ __align__(128) uint64_t dyn[];
   __shared__ __align__(8) uint64_t mbar[2];
-  uint64_t* bufs = dyn;                                   // [2][ROWS][S]
+  const uint32_t sbuf = smem_u32(dyn);                    // [2][ROWS][S] words
   ShoupW* tw1 = (ShoupW*)(dyn + 2 * TILE);                 // [ROWS][NT1]
   const int t = threadIdx.x % D::T, rho = threadIdx.x / D::T;
-  const int limb = blockIdx.y, prime = b.first_prime + limb;
   const long N = 1L << b.log_n;
+  const int G = gridDim.y;
   const uint32_t row0 = blockIdx.x * ROWS;
   const uint32_t Kbase = (1u << b.log_r) + row0;
-  const uint64_t q = b.pc[prime].q;
-  const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
-  const int p0 = blockIdx.z * b.polys_per_cta;
-  const int p1 = min(b.npolys, p0 + b.polys_per_cta);
-  for (int e = threadIdx.x; e < ROWS * NT1; e += blockDim.x) {
-    const int r = e / NT1, j = e % NT1;
-    const int lvl = 31 - __clz(j + 1);                    // stage level: 2^lvl twiddles
-    const int g = j + 1 - (1 << lvl);
-    tw1[e] = tw[((Kbase + r) << lvl) + g];
-  }
-  ShoupW w2[D::G][D::L - 1];
-  load_low_tw<LOG_C>(w2, tw, Kbase + rho, t);
+  const uint32_t st1 = smem_u32(tw1 + rho * NT1);
   if (threadIdx.x == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     mbar_init_fence();
   }
   __syncthreads();
-  auto tile_src = [&](int p) -> uint64_t* {
+  auto src_of = [&](int j) -> uint64_t* {
+    const int limb = j / b.npolys, p = j % b.npolys;
     return b.data + ((long)p * b.poly_stride + limb) * N + ((long)row0 << LOG_C);
   };
-  auto issue = [&](int p, int bi) {
+  auto issue = [&](int j, int bi) {
     mbar_expect_tx(&mbar[bi], TILE * 8);
-    bulk_g2s(bufs + bi * TILE, tile_src(p), TILE * 8, &mbar[bi]);
+    bulk_g2s(sbuf + bi * TILE * 8, src_of(j), TILE * 8, &mbar[bi]);
   };
-  if (threadIdx.x == 0 && p0 < p1) issue(p0, 0);
-  const ShoupW* t1 = tw1 + rho * NT1;
-  for (int p = p0; p < p1; p++) {
-    const int it = p - p0, bi = it & 1;
-    if (threadIdx.x == 0 && p + 1 < p1) issue(p + 1, bi ^ 1);
+  ShoupW w2[D::G][D::L - 1];
+  int cur_limb = -1;
+  uint64_t q = 0;
+  if (threadIdx.x == 0 && (int)blockIdx.y < b.nitems) issue(blockIdx.y, 0);
+  for (int j = blockIdx.y, it = 0; j < b.nitems; j += G, it++) {
+    const int bi = it & 1;
+    const int limb = j / b.npolys;
+    if (threadIdx.x == 0 && j + G < b.nitems) issue(j + G, bi ^ 1);
+    if (limb != cur_limb) {
+      const int prime = b.first_prime + limb;
+      const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
+      for (int e = threadIdx.x; e < ROWS * NT1; e += blockDim.x) {
+        const int r = e / NT1, jj = e % NT1;
+        const int lvl = 31 - __clz(jj + 1);
+        tw1[e] = tw[((Kbase + r) << lvl) + jj + 1 - (1 << lvl)];
+      }
+      load_low_tw<LOG_C>(w2, tw, Kbase + rho, t);
+      q = b.pc[prime].q;
+      cur_limb = limb;
+    }
     const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
-      if (p + 1 < p1) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);
+      if (j + G < b.nitems) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);
       return;
     }
-    uint64_t* s = bufs + bi * TILE + rho * D::S;
-    uint64_t* x = tile_src(p) + rho * D::S;
+    const uint32_t s = sbuf + (bi * TILE + rho * D::S) * 8;
+    uint64_t* x = src_of(j) + rho * D::S;
     uint64_t v[D::E];
     if (FWD) {
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = s[(h << D::LO) + t];
-      // high-digit stages: twiddle (K << (HI-1-i)) + g sits at t1[2^(HI-1-i) - 1 + g]
+      for (int h = 0; h < D::E; h++) v[h] = lds64(s + ((h << D::LO) + t) * 8);
 #pragma unroll
       for (int i = D::HI - 1; i >= 0; i--) {
         const int span = 1 << i;
 #pragma unroll
         for (int h = 0; h < D::E; h++) {
           if (h & span) continue;
-          const int g = h >> (i + 1);
-          const ShoupW wv = t1[(1 << (D::HI - 1 - i)) - 1 + g];
-            Bf<LAZY>::ct(v[h], v[h + span], wv, q);
+          const ShoupW wv = ldsw(st1 + 16 * ((1 << (D::HI - 1 - i)) - 1 + (h >> (i + 1))));
+          Bf<LAZY>::ct(v[h], v[h + span], wv, q);
         }
       }
       __syncwarp();
 #pragma unroll
-      for (int h = 0; h < D::E; h++) s[swz<LOG_C>(h, t)] = v[h];
+      for (int h = 0; h < D::E; h++) sts64(s + swz<LOG_C>(h, t) * 8, v[h]);
       __syncwarp();
 #pragma unroll
       for (int gg = 0; gg < D::G; gg++) {
         const int hi = t * D::G + gg;
         uint64_t u[D::L];
 #pragma unroll
-        for (int l = 0; l < D::L; l++) u[l] = s[swz<LOG_C>(hi, l)];
+        for (int l = 0; l < D::L; l++) u[l] = lds64(s + swz<LOG_C>(hi, l) * 8);
         fwd_low_r<LOG_C, LAZY>(u, w2[gg], q);
 #pragma unroll
-        for (int l = 0; l < D::L; l++) s[swz<LOG_C>(hi, l)] = u[l];
+        for (int l = 0; l < D::L; l++) sts64(s + swz<LOG_C>(hi, l) * 8, u[l]);
       }
       __syncwarp();
 #pragma unroll
-      for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = Bf<LAZY>::fwd_out(s[swz<LOG_C>(h, t)], q);
+      for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = Bf<LAZY>::fwd_out(lds64(s + swz<LOG_C>(h, t) * 8), q);
     } else {
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = s[(h << D::LO) + t];
+      for (int h = 0; h < D::E; h++) v[h] = lds64(s + ((h << D::LO) + t) * 8);
       __syncwarp();
 #pragma unroll
-      for (int h = 0; h < D::E; h++) s[swz<LOG_C>(h, t)] = v[h];
+      for (int h = 0; h < D::E; h++) sts64(s + swz<LOG_C>(h, t) * 8, v[h]);
       __syncwarp();
 #pragma unroll
       for (int gg = 0; gg < D::G; gg++) {
         const int hi = t * D::G + gg;
         uint64_t u[D::L];
 #pragma unroll
-        for (int l = 0; l < D::L; l++) u[l] = s[swz<LOG_C>(hi, l)];
+        for (int l = 0; l < D::L; l++) u[l] = lds64(s + swz<LOG_C>(hi, l) * 8);
         inv_low_r<LOG_C, LAZY>(u, w2[gg], q);
 #pragma unroll
-        for (int l = 0; l < D::L; l++) s[swz<LOG_C>(hi, l)] = u[l];
+        for (int l = 0; l < D::L; l++) sts64(s + swz<LOG_C>(hi, l) * 8, u[l]);
       }
       __syncwarp();
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = s[swz<LOG_C>(h, t)];
+      for (int h = 0; h < D::E; h++) v[h] = lds64(s + swz<LOG_C>(h, t) * 8);
 #pragma unroll
       for (int i = 0; i < D::HI; i++) {
         const int span = 1 << i;
 #pragma unroll
         for (int h = 0; h < D::E; h++) {
           if (h & span) continue;
-          const int g = h >> (i + 1);
-          const ShoupW wv = t1[(1 << (D::HI - 1 - i)) - 1 + g];
-            Bf<LAZY>::gs(v[h], v[h + span], wv, q);
+          const ShoupW wv = ldsw(st1 + 16 * ((1 << (D::HI - 1 - i)) - 1 + (h >> (i + 1))));
+          Bf<LAZY>::gs(v[h], v[h + span], wv, q);
         }
       }
 #pragma unroll
@@ -538,12 +555,12 @@ ntt_rows(NttBatch b) {
 // ---- host launchers ----------------------------------------------------------
 
 template <int LOG_R, bool LAZY>
-static void launch_cols(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
+static void launch_cols(const NttBatch& b, int ctas_per_tile, bool fwd, cudaStream_t st) {
   constexpr int T = Sub<LOG_R>::T;
   constexpr int W = Sub<LOG_R>::PER_CTA;
   const int C = 1 << b.log_c;
   if (C % W) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: column tile does not divide C");
-  dim3 grid(C / W, nlimbs, groups);
+  dim3 grid(C / W, ctas_per_tile);
   constexpr size_t smem = cols_smem<LOG_R>();
   if (fwd) ntt_cols<LOG_R, LAZY, true><<<grid, T * W, smem, st>>>(b);
   else ntt_cols<LOG_R, LAZY, false><<<grid, T * W, smem, st>>>(b);
@@ -551,12 +568,12 @@ static void launch_cols(const NttBatch& b, int nlimbs, int groups, bool fwd, cud
 }
 
 template <int LOG_C, bool LAZY>
-static void launch_rows(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
+static void launch_rows(const NttBatch& b, int ctas_per_tile, bool fwd, cudaStream_t st) {
   constexpr int T = Sub<LOG_C>::T;
   constexpr int ROWS = Sub<LOG_C>::PER_CTA;
   const int R = 1 << b.log_r;
   if (R % ROWS) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: row tile does not divide R");
-  dim3 grid(R / ROWS, nlimbs, groups);
+  dim3 grid(R / ROWS, ctas_per_tile);
   constexpr size_t smem = rows_smem<LOG_C>();
   if (fwd) ntt_rows<LOG_C, LAZY, true><<<grid, T * ROWS, smem, st>>>(b);
   else ntt_rows<LOG_C, LAZY, false><<<grid, T * ROWS, smem, st>>>(b);
@@ -565,22 +582,34 @@ static void launch_rows(const NttBatch& b, int nlimbs, int groups, bool fwd, cud
 
 #define AOA_NTT_SIZES(X) X(5) X(6) X(7) X(8) X(9) X(10)
 
+// CTAs per tile column: about one resident wave of CTAs (blocks_per_sm per SM)
+static int ctas_per_tile(const Engine& E, int tiles, int items, int blocks_per_sm) {
+  const int target = std::max(1, (int)(E.tune.ntt_waves * E.num_sms * blocks_per_sm) / std::max(1, tiles));
+  return std::max(1, std::min(items, target));
+}
+
 template <bool LAZY>
-static void run_cols(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
+static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+  const int tiles = (1 << b.log_c) / (1 << 4);
   switch (b.log_r) {
-#define AOA_CASE(s) \
-  case s: launch_cols<s, LAZY>(b, nlimbs, groups, fwd, st); break;
+#define AOA_CASE(s)                                                                                     \
+  case s:                                                                                               \
+    launch_cols<s, LAZY>(b, ctas_per_tile(E, (1 << b.log_c) / Sub<s>::PER_CTA, b.nitems, 3), fwd, st); \
+    break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
     default: throw AoaError(AOA_ERR_BAD_PARAM, "ntt: unsupported column size");
   }
+  (void)tiles;
 }
 
 template <bool LAZY>
-static void run_rows(const NttBatch& b, int nlimbs, int groups, bool fwd, cudaStream_t st) {
+static void run_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
   switch (b.log_c) {
-#define AOA_CASE(s) \
-  case s: launch_rows<s, LAZY>(b, nlimbs, groups, fwd, st); break;
+#define AOA_CASE(s)                                                                                     \
+  case s:                                                                                               \
+    launch_rows<s, LAZY>(b, ctas_per_tile(E, (1 << b.log_r) / Sub<s>::PER_CTA, b.nitems, 2), fwd, st); \
+    break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
     default: throw AoaError(AOA_ERR_BAD_PARAM, "ntt: unsupported row size");
@@ -593,7 +622,7 @@ static void allow_smem(K kernel, size_t bytes) {
 }
 
 // Once per engine: opt every transform kernel in to its dynamic shared memory.
-void ntt_init(Engine&) {
+void ntt_init(Engine& E) {
 #define AOA_ALLOW(s)                                                         \
   allow_smem(ntt_cols<s, true, true>, cols_smem<s>());                       \
   allow_smem(ntt_cols<s, true, false>, cols_smem<s>());                      \
@@ -605,12 +634,14 @@ void ntt_init(Engine&) {
   allow_smem(ntt_rows<s, false, false>, rows_smem<s>());
   AOA_NTT_SIZES(AOA_ALLOW)
 #undef AOA_ALLOW
+  int sms = 0;
+  AOA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E.device));
+  E.num_sms = sms;
 }
 
 // Transform limbs [0, nlimbs) of npolys polys (layout [npolys][poly_stride][N]),
 // limb l under prime first_prime + l.  Work is split into chunks of whole polys
-// whose total size stays within the L2 budget, column and row pass per chunk;
-// inside a pass each CTA streams up to polys_per_cta polys of one limb tile.
+// whose total size stays within the L2 budget, column and row pass per chunk.
 void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
                long poly_stride, bool forward, cudaStream_t st) {
   if (npolys <= 0 || nlimbs <= 0) return;
@@ -622,22 +653,17 @@ void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
   b.first_prime = first_prime; b.poly_stride = poly_stride;
   const long limb_bytes = (8L << E.log_n);
   const long chunk = std::max(1L, E.tune.ntt_chunk_bytes / (limb_bytes * nlimbs));
-  // CTAs per pass ~ tiles * nlimbs * groups; keep a few waves of 148 SMs
-  const int tiles = 16;
   for (long c0 = 0; c0 < npolys; c0 += chunk) {
     const int np = (int)std::min<long>(chunk, npolys - c0);
-    int per = std::max(1, std::min(np, (int)((long)np * tiles * nlimbs / 1200)));
-    per = std::min(per, E.tune.ntt_polys_per_cta);
     b.npolys = np;
-    b.polys_per_cta = per;
-    const int groups = (np + per - 1) / per;
+    b.nitems = np * nlimbs;
     b.data = data + c0 * poly_stride * (1L << E.log_n);
     if (E.lazy) {
-      if (forward) { run_cols<true>(b, nlimbs, groups, true, st); run_rows<true>(b, nlimbs, groups, true, st); }
-      else { run_rows<true>(b, nlimbs, groups, false, st); run_cols<true>(b, nlimbs, groups, false, st); }
+      if (forward) { run_cols<true>(E, b, true, st); run_rows<true>(E, b, true, st); }
+      else { run_rows<true>(E, b, false, st); run_cols<true>(E, b, false, st); }
     } else {
-      if (forward) { run_cols<false>(b, nlimbs, groups, true, st); run_rows<false>(b, nlimbs, groups, true, st); }
-      else { run_rows<false>(b, nlimbs, groups, false, st); run_cols<false>(b, nlimbs, groups, false, st); }
+      if (forward) { run_cols<false>(E, b, true, st); run_rows<false>(E, b, true, st); }
+      else { run_rows<false>(E, b, false, st); run_cols<false>(E, b, false, st); }
     }
   }
   AOA_CHECK_LAUNCH();
