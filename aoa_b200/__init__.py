@@ -292,3 +292,8 @@ class PinnedArray:
 def kernel_launches():
     """Kernels launched by libaoa_b200.so so far in this process."""
     return int(capi.load().aoa_kernel_launches())
+
+
+def ckks_mul_plain(ctx, c3, c1, c2, evk):
+    """The reference's per-call ckks_mul sequence on this engine (comparison path)."""
+    capi.check(capi.load().aoa_hmult_plain(ctx.handle, c3.handle, c1.handle, c2.handle, _h(evk)))

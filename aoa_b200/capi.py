@@ -77,6 +77,7 @@ SIGNATURES = {
     "aoa_swk_destroy": (c_int, [c_void_p, c_void_p]),
     "aoa_hmult": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_hmult_relin_rescale": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_hmult_plain": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_rescale": (c_int, [c_void_p, c_void_p]),
     "aoa_add": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_sub": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -30,27 +30,33 @@ struct aoa_swk {
 
 namespace aoa {
 
-// Workspace for one key switch / HMult at the engine's largest level:
+// Workspace for one key switch / HMult at the engine's largest level (words):
 //   D   [3][k]       tensor outputs d0 d1 d2 (transform domain)
 //   T   [k]          coefficient-domain copy of the key-switch input
 //   UB  [kl]         ModUp output (B limbs)
-//   KS  [2][k + kl]  key products, then their inverse transforms
-//   R0  [k]          rotated c0
+//   KS  [2][k + kl]  key products: Q limbs transform domain, B limbs coefficients
+//   L4  [4]          single limbs (d0_l, d1_l, k0_l, k1_l) for the merged rescale
+//   CL  [2]          c_l, limb l of the product in coefficients
+//   Y   [2][k]       ModDown corrections
+//   R0  [k]          automorphism of c0
 struct Workspace {
-  uint64_t *D, *T, *UB, *KS, *R0;
+  uint64_t *D, *T, *UB, *KS, *L4, *CL, *Y, *R0;
 };
 
 size_t workspace_words(const Engine& E) {
-  return (size_t)E.N * (3 * E.k + E.k + std::max(E.kl, 1) + 2 * (E.k + E.kl) + E.k);
+  return (size_t)E.N * (3 * E.k + E.k + std::max(E.kl, 1) + 2 * (E.k + E.kl) + 4 + 2 + 2 * E.k + E.k);
 }
 
-static Workspace carve(const Engine& E, uint64_t* p) {
+Workspace carve(const Engine& E, uint64_t* p) {
   const size_t limb = (size_t)E.N;
   Workspace w;
   w.D = p; p += 3 * E.k * limb;
   w.T = p; p += E.k * limb;
   w.UB = p; p += std::max(E.kl, 1) * limb;
   w.KS = p; p += 2 * (E.k + E.kl) * limb;
+  w.L4 = p; p += 4 * limb;
+  w.CL = p; p += 2 * limb;
+  w.Y = p; p += 2 * E.k * limb;
   w.R0 = p;
   return w;
 }
@@ -78,37 +84,23 @@ static void to_domain(Ctx& C, aoa_ct* ct, int domain, int nlimbs) {
   ct->domain = domain;
 }
 
-// Key switch of the coefficient-domain Q limbs 0..level at `x_coef`, whose
-// transform-domain image is `x_ntt` (may be null: computed here).  Writes the
-// two coefficient-domain results to out0 / out1 (limbs 0..level).
-static void keyswitch(Ctx& C, const Workspace& w, const uint64_t* x_coef, const uint64_t* x_ntt, const aoa_swk* key,
-                      int level, uint64_t* out0, uint64_t* out1, long out_stride) {
+static void copy_limbs(Ctx& C, uint64_t* dst, const uint64_t* src, long words) {
+  AOA_CUDA(cudaMemcpyAsync(dst, src, (size_t)words * 8, cudaMemcpyDeviceToDevice, C.stream));
+}
+
+// Key-switch core on the Q limbs 0..level of x, given in both domains
+// (x_coef, x_ntt).  Leaves in w.KS = [x*b | x*a] (stride k + kl limbs): the Q
+// limbs in the transform domain, the kl B limbs back in coefficients.
+// (ModUp poly_modup, key products poly_mul, ckks.cpp:309-314.)
+static void keyswitch_core(Ctx& C, const Workspace& w, const uint64_t* x_coef, const uint64_t* x_ntt,
+                           const aoa_swk* key, int level) {
   const Engine& E = *C.E;
   const long N = E.N;
   const int m = level + 1;
-  const long ks_stride = (long)(E.k + E.kl) * N;
-  // ModUp of the coefficient-domain input, then its B limbs to the transform domain
   modup(E, x_coef, 0, w.UB, 0, 1, level, C.stream);
   ntt_batch(E, w.UB, 1, E.k, E.kl, E.kl, true, C.stream);
-  if (!x_ntt) {
-    AOA_CUDA(cudaMemcpyAsync(w.KS, x_coef, (size_t)m * N * 8, cudaMemcpyDeviceToDevice, C.stream));
-    ntt_batch(E, w.KS, 1, 0, m, m, true, C.stream);
-    x_ntt = w.KS;
-  }
-  // products with the key over Q limbs 0..level and all B limbs:
-  // KS[0] = x * b, KS[1] = x * a, layout [2][m Q limbs | kl B limbs] (stride k + kl)
-  // (x_ntt may alias KS[0]'s Q limbs: keyswitch_mul reads x before writing k0)
-  keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + ks_stride, m, C.stream);
-  // back to coefficients: Q limbs under primes 0..level, B limbs under k..k+kl-1
-  ntt_batch(E, w.KS, 2, 0, m, E.k + E.kl, false, C.stream);
+  keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + (long)(E.k + E.kl) * N, m, C.stream);
   ntt_batch(E, w.KS + (long)m * N, 2, E.k, E.kl, E.k + E.kl, false, C.stream);
-  // ModDown both products
-  if (out1 == out0 + out_stride) {
-    moddown(E, w.KS, w.KS + (long)m * N, ks_stride, out0, out_stride, 2, level, C.stream);
-  } else {
-    moddown(E, w.KS, w.KS + (long)m * N, ks_stride, out0, 0, 1, level, C.stream);
-    moddown(E, w.KS + ks_stride, w.KS + ks_stride + (long)m * N, 0, out1, 0, 1, level, C.stream);
-  }
 }
 
 static uint64_t scale_after_mult(const Engine& E, uint64_t sa, uint64_t sb, int level) {
@@ -116,8 +108,60 @@ static uint64_t scale_after_mult(const Engine& E, uint64_t sa, uint64_t sb, int 
   return (uint64_t)(p / E.primes[level]);
 }
 
+// Finishes a key switch whose products sit in w.KS and writes the transform
+// domain result to out (2 polys of stride `half`):
+//   rescale:  out = Rescale(base + ModDown(KS))   (limbs 0..level-1)
+//   else:     out = base + ModDown(KS)            (limbs 0..level)
+// base = [b0 | b1] (stride `half`, transform domain) or b1 == nullptr (zero).
+static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long half, const uint64_t* b0,
+                             const uint64_t* b1, int level, bool do_rescale) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  const int m = level + 1;
+  const long ks_stride = (long)(E.k + E.kl) * N;
+  const uint64_t* kb = w.KS + (long)m * N;
+  if (do_rescale) {
+    // limb l of both products and of the base, in coefficients
+    int nl = 2;
+    copy_limbs(C, w.L4 + 2 * N, w.KS + (long)level * N, N);
+    copy_limbs(C, w.L4 + 3 * N, w.KS + ks_stride + (long)level * N, N);
+    if (b0) {
+      copy_limbs(C, w.L4, b0 + (long)level * N, N);
+      if (b1) copy_limbs(C, w.L4 + N, b1 + (long)level * N, N);
+      else AOA_CUDA(cudaMemsetAsync(w.L4 + N, 0, N * 8, C.stream));
+      nl = 4;
+    } else {
+      AOA_CUDA(cudaMemsetAsync(w.L4, 0, 2 * N * 8, C.stream));
+    }
+    ntt_batch(E, w.L4 + (4 - nl) * N, nl, level, 1, 1, false, C.stream);
+    rescale_top(E, kb, ks_stride, w.L4 + 2 * N, N, w.L4, N, w.CL, N, 2, level, C.stream);
+    rescale_y(E, kb, ks_stride, w.CL, N, w.Y, (long)E.k * N, 2, level, C.stream);
+    ntt_batch(E, w.Y, 2, 0, level, E.k, true, C.stream);
+    if (b0 && b1 == b0 + half) {
+      ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, level, 2, level, C.stream);
+    } else {
+      ks_combine(E, out, 0, b0, 0, w.KS, 0, w.Y, 0, level, 1, level, C.stream);
+      ks_combine(E, out + half, 0, b1, 0, w.KS + ks_stride, 0, w.Y + (long)E.k * N, 0, level, 1, level, C.stream);
+    }
+  } else {
+    moddown_conv(E, kb, ks_stride, w.Y, (long)E.k * N, 2, m, C.stream);
+    ntt_batch(E, w.Y, 2, 0, m, E.k, true, C.stream);
+    if (b0 && b1 == b0 + half) {
+      ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, m, 2, 0, C.stream);
+    } else {
+      ks_combine(E, out, 0, b0, 0, w.KS, 0, w.Y, 0, m, 1, 0, C.stream);
+      ks_combine(E, out + half, 0, b1, 0, w.KS + ks_stride, 0, w.Y + (long)E.k * N, 0, m, 1, 0, C.stream);
+    }
+  }
+}
+
 // HMult + relinearisation (ckks_mul_without_rescale, ckks.cpp:273-332),
 // optionally followed by the rescale of ckks_mul (ckks.cpp:334-347).
+// Transform-domain pipeline: tensor, one inverse transform of d2 for ModUp,
+// the key products, inverse transforms of their B limbs only, and ModDown
+// merged with the rescale (one forward transform per output limb).  The
+// result is left in the transform domain (the reference leaves coefficients;
+// the residues of every live limb are the same after a domain change).
 void hmult(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool do_rescale) {
   const Engine& E = *C.E;
   const long N = E.N;
@@ -131,33 +175,27 @@ void hmult(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool d
   const long half = (long)E.k * N;
   Workspace w = get_ws(C);
   // operands to the transform domain, in place (poly_mul does the same, poly_t.cpp:201-220)
-  to_domain(C, a, AOA_NTT, std::max(a->level, level) + 1);
-  if (b != a) to_domain(C, b, AOA_NTT, std::max(b->level, level) + 1);
+  to_domain(C, a, AOA_NTT, a->level + 1);
+  if (b != a) to_domain(C, b, AOA_NTT, b->level + 1);
   uint64_t* D0 = w.D;
-  uint64_t* D1 = w.D + half;
   uint64_t* D2 = w.D + 2 * half;
-  tensor_op(E, a->d, half, b->d, half, D0, D1, D2, m, C.stream);
-  // coefficient-domain d2 for ModUp
-  AOA_CUDA(cudaMemcpyAsync(w.T, D2, (size_t)m * N * 8, cudaMemcpyDeviceToDevice, C.stream));
-  ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  tensor_op(E, a->d, half, b->d, half, D0, D0 + half, D2, m, C.stream);
   const uint64_t sa = a->scale, sb = b->scale;
   const int slots = a->slots;
-  keyswitch(C, w, w.T, D2, evk, level, out->d, out->d + half, half);
-  // c = (d0, d1) in coefficients + key-switch output
-  ntt_batch(E, D0, 2, 0, m, E.k, false, C.stream);
-  ew_binary_op(E, out->d, half, out->d, half, D0, half, 0, 0, m, 2, C.stream);
-  out->level = level;
+  copy_limbs(C, w.T, D2, (long)m * N);
+  ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  keyswitch_core(C, w, w.T, D2, evk, level);
+  keyswitch_finish(C, w, out->d, half, D0, D0 + half, level, do_rescale);
+  out->level = do_rescale ? level - 1 : level;
   out->slots = slots;
   out->scale = scale_after_mult(E, sa, sb, level);
-  out->domain = AOA_COEF;
-  if (do_rescale) {
-    rescale(E, out->d, half, 2, level, C.stream);
-    out->level = level - 1;
-  }
+  out->domain = AOA_NTT;
 }
 
 // Galois automorphism X -> X^g followed by the key switch with `key`
 // (ckks_rotate_left/right, ckks.cpp:953-1009; ckks_conjugate, ckks.cpp:1011-1040).
+// The automorphism is applied in the transform domain as a permutation of the
+// evaluation points (the reference permutes coefficients with a sign).
 void apply_galois(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* key) {
   const Engine& E = *C.E;
   const long N = E.N;
@@ -166,17 +204,97 @@ void apply_galois(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* k
   const int level = in->level, m = level + 1;
   const long half = (long)E.k * N;
   Workspace w = get_ws(C);
-  // the reference transforms the input to coefficients in place (encoder.cu:340)
-  to_domain(C, in, AOA_COEF, m);
-  automorph_coef_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
-  automorph_coef_op(E, w.T, in->d + half, 0, galois, m, 1, C.stream);
+  to_domain(C, in, AOA_NTT, m);
+  uint64_t* X = w.D + 2 * half;
+  automorph_ntt_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
+  automorph_ntt_op(E, X, in->d + half, 0, galois, m, 1, C.stream);
   const int slots = in->slots;
   const uint64_t scale = in->scale;
-  keyswitch(C, w, w.T, nullptr, key, level, out->d, out->d + half, half);
-  ew_binary_op(E, out->d, half, out->d, half, w.R0, 0, 0, 0, m, 1, C.stream);
+  copy_limbs(C, w.T, X, (long)m * N);
+  ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  keyswitch_core(C, w, w.T, X, key, level);
+  keyswitch_finish(C, w, out->d, half, w.R0, nullptr, level, false);
   out->level = level;
   out->slots = slots;
   out->scale = scale;
+  out->domain = AOA_NTT;
+}
+
+// The reference's per-call HMult + relinearise + rescale, step for step
+// (ckks_mul, ckks.cpp:273-347 over poly_t.cpp's domain rules): every poly op
+// covers the full base (k limbs, k + kl for the extended polys) whatever the
+// level, operands are transformed on demand, d2 goes through a full QB inverse
+// and forward transform, both key products through full QB inverse transforms,
+// and d0 / d1 / d2 come back to coefficients before the additions.  Same
+// residues as hmult(); kept as the plain per-call path the batched pipeline is
+// compared against.
+struct PlainWs {
+  uint64_t *axbx1, *axbx2, *bxbx, *axax, *qb, *t0, *t1;
+};
+
+void hmult_plain(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  if (a->level == 0 || b->level == 0)
+    throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
+  if (a->slots != b->slots) throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
+  if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
+  const int k = E.k, nqb = E.k + E.kl;
+  const int level = std::min(a->level, b->level);
+  const long half = (long)k * N, qb = (long)nqb * N;
+  if (!C.plain || C.plain_bytes < (size_t)(4 * half + 3 * qb) * 8) {
+    if (C.plain) AOA_CUDA(cudaFreeAsync(C.plain, C.stream));
+    C.plain = nullptr;
+    if (cudaMallocAsync(&C.plain, (size_t)(4 * half + 3 * qb) * 8, C.stream) != cudaSuccess) {
+      cudaGetLastError();
+      throw AoaError(AOA_ERR_OOM, "plain-path workspace allocation failed");
+    }
+    C.plain_bytes = (size_t)(4 * half + 3 * qb) * 8;
+  }
+  uint64_t* p = (uint64_t*)C.plain;
+  PlainWs s{p, p + half, p + 2 * half, p + 3 * half, p + 4 * half, p + 4 * half + qb, p + 4 * half + 2 * qb};
+  cudaStream_t st = C.stream;
+  int a_dom = a->domain, b_dom = b->domain;
+  // poly_add_add(axbx1 = c1[1] + c1[0], axbx2 = c2[1] + c2[0]) in the operands' domain
+  ew_binary_op(E, s.axbx1, 0, a->d + half, 0, a->d, 0, 0, 0, k, 1, st);
+  ew_binary_op(E, s.axbx2, 0, b->d + half, 0, b->d, 0, 0, 0, k, 1, st);
+  // poly_mul(axbx1, axbx1, axbx2): both to the transform domain, full base
+  if (a_dom == AOA_COEF) ntt_batch(E, s.axbx1, 1, 0, k, k, true, st);
+  if (b_dom == AOA_COEF) ntt_batch(E, s.axbx2, 1, 0, k, k, true, st);
+  ew_binary_op(E, s.axbx1, 0, s.axbx1, 0, s.axbx2, 0, 2, 0, k, 1, st);
+  // poly_mul(bxbx, c1[0], c2[0]) and poly_mul(axax, c1[1], c2[1]): operands transformed in place
+  to_domain(C, a, AOA_NTT, k);
+  if (b != a) to_domain(C, b, AOA_NTT, k);
+  ew_binary_op(E, s.bxbx, 0, a->d, 0, b->d, 0, 2, 0, k, 1, st);
+  ew_binary_op(E, s.axax, 0, a->d + half, 0, b->d + half, 0, 2, 0, k, 1, st);
+  const uint64_t sa = a->scale, sb = b->scale;
+  const int slots = a->slots;
+  // poly_modup: copy the Q part into a QB poly, inverse transform over QB, convert
+  copy_limbs(C, s.qb, s.axax, half);
+  ntt_batch(E, s.qb, 1, 0, nqb, nqb, false, st);
+  modup(E, s.qb, 0, s.qb + half, 0, 1, level, st);
+  // poly_mul with evk.b / evk.a over QB (forward transform of the whole QB poly)
+  ntt_batch(E, s.qb, 1, 0, nqb, nqb, true, st);
+  ew_binary_op(E, s.t0, 0, s.qb, 0, evk->d, 0, 2, 0, nqb, 1, st);
+  ew_binary_op(E, s.t1, 0, s.qb, 0, evk->d + qb, 0, 2, 0, nqb, 1, st);
+  // poly_moddown x2: full QB inverse transforms, then B -> Q
+  ntt_batch(E, s.t0, 2, 0, nqb, nqb, false, st);
+  moddown(E, s.t0, s.t0 + half, 0, s.t0, 0, 1, level, st);
+  moddown(E, s.t1, s.t1 + half, 0, s.t1, 0, 1, level, st);
+  // poly_add_add(c0 = bxbx + ks0, c1 = axbx1 + ks1): mixed domains -> coefficients
+  ntt_batch(E, s.bxbx, 1, 0, k, k, false, st);
+  ntt_batch(E, s.axbx1, 1, 0, k, k, false, st);
+  ew_binary_op(E, out->d, 0, s.bxbx, 0, s.t0, 0, 0, 0, k, 1, st);
+  ew_binary_op(E, out->d + half, 0, s.axbx1, 0, s.t1, 0, 0, 0, k, 1, st);
+  // poly_sub(c1 -= bxbx); poly_sub(c1 -= axax) with axax back to coefficients
+  ew_binary_op(E, out->d + half, 0, out->d + half, 0, s.bxbx, 0, 1, 0, k, 1, st);
+  ntt_batch(E, s.axax, 1, 0, k, k, false, st);
+  ew_binary_op(E, out->d + half, 0, out->d + half, 0, s.axax, 0, 1, 0, k, 1, st);
+  // ckks_rescale
+  rescale(E, out->d, half, 2, level, st);
+  out->level = level - 1;
+  out->slots = slots;
+  out->scale = scale_after_mult(E, sa, sb, level);
   out->domain = AOA_COEF;
 }
 
@@ -310,6 +428,11 @@ int aoa_hmult(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk)
 int aoa_hmult_relin_rescale(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
   if (!c || !out || !a || !b) return fail(AOA_ERR_BAD_PARAM, "null argument");
   return guarded([&] { hmult(c->c, out, a, b, evk, true); });
+}
+
+int aoa_hmult_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
+  if (!c || !out || !a || !b) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { hmult_plain(c->c, out, a, b, evk); });
 }
 
 int aoa_rescale(aoa_ctx* c, aoa_ct* ct) {

@@ -256,6 +256,7 @@ int aoa_ctx_destroy(aoa_ctx* h) {
   if (!h) return AOA_OK;
   int st = guarded([&] {
     if (h->c.scratch) AOA_CUDA(cudaFreeAsync(h->c.scratch, h->c.stream));
+    if (h->c.plain) AOA_CUDA(cudaFreeAsync(h->c.plain, h->c.stream));
     AOA_CUDA(cudaStreamSynchronize(h->c.stream));
     if (h->c.own_stream) AOA_CUDA(cudaStreamDestroy(h->c.stream));
   });

@@ -1,16 +1,24 @@
-// RNS basis conversion (ModUp / ModDown) and rescale, sm_100a CUDA cores.
+// RNS basis conversion (ModUp / ModDown), rescale and the key-switch epilogues,
+// sm_100a CUDA cores.
 //
 // Both conversions are small dense modular matrix products per coefficient:
 //   ModUp   (fast_conv_Q_to_B_opt, aoa-ntt src/cuda/manager.cu:180-223)
 //     B_j = sum_{i<=l} [x_i (Q_l/q_i)^-1]_{q_i} * [(Q_l/q_i)]_{b_j}   mod b_j
 //   ModDown (fast_conv_B_to_Q, manager.cu:312-341)
-//     out_i = (x_i - sum_j [x_j (B/b_j)^-1]_{b_j} * [(B/b_j)]_{q_i}) * B^-1 mod q_i
+//     out_i = (x_i - conv_i) * B^-1 mod q_i,
+//     conv_i = sum_j [x_j (B/b_j)^-1]_{b_j} * [(B/b_j)]_{q_i}          mod q_i
 // The reference reduces after every term (mulmod + addmod per term); here the
 // products accumulate exactly in 128 bits and each output is reduced once
-// (sum of <= 64 products of two < 2^63 values stays below 2^128).  The exact
-// residues are identical.  One thread owns one coefficient and keeps up to
-// 32 accumulators in registers; the constant matrix slice sits in shared
-// memory and is read as a warp broadcast.
+// (the 128-bit bound is checked per engine in rns_init).  The exact residues
+// are identical.  One thread owns one coefficient and keeps 16 accumulators in
+// registers; a CTA covers 128 coefficients x 32 outputs, the constant matrix
+// slice sits in shared memory and is read as a warp broadcast.
+//
+// Epilogues (what a conversion writes, per output limb i under prime p_i):
+//   kRaw        out = conv_i                                  (ModUp; ModDown's conv)
+//   kModDown    out = (x_i - conv_i) * B^-1                   (ModDown, coefficients)
+//   kRescaleTop out = d_l + (x_l - conv_l) * B^-1             (limb l of d + ModDown(x))
+//   kRescaleY   out = conv_i * B^-1 + [c_l]_{q_i}              (merged ModDown + rescale)
 #include "aoa_internal.h"
 
 namespace aoa {
@@ -21,34 +29,36 @@ constexpr int kConvHalves = kConvOut / kConvAcc;
 constexpr int kConvCoefs = 128;  // coefficients per CTA
 constexpr int kConvThreads = kConvCoefs * kConvHalves;
 
+enum { kRaw = 0, kModDown = 1, kRescaleTop = 2, kRescaleY = 3 };
+
 // in:  nin limbs at `in` (stride N), under primes in_prime0 + i
-// out: nout limbs at `out` (stride N), under primes out_prime0 + j
+// out: limbs j in [j_begin, j_end) at `out` + (j - out_shift)*N, under primes out_prime0 + j
 // zc[i]  : Shoup constant applied to input limb i before the product
 // mat    : [nin][mat_ld] matrix, entry (i, j) = multiplier of z_i for output j
-// post   : 0 = out_j = acc_j mod p_j (ModUp)
-//          1 = out_j = (x_j - acc_j mod p_j) * post_c[j]  with x_j = sub_src limb j (ModDown)
 struct ConvArgs {
   const uint64_t* in;
   uint64_t* out;
-  const uint64_t* sub_src;
-  long in_poly_stride, out_poly_stride, sub_poly_stride;   // in elements
-  int nin, nout, mat_ld;
+  const uint64_t* x;        // kModDown / kRescaleTop: x limbs (limb j at x + (j - x_shift)*N)
+  const uint64_t* d;        // kRescaleTop: d_l (one limb);  kRescaleY: c_l (one limb)
+  long in_poly_stride, out_poly_stride, x_poly_stride, d_poly_stride;   // in words
+  int nin, mat_ld;
   int in_prime0, out_prime0;
+  int out_shift, x_shift;
   const ShoupW* zc;
   const uint64_t* mat;
-  const ShoupW* post_c;
+  const ShoupW* binv;       // B^-1 mod q_j (Shoup form), indexed by output j
   const PrimeConst* pc;
   int log_n;
-  int post;
+  int mode;
 };
 
 __global__ void __launch_bounds__(kConvThreads, 2)
-basis_convert(ConvArgs a, int out_first) {
+basis_convert(ConvArgs a, int j_first, int j_end) {
   extern __shared__ uint64_t smat[];    // [nin][kConvOut]
-  const int nout = min(kConvOut, a.nout - out_first);
+  const int nout = min(kConvOut, j_end - j_first);
   for (int e = threadIdx.x; e < a.nin * kConvOut; e += blockDim.x) {
     const int i = e / kConvOut, j = e % kConvOut;
-    smat[e] = j < nout ? a.mat[(long)i * a.mat_ld + out_first + j] : 0;
+    smat[e] = j < nout ? a.mat[(long)i * a.mat_ld + j_first + j] : 0;
   }
   __syncthreads();
   const long N = 1L << a.log_n;
@@ -60,39 +70,44 @@ basis_convert(ConvArgs a, int out_first) {
   for (int j = 0; j < kConvAcc; j++) lo[j] = hi[j] = 0;
   uint64_t x_next = in[0];
   for (int i = 0; i < a.nin; i++) {
-    const uint64_t x = x_next;
+    const uint64_t xi = x_next;
     if (i + 1 < a.nin) x_next = in[(long)(i + 1) * N];     // prefetch the next input limb
     const uint64_t qi = a.pc[a.in_prime0 + i].q;
-    const uint64_t z = shoup(x, a.zc[i], qi);
+    const uint64_t z = shoup(xi, a.zc[i], qi);
     const uint64_t* row = smat + i * kConvOut + half * kConvAcc;
 #pragma unroll
     for (int j = 0; j < kConvAcc; j++) mac128(lo[j], hi[j], z, row[j]);
   }
   uint64_t* out = a.out + blockIdx.y * a.out_poly_stride + c;
+  uint64_t dv = 0;
+  if (a.mode == kRescaleTop || a.mode == kRescaleY) dv = a.d[blockIdx.y * a.d_poly_stride + c];
 #pragma unroll
   for (int jl = 0; jl < kConvAcc; jl++) {
     const int j = half * kConvAcc + jl;
     if (j < nout) {
-      const int jj = out_first + j;
+      const int jj = j_first + j;
       const PrimeConst& P = a.pc[a.out_prime0 + jj];
       uint64_t r = reduce128(lo[jl], hi[jl], P);
-      if (a.post) {
-        const uint64_t x = a.sub_src[blockIdx.y * a.sub_poly_stride + (long)jj * N + c];
-        r = shoup(sub_mod(x, r, P.q), a.post_c[jj], P.q);
+      if (a.mode == kModDown || a.mode == kRescaleTop) {
+        const uint64_t x = a.x[blockIdx.y * a.x_poly_stride + (long)(jj - a.x_shift) * N + c];
+        r = shoup(sub_mod(x, r, P.q), a.binv[jj], P.q);
+        if (a.mode == kRescaleTop) r = add_mod(r, dv, P.q);
+      } else if (a.mode == kRescaleY) {
+        r = add_mod(shoup(r, a.binv[jj], P.q), shoup(dv, 1, P.one_sh, P.q), P.q);
       }
-      out[(long)jj * N] = r;
+      out[(long)(jj - a.out_shift) * N] = r;
     }
   }
 }
 
-static void run_convert(const Engine& E, ConvArgs a, int npolys, cudaStream_t st) {
+static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_begin, int j_end, cudaStream_t st) {
   const long N = E.N;
   if (N % kConvCoefs) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: N too small");
   const size_t smem = (size_t)a.nin * kConvOut * sizeof(uint64_t);
   if (smem > 200 * 1024) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: too many input limbs");
   dim3 grid(N / kConvCoefs, npolys);
-  for (int j0 = 0; j0 < a.nout; j0 += kConvOut) {
-    basis_convert<<<grid, kConvThreads, smem, st>>>(a, j0);
+  for (int j0 = j_begin; j0 < j_end; j0 += kConvOut) {
+    basis_convert<<<grid, kConvThreads, smem, st>>>(a, j0, j_end);
     note_launch();
   }
   AOA_CHECK_LAUNCH();
@@ -117,14 +132,26 @@ void modup(const Engine& E, const uint64_t* in, long in_stride, uint64_t* out_b,
   if (E.kl == 0) return;
   if (level < 0 || level >= E.k) throw AoaError(AOA_ERR_BAD_PARAM, "modup: bad level");
   ConvArgs a{};
-  a.in = in; a.out = out_b; a.sub_src = nullptr;
+  a.in = in; a.out = out_b;
   a.in_poly_stride = in_stride; a.out_poly_stride = out_stride;
-  a.nin = level + 1; a.nout = E.kl; a.mat_ld = E.kl;
+  a.nin = level + 1; a.mat_ld = E.kl;
   a.in_prime0 = 0; a.out_prime0 = E.k;
   a.zc = E.rns.modup_inv + (long)level * E.k;
   a.mat = E.rns.modup_hat + (long)level * E.k * E.kl;
-  a.post_c = nullptr; a.pc = E.d_pc; a.log_n = E.log_n; a.post = 0;
-  run_convert(E, a, npolys, st);
+  a.pc = E.d_pc; a.log_n = E.log_n; a.mode = kRaw;
+  run_convert(E, a, npolys, 0, E.kl, st);
+}
+
+static ConvArgs moddown_args(const Engine& E, const uint64_t* in_b, long in_stride, uint64_t* out, long out_stride) {
+  ConvArgs a{};
+  a.in = in_b; a.out = out;
+  a.in_poly_stride = in_stride; a.out_poly_stride = out_stride;
+  a.nin = E.kl; a.mat_ld = E.k;
+  a.in_prime0 = E.k; a.out_prime0 = 0;
+  a.zc = E.rns.moddown_inv;
+  a.mat = E.rns.moddown_hat;
+  a.binv = E.rns.moddown_binv; a.pc = E.d_pc; a.log_n = E.log_n;
+  return a;
 }
 
 // ModDown: `in` holds Q limbs 0..level at in_q and kl B limbs at in_b
@@ -132,15 +159,39 @@ void modup(const Engine& E, const uint64_t* in, long in_stride, uint64_t* out_b,
 void moddown(const Engine& E, const uint64_t* in_q, const uint64_t* in_b, long in_stride, uint64_t* out,
              long out_stride, int npolys, int level, cudaStream_t st) {
   if (level < 0 || level >= E.k) throw AoaError(AOA_ERR_BAD_PARAM, "moddown: bad level");
-  ConvArgs a{};
-  a.in = in_b; a.out = out; a.sub_src = in_q;
-  a.in_poly_stride = in_stride; a.out_poly_stride = out_stride; a.sub_poly_stride = in_stride;
-  a.nin = E.kl; a.nout = level + 1; a.mat_ld = E.k;
-  a.in_prime0 = E.k; a.out_prime0 = 0;
-  a.zc = E.rns.moddown_inv;
-  a.mat = E.rns.moddown_hat;
-  a.post_c = E.rns.moddown_binv; a.pc = E.d_pc; a.log_n = E.log_n; a.post = 1;
-  run_convert(E, a, npolys, st);
+  ConvArgs a = moddown_args(E, in_b, in_stride, out, out_stride);
+  a.x = in_q; a.x_poly_stride = in_stride; a.mode = kModDown;
+  run_convert(E, a, npolys, 0, level + 1, st);
+}
+
+// conv_i (coefficient domain) of ModDown for outputs 0..nout-1, written to out.
+void moddown_conv(const Engine& E, const uint64_t* in_b, long in_stride, uint64_t* out, long out_stride,
+                  int npolys, int nout, cudaStream_t st) {
+  ConvArgs a = moddown_args(E, in_b, in_stride, out, out_stride);
+  a.mode = kRaw;
+  run_convert(E, a, npolys, 0, nout, st);
+}
+
+// Limb `level` of d + ModDown(x) in coefficients: d_l + (x_l - conv_l) B^-1.
+// x_l / d_l: one limb per poly (coefficient domain); out: one limb per poly.
+void rescale_top(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* x_l, long x_stride,
+                 const uint64_t* d_l, long d_stride, uint64_t* out, long out_stride, int npolys, int level,
+                 cudaStream_t st) {
+  ConvArgs a = moddown_args(E, in_b, in_stride, out, out_stride);
+  a.mode = kRescaleTop;
+  a.x = x_l; a.x_poly_stride = x_stride; a.x_shift = level;
+  a.d = d_l; a.d_poly_stride = d_stride;
+  a.out_shift = level;
+  run_convert(E, a, npolys, level, level + 1, st);
+}
+
+// y_i = conv_i B^-1 + [c_l]_{q_i} for i < level (coefficient domain).
+void rescale_y(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* c_l, long c_stride,
+               uint64_t* out, long out_stride, int npolys, int level, cudaStream_t st) {
+  ConvArgs a = moddown_args(E, in_b, in_stride, out, out_stride);
+  a.mode = kRescaleY;
+  a.d = c_l; a.d_poly_stride = c_stride;
+  run_convert(E, a, npolys, 0, level, st);
 }
 
 // Rescale by q_level (ckks_rescale, manager.cu:90-118): for i < level,
@@ -161,7 +212,44 @@ void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int lev
   if (level < 1 || level >= E.k) throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "rescale: level must be >= 1");
   dim3 grid(E.N / 256, level, npolys);
   rescale_kernel<<<grid, 256, 0, st>>>(d, poly_stride, level, E.rns.resc_inv + (long)level * E.k, E.d_pc,
-                                       E.log_n); note_launch();
+                                       E.log_n);
+  note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+// Transform-domain key-switch epilogue, limbs i < nlimbs of npolys polys:
+//   rescale_level > 0: out_i = (base_i + k_i B^-1 - y_i) * q_l^-1   (merged ModDown + rescale)
+//   else:              out_i = base_i + (k_i - y_i) * B^-1           (ModDown)
+// base may be null (treated as 0).  Strides are per poly, in words.
+__global__ void ks_combine_kernel(uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
+                                  const uint64_t* k, long k_stride, const uint64_t* y, long y_stride,
+                                  const ShoupW* binv, const ShoupW* resc, const PrimeConst* pc, int log_n) {
+  const long N = 1L << log_n;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y, p = blockIdx.z;
+  const long off = (long)i * N + c;
+  const uint64_t q = pc[i].q;
+  const uint64_t kv = k[p * k_stride + off], yv = y[p * y_stride + off];
+  const uint64_t bv = base ? base[p * base_stride + off] : 0;
+  uint64_t r;
+  if (resc) {
+    r = sub_mod(add_mod(bv, shoup(kv, binv[i], q), q), yv, q);
+    r = shoup(r, resc[i], q);
+  } else {
+    r = add_mod(bv, shoup(sub_mod(kv, yv, q), binv[i], q), q);
+  }
+  out[p * out_stride + off] = r;
+}
+
+void ks_combine(const Engine& E, uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
+                const uint64_t* k, long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys,
+                int rescale_level, cudaStream_t st) {
+  if (nlimbs <= 0) return;
+  dim3 grid(E.N / 256, nlimbs, npolys);
+  const ShoupW* resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
+  ks_combine_kernel<<<grid, 256, 0, st>>>(out, out_stride, base, base_stride, k, k_stride, y, y_stride,
+                                          E.rns.moddown_binv, resc, E.d_pc, E.log_n);
+  note_launch();
   AOA_CHECK_LAUNCH();
 }
 

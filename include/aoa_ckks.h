@@ -156,6 +156,11 @@ int aoa_swk_destroy(aoa_ctx* c, aoa_swk* k);
 int aoa_hmult(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
 /* ckks_mul (ckks.cpp:334-347): HMult + relinearise + rescale.                */
 int aoa_hmult_relin_rescale(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
+/* The reference's per-call ckks_mul sequence (ckks.cpp:273-347 with the
+ * poly_t.cpp domain rules: full-base transforms, unfused element-wise ops),
+ * on this engine's kernels; same residues as aoa_hmult_relin_rescale, output
+ * in coefficients.  The plain per-call baseline of the benchmarks.           */
+int aoa_hmult_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
 /* ckks_rescale (ckks.cpp:220-230) */
 int aoa_rescale(aoa_ctx* c, aoa_ct* ct);
 /* ckks_add / ckks_sub (ckks.cpp:232-271) */

@@ -88,6 +88,53 @@ def test_hmult_relin_rescale_bit_exact(ref_table, pset, log_n, in_domain):
         assert np.array_equal(g0, w0[:level]) and np.array_equal(g1, w1[:level])
 
 
+@pytest.mark.parametrize("pset", ["ref55", "p60"])
+def test_hmult_plain_path_matches_oracle(ref_table, pset):
+    """The reference-structured per-call path gives the same residues."""
+    require_gpu()
+    Q, B = _sets(ref_table)[pset]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=31)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(77)
+    N, k = E.N, E.k
+    a = _rand_ct(rng, Q, N, k)
+    b = _rand_ct(rng, Q, N, k)
+    ca = aoa.Ciphertext.from_residues(ctx, *a, slots=8, scale=1 << 40)
+    cb = aoa.Ciphertext.from_residues(ctx, *b, slots=8, scale=1 << 41)
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_mul_plain(ctx, out, ca, cb, evk)
+    w0, w1, wsc = o.hmult(a, b, keys["evk"], k - 1, 1 << 40, 1 << 41, rescale=True)
+    g0, g1 = out.download(nlimbs=k - 1)
+    assert out.level == k - 2 and out.scale == wsc and out.domain == aoa.AOA_COEF
+    assert np.array_equal(g0, w0[: k - 1]) and np.array_equal(g1, w1[: k - 1])
+
+
+def test_hmult_chain_in_transform_domain(ref_table):
+    """Three chained HMults stay in the transform domain and match the oracle chain."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=5)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(3)
+    N, k = E.N, E.k
+    x = _rand_ct(rng, Q, N, k)
+    cx = aoa.Ciphertext.from_residues(ctx, *x, slots=4, scale=1 << 30)
+    cur, sc = (x[0].copy(), x[1].copy()), 1 << 30
+    lvl = k - 1
+    for _ in range(3):
+        aoa.ckks_mul(ctx, cx, cx, cx, evk)
+        assert cx.domain == aoa.AOA_NTT
+        pad = lambda v: np.concatenate([v[: lvl + 1], np.zeros((k - lvl - 1, N), dtype=np.uint64)])
+        w0, w1, sc = o.hmult((pad(cur[0]), pad(cur[1])), (pad(cur[0]), pad(cur[1])), keys["evk"], lvl, sc, sc)
+        lvl -= 1
+        cur = (w0, w1)
+        g0, g1 = cx.download(nlimbs=lvl + 1)
+        assert cx.level == lvl and cx.scale == sc
+        assert np.array_equal(g0, w0[: lvl + 1]) and np.array_equal(g1, w1[: lvl + 1])
+
+
 def test_hmult_without_rescale_and_aliasing(ref_table):
     require_gpu()
     Q, B = _sets(ref_table)["p60"]
