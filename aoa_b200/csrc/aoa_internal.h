@@ -123,14 +123,12 @@ void moddown(const Engine& E, const uint64_t* in_q, const uint64_t* in_b, long i
 void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int level, cudaStream_t st);
 void moddown_conv(const Engine& E, const uint64_t* in_b, long in_stride, uint64_t* out, long out_stride,
                   int npolys, int nout, cudaStream_t st);
-void rescale_top(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* x_l, long x_stride,
-                 const uint64_t* d_l, long d_stride, uint64_t* out, long out_stride, int npolys, int level,
-                 cudaStream_t st);
-void rescale_y(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* c_l, long c_stride,
-               uint64_t* out, long out_stride, int npolys, int level, cudaStream_t st);
+void rescale_corrections(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* u_l,
+                         long u_stride, uint64_t* cl_tmp, long cl_stride, uint64_t* y, long y_stride, int npolys,
+                         int level, cudaStream_t st);
 void ks_combine(const Engine& E, uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
                 const uint64_t* k, long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys,
-                int rescale_level, cudaStream_t st);
+                int rescale_level, cudaStream_t st, int prime0 = 0);
 
 // ops.cu  (op: 0 add, 1 sub, 2 mul, 3 neg)
 void ew_binary_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as, const uint64_t* b, long bs,

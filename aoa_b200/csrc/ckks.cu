@@ -121,21 +121,19 @@ static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long hal
   const long ks_stride = (long)(E.k + E.kl) * N;
   const uint64_t* kb = w.KS + (long)m * N;
   if (do_rescale) {
-    // limb l of both products and of the base, in coefficients
-    int nl = 2;
-    copy_limbs(C, w.L4 + 2 * N, w.KS + (long)level * N, N);
-    copy_limbs(C, w.L4 + 3 * N, w.KS + ks_stride + (long)level * N, N);
-    if (b0) {
-      copy_limbs(C, w.L4, b0 + (long)level * N, N);
-      if (b1) copy_limbs(C, w.L4 + N, b1 + (long)level * N, N);
-      else AOA_CUDA(cudaMemsetAsync(w.L4 + N, 0, N * 8, C.stream));
-      nl = 4;
+    // u_l = limb l of (base + k B^-1) in coefficients, for both polys
+    uint64_t* U = w.L4;
+    if (b0 && b1 == b0 + half) {
+      ks_combine(E, U, N, b0 + (long)level * N, half, w.KS + (long)level * N, ks_stride, nullptr, 0, 1, 2, 0,
+                 C.stream, level);
     } else {
-      AOA_CUDA(cudaMemsetAsync(w.L4, 0, 2 * N * 8, C.stream));
+      ks_combine(E, U, 0, b0 ? b0 + (long)level * N : nullptr, 0, w.KS + (long)level * N, 0, nullptr, 0, 1, 1,
+                 0, C.stream, level);
+      ks_combine(E, U + N, 0, b1 ? b1 + (long)level * N : nullptr, 0, w.KS + ks_stride + (long)level * N, 0,
+                 nullptr, 0, 1, 1, 0, C.stream, level);
     }
-    ntt_batch(E, w.L4 + (4 - nl) * N, nl, level, 1, 1, false, C.stream);
-    rescale_top(E, kb, ks_stride, w.L4 + 2 * N, N, w.L4, N, w.CL, N, 2, level, C.stream);
-    rescale_y(E, kb, ks_stride, w.CL, N, w.Y, (long)E.k * N, 2, level, C.stream);
+    ntt_batch(E, U, 2, level, 1, 1, false, C.stream);
+    rescale_corrections(E, kb, ks_stride, U, N, w.CL, N, w.Y, (long)E.k * N, 2, level, C.stream);
     ntt_batch(E, w.Y, 2, 0, level, E.k, true, C.stream);
     if (b0 && b1 == b0 + half) {
       ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, level, 2, level, C.stream);

@@ -17,8 +17,11 @@
 // Epilogues (what a conversion writes, per output limb i under prime p_i):
 //   kRaw        out = conv_i                                  (ModUp; ModDown's conv)
 //   kModDown    out = (x_i - conv_i) * B^-1                   (ModDown, coefficients)
-//   kRescaleTop out = d_l + (x_l - conv_l) * B^-1             (limb l of d + ModDown(x))
+//   kRescaleTop out = u_l - conv_l * B^-1                      (c_l: limb l of d + ModDown(x),
+//                                                               u_l = d_l + x_l B^-1 in coefficients)
 //   kRescaleY   out = conv_i * B^-1 + [c_l]_{q_i}              (merged ModDown + rescale)
+//   kRescaleFused  both in one pass when all outputs 0..l fit one launch: the
+//               thread owning output l shares c_l through shared memory
 #include "aoa_internal.h"
 
 namespace aoa {
@@ -29,7 +32,7 @@ constexpr int kConvHalves = kConvOut / kConvAcc;
 constexpr int kConvCoefs = 128;  // coefficients per CTA
 constexpr int kConvThreads = kConvCoefs * kConvHalves;
 
-enum { kRaw = 0, kModDown = 1, kRescaleTop = 2, kRescaleY = 3 };
+enum { kRaw = 0, kModDown = 1, kRescaleTop = 2, kRescaleY = 3, kRescaleFused = 4 };
 
 // in:  nin limbs at `in` (stride N), under primes in_prime0 + i
 // out: limbs j in [j_begin, j_end) at `out` + (j - out_shift)*N, under primes out_prime0 + j
@@ -38,8 +41,8 @@ enum { kRaw = 0, kModDown = 1, kRescaleTop = 2, kRescaleY = 3 };
 struct ConvArgs {
   const uint64_t* in;
   uint64_t* out;
-  const uint64_t* x;        // kModDown / kRescaleTop: x limbs (limb j at x + (j - x_shift)*N)
-  const uint64_t* d;        // kRescaleTop: d_l (one limb);  kRescaleY: c_l (one limb)
+  const uint64_t* x;        // kModDown: x limbs (limb j at x + (j - x_shift)*N)
+  const uint64_t* d;        // kRescaleTop / kRescaleFused: u_l;  kRescaleY: c_l (one limb per poly)
   long in_poly_stride, out_poly_stride, x_poly_stride, d_poly_stride;   // in words
   int nin, mat_ld;
   int in_prime0, out_prime0;
@@ -80,7 +83,33 @@ basis_convert(ConvArgs a, int j_first, int j_end) {
   }
   uint64_t* out = a.out + blockIdx.y * a.out_poly_stride + c;
   uint64_t dv = 0;
-  if (a.mode == kRescaleTop || a.mode == kRescaleY) dv = a.d[blockIdx.y * a.d_poly_stride + c];
+  if (a.mode >= kRescaleTop) dv = a.d[blockIdx.y * a.d_poly_stride + c];
+  if (a.mode == kRescaleFused) {
+    // outputs 0..l with l = j_end - 1 < kConvOut: c_l first, shared through smem
+    __shared__ uint64_t s_cl[kConvCoefs];
+    const int l = j_end - 1;
+    if (half == l / kConvAcc) {
+#pragma unroll
+      for (int jl = 0; jl < kConvAcc; jl++)
+        if (jl == l % kConvAcc) {
+          const PrimeConst& P = a.pc[a.out_prime0 + l];
+          const uint64_t r = reduce128(lo[jl], hi[jl], P);
+          s_cl[threadIdx.x % kConvCoefs] = sub_mod(dv, shoup(r, a.binv[l], P.q), P.q);
+        }
+    }
+    __syncthreads();
+    const uint64_t cl = s_cl[threadIdx.x % kConvCoefs];
+#pragma unroll
+    for (int jl = 0; jl < kConvAcc; jl++) {
+      const int j = half * kConvAcc + jl;
+      if (j < l) {
+        const PrimeConst& P = a.pc[a.out_prime0 + j];
+        const uint64_t r = reduce128(lo[jl], hi[jl], P);
+        out[(long)(j - a.out_shift) * N] = add_mod(shoup(r, a.binv[j], P.q), shoup(cl, 1, P.one_sh, P.q), P.q);
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int jl = 0; jl < kConvAcc; jl++) {
     const int j = half * kConvAcc + jl;
@@ -88,10 +117,11 @@ basis_convert(ConvArgs a, int j_first, int j_end) {
       const int jj = j_first + j;
       const PrimeConst& P = a.pc[a.out_prime0 + jj];
       uint64_t r = reduce128(lo[jl], hi[jl], P);
-      if (a.mode == kModDown || a.mode == kRescaleTop) {
+      if (a.mode == kModDown) {
         const uint64_t x = a.x[blockIdx.y * a.x_poly_stride + (long)(jj - a.x_shift) * N + c];
         r = shoup(sub_mod(x, r, P.q), a.binv[jj], P.q);
-        if (a.mode == kRescaleTop) r = add_mod(r, dv, P.q);
+      } else if (a.mode == kRescaleTop) {
+        r = sub_mod(dv, shoup(r, a.binv[jj], P.q), P.q);
       } else if (a.mode == kRescaleY) {
         r = add_mod(shoup(r, a.binv[jj], P.q), shoup(dv, 1, P.one_sh, P.q), P.q);
       }
@@ -172,25 +202,27 @@ void moddown_conv(const Engine& E, const uint64_t* in_b, long in_stride, uint64_
   run_convert(E, a, npolys, 0, nout, st);
 }
 
-// Limb `level` of d + ModDown(x) in coefficients: d_l + (x_l - conv_l) B^-1.
-// x_l / d_l: one limb per poly (coefficient domain); out: one limb per poly.
-void rescale_top(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* x_l, long x_stride,
-                 const uint64_t* d_l, long d_stride, uint64_t* out, long out_stride, int npolys, int level,
-                 cudaStream_t st) {
-  ConvArgs a = moddown_args(E, in_b, in_stride, out, out_stride);
-  a.mode = kRescaleTop;
-  a.x = x_l; a.x_poly_stride = x_stride; a.x_shift = level;
-  a.d = d_l; a.d_poly_stride = d_stride;
-  a.out_shift = level;
-  run_convert(E, a, npolys, level, level + 1, st);
-}
-
-// y_i = conv_i B^-1 + [c_l]_{q_i} for i < level (coefficient domain).
-void rescale_y(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* c_l, long c_stride,
-               uint64_t* out, long out_stride, int npolys, int level, cudaStream_t st) {
-  ConvArgs a = moddown_args(E, in_b, in_stride, out, out_stride);
+// Merged ModDown + rescale corrections: given the key products' B limbs (in_b,
+// coefficients) and u_l = limb l of (d + k B^-1) in coefficients, writes
+// y_i = conv_i B^-1 + [c_l]_{q_i} for i < level, c_l = u_l - conv_l B^-1.
+// One launch when level < 32, else c_l first (into cl_tmp) and then the y_i.
+void rescale_corrections(const Engine& E, const uint64_t* in_b, long in_stride, const uint64_t* u_l,
+                         long u_stride, uint64_t* cl_tmp, long cl_stride, uint64_t* y, long y_stride, int npolys,
+                         int level, cudaStream_t st) {
+  ConvArgs a = moddown_args(E, in_b, in_stride, y, y_stride);
+  if (level < kConvOut) {
+    a.mode = kRescaleFused;
+    a.d = u_l; a.d_poly_stride = u_stride;
+    run_convert(E, a, npolys, 0, level + 1, st);
+    return;
+  }
+  ConvArgs t = moddown_args(E, in_b, in_stride, cl_tmp, cl_stride);
+  t.mode = kRescaleTop;
+  t.d = u_l; t.d_poly_stride = u_stride;
+  t.out_shift = level;
+  run_convert(E, t, npolys, level, level + 1, st);
   a.mode = kRescaleY;
-  a.d = c_l; a.d_poly_stride = c_stride;
+  a.d = cl_tmp; a.d_poly_stride = cl_stride;
   run_convert(E, a, npolys, 0, level, st);
 }
 
@@ -220,16 +252,18 @@ void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int lev
 // Transform-domain key-switch epilogue, limbs i < nlimbs of npolys polys:
 //   rescale_level > 0: out_i = (base_i + k_i B^-1 - y_i) * q_l^-1   (merged ModDown + rescale)
 //   else:              out_i = base_i + (k_i - y_i) * B^-1           (ModDown)
-// base may be null (treated as 0).  Strides are per poly, in words.
+// base and y may be null (treated as 0); limb b of the launch is limb prime0 + b
+// (prime prime0 + b).  Strides are per poly, in words.
 __global__ void ks_combine_kernel(uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
                                   const uint64_t* k, long k_stride, const uint64_t* y, long y_stride,
-                                  const ShoupW* binv, const ShoupW* resc, const PrimeConst* pc, int log_n) {
+                                  const ShoupW* binv, const ShoupW* resc, const PrimeConst* pc, int prime0,
+                                  int log_n) {
   const long N = 1L << log_n;
   const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y, p = blockIdx.z;
-  const long off = (long)i * N + c;
+  const int i = prime0 + blockIdx.y, p = blockIdx.z;
+  const long off = (long)blockIdx.y * N + c;
   const uint64_t q = pc[i].q;
-  const uint64_t kv = k[p * k_stride + off], yv = y[p * y_stride + off];
+  const uint64_t kv = k[p * k_stride + off], yv = y ? y[p * y_stride + off] : 0;
   const uint64_t bv = base ? base[p * base_stride + off] : 0;
   uint64_t r;
   if (resc) {
@@ -243,12 +277,12 @@ __global__ void ks_combine_kernel(uint64_t* out, long out_stride, const uint64_t
 
 void ks_combine(const Engine& E, uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
                 const uint64_t* k, long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys,
-                int rescale_level, cudaStream_t st) {
+                int rescale_level, cudaStream_t st, int prime0) {
   if (nlimbs <= 0) return;
   dim3 grid(E.N / 256, nlimbs, npolys);
   const ShoupW* resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
   ks_combine_kernel<<<grid, 256, 0, st>>>(out, out_stride, base, base_stride, k, k_stride, y, y_stride,
-                                          E.rns.moddown_binv, resc, E.d_pc, E.log_n);
+                                          E.rns.moddown_binv, resc, E.d_pc, prime0, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
 }
