@@ -297,3 +297,15 @@ def kernel_launches():
 def ckks_mul_plain(ctx, c3, c1, c2, evk):
     """The reference's per-call ckks_mul sequence on this engine (comparison path)."""
     capi.check(capi.load().aoa_hmult_plain(ctx.handle, c3.handle, c1.handle, c2.handle, _h(evk)))
+
+
+def ckks_mul_batch(ctx, outs, c1s, c2s, evk, rescale=True):
+    """outs[i] = c1s[i] * c2s[i] (+ relinearise, + rescale) in grouped batched launches."""
+    n = len(outs)
+    if not (len(c1s) == len(c2s) == n):
+        raise ValueError("batch lists differ in length")
+    arr = ctypes.c_void_p * max(n, 1)
+    o = arr(*[x.handle.value for x in outs])
+    a = arr(*[x.handle.value for x in c1s])
+    b = arr(*[x.handle.value for x in c2s])
+    capi.check(capi.load().aoa_hmult_batch(ctx.handle, n, o, a, b, _h(evk), 1 if rescale else 0))

@@ -87,6 +87,20 @@ struct Ctx {
   size_t scratch_bytes = 0;
   void* plain = nullptr;        // workspace of the reference-structured per-call path
   size_t plain_bytes = 0;
+  void* batch = nullptr;        // workspace of batched HMult
+  size_t batch_bytes = 0;
+  void* conv = nullptr;         // domain-conversion buffer for downloads
+  size_t conv_bytes = 0;
+};
+
+// Per-launch pointer lists for batched kernels (passed by value).
+constexpr int kMaxBatch = 64;
+struct CtPtrs {
+  const uint64_t* a[kMaxBatch];
+  const uint64_t* b[kMaxBatch];
+};
+struct OutPtrs {
+  uint64_t* p[2 * kMaxBatch];
 };
 
 // count of kernel launches issued by this library (engine.cu)
@@ -139,6 +153,12 @@ void ew_muladd_op(const Engine& E, uint64_t* d, long ds, const uint64_t* a, long
                   const uint64_t* c, long cs, int prime0, int nlimbs, int npolys, cudaStream_t st);
 void tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
                uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st);
+void tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D, int n, int nlimbs, cudaStream_t st);
+void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                            const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st);
+void ks_combine_ptr(const Engine& E, const OutPtrs& outp, const uint64_t* base, long base_stride, const uint64_t* k,
+                    long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys, int rescale_level,
+                    cudaStream_t st);
 void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
                       uint64_t* k1, int nq, cudaStream_t st);
 void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,

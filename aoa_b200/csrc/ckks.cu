@@ -218,6 +218,121 @@ void apply_galois(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* k
   out->domain = AOA_NTT;
 }
 
+// Batched HMult (+ relinearise + rescale) of n <= kMaxBatch independent
+// products at one level: every pipeline stage is one launch over the whole
+// batch (transforms over n x limbs items, conversions over n x polys, the
+// element-wise kernels over n ciphertexts), so small per-op stages no longer
+// leave the GPU idle.  Batch workspace layout (N-word limbs):
+//   D [3][n][k]  T [n][k]  UB [n][kl]  KS [2][n][k+kl]  U [2][n]  CL [2][n]  Y [2][n][k]
+static size_t batch_words(const Engine& E, int n) {
+  return (size_t)E.N * n * (8 * E.k + 3 * std::max(E.kl, 1) + 4);
+}
+
+static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b,
+                              const aoa_swk* evk, bool do_rescale, int level) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  const int m = level + 1, k = E.k, kl = E.kl;
+  const long half = (long)k * N, ks = (long)(k + kl) * N;
+  const size_t need = batch_words(E, n) * 8;
+  if (C.batch_bytes < need) {
+    if (C.batch) AOA_CUDA(cudaFreeAsync(C.batch, C.stream));
+    C.batch = nullptr;
+    C.batch_bytes = 0;
+    if (cudaMallocAsync(&C.batch, need, C.stream) != cudaSuccess) {
+      cudaGetLastError();
+      throw AoaError(AOA_ERR_OOM, "batch workspace allocation failed");
+    }
+    C.batch_bytes = need;
+  }
+  uint64_t* p = (uint64_t*)C.batch;
+  uint64_t* D = p;  p += 3L * n * half;
+  uint64_t* T = p;  p += (long)n * half;
+  uint64_t* UB = p; p += (long)n * kl * N;
+  uint64_t* KS = p; p += 2L * n * ks;
+  uint64_t* U = p;  p += 2L * n * N;
+  uint64_t* CL = p; p += 2L * n * N;
+  uint64_t* Y = p;
+  cudaStream_t st = C.stream;
+  CtPtrs ptr;
+  uint64_t sa[kMaxBatch], sb[kMaxBatch];
+  int slots[kMaxBatch];
+  for (int z = 0; z < n; z++) {
+    to_domain(C, a[z], AOA_NTT, a[z]->level + 1);
+    to_domain(C, b[z], AOA_NTT, b[z]->level + 1);
+    ptr.a[z] = a[z]->d;
+    ptr.b[z] = b[z]->d;
+    sa[z] = a[z]->scale;
+    sb[z] = b[z]->scale;
+    slots[z] = a[z]->slots;
+  }
+  tensor_batch_op(E, ptr, half, D, n, m, st);
+  uint64_t* D2 = D + 2L * n * half;
+  AOA_CUDA(cudaMemcpy2DAsync(T, half * 8, D2, half * 8, (size_t)m * N * 8, n, cudaMemcpyDeviceToDevice, st));
+  ntt_batch(E, T, n, 0, m, k, false, st);
+  modup(E, T, half, UB, (long)kl * N, n, level, st);
+  ntt_batch(E, UB, n, k, kl, kl, true, st);
+  keyswitch_mul_batch_op(E, D2, half, UB, (long)kl * N, evk->d, KS, ks, n, m, st);
+  ntt_batch(E, KS + (long)m * N, 2 * n, k, kl, k + kl, false, st);
+  OutPtrs outp;
+  for (int z = 0; z < n; z++) {
+    outp.p[z] = out[z]->d;
+    outp.p[n + z] = out[z]->d + half;
+  }
+  if (do_rescale) {
+    ks_combine(E, U, N, D + (long)level * N, half, KS + (long)level * N, ks, nullptr, 0, 1, 2 * n, 0, st, level);
+    ntt_batch(E, U, 2 * n, level, 1, 1, false, st);
+    rescale_corrections(E, KS + (long)m * N, ks, U, N, CL, N, Y, half, 2 * n, level, st);
+    ntt_batch(E, Y, 2 * n, 0, level, k, true, st);
+    ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, level, 2 * n, level, st);
+  } else {
+    moddown_conv(E, KS + (long)m * N, ks, Y, half, 2 * n, m, st);
+    ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
+    ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, m, 2 * n, 0, st);
+  }
+  for (int z = 0; z < n; z++) {
+    out[z]->level = do_rescale ? level - 1 : level;
+    out[z]->slots = slots[z];
+    out[z]->scale = scale_after_mult(E, sa[z], sb[z], level);
+    out[z]->domain = AOA_NTT;
+  }
+}
+
+void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b, const aoa_swk* evk,
+                 bool do_rescale) {
+  const Engine& E = *C.E;
+  if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
+  if (n == 0) return;
+  if (!out || !a || !b) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
+  if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
+  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
+  std::vector<int> idx(n);
+  for (int z = 0; z < n; z++) {
+    if (!out[z] || !a[z] || !b[z]) throw AoaError(AOA_ERR_BAD_PARAM, "null ciphertext in batch");
+    if (a[z]->level == 0 || b[z]->level == 0)
+      throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
+    if (a[z]->slots != b[z]->slots)
+      throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
+    idx[z] = z;
+  }
+  // group by level (the operands' common limb count), chunks of kMaxBatch
+  auto lvl = [&](int z) { return std::min(a[z]->level, b[z]->level); };
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lvl(x) > lvl(y); });
+  std::vector<aoa_ct*> go, ga, gb;
+  for (int s = 0; s < n;) {
+    int e = s;
+    while (e < n && lvl(idx[e]) == lvl(idx[s]) && e - s < kMaxBatch) e++;
+    go.clear(); ga.clear(); gb.clear();
+    for (int t = s; t < e; t++) {
+      go.push_back(out[idx[t]]);
+      ga.push_back(a[idx[t]]);
+      gb.push_back(b[idx[t]]);
+    }
+    hmult_batch_group(C, e - s, go.data(), ga.data(), gb.data(), evk, do_rescale, lvl(idx[s]));
+    s = e;
+  }
+}
+
 // The reference's per-call HMult + relinearise + rescale, step for step
 // (ckks_mul, ckks.cpp:273-347 over poly_t.cpp's domain rules): every poly op
 // covers the full base (k limbs, k + kl for the extended polys) whatever the
@@ -376,15 +491,21 @@ int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, in
     const uint64_t* src = ct->d;
     uint64_t* tmp = nullptr;
     if (domain != ct->domain) {
-      AOA_CUDA(cudaMallocAsync(&tmp, 2 * E.k * limb, C.stream));
-      AOA_CUDA(cudaMemcpyAsync(tmp, ct->d, 2 * E.k * limb, cudaMemcpyDeviceToDevice, C.stream));
+      if (C.conv_bytes < 2 * E.k * limb) {
+        if (C.conv) AOA_CUDA(cudaFreeAsync(C.conv, C.stream));
+        C.conv = nullptr;
+        AOA_CUDA(cudaMallocAsync(&C.conv, 2 * E.k * limb, C.stream));
+        C.conv_bytes = 2 * E.k * limb;
+      }
+      tmp = (uint64_t*)C.conv;
+      AOA_CUDA(cudaMemcpy2DAsync(tmp, E.k * limb, ct->d, E.k * limb, nlimbs * limb, 2, cudaMemcpyDeviceToDevice,
+                                 C.stream));
       ntt_batch(E, tmp, 2, 0, nlimbs, E.k, domain == AOA_NTT, C.stream);
       src = tmp;
     }
     for (int p = 0; p < 2; p++)
       AOA_CUDA(cudaMemcpyAsync(host + (size_t)p * nlimbs * E.N, src + (size_t)p * E.k * E.N, nlimbs * limb,
                                cudaMemcpyDeviceToHost, C.stream));
-    if (tmp) AOA_CUDA(cudaFreeAsync(tmp, C.stream));
     AOA_CUDA(cudaStreamSynchronize(C.stream));
   });
 }
@@ -426,6 +547,12 @@ int aoa_hmult(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk)
 int aoa_hmult_relin_rescale(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
   if (!c || !out || !a || !b) return fail(AOA_ERR_BAD_PARAM, "null argument");
   return guarded([&] { hmult(c->c, out, a, b, evk, true); });
+}
+
+int aoa_hmult_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b,
+                    const aoa_swk* evk, int rescale) {
+  if (!c) return fail(AOA_ERR_BAD_PARAM, "null context");
+  return guarded([&] { hmult_batch(c->c, n, out, a, b, evk, rescale != 0); });
 }
 
 int aoa_hmult_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {

@@ -183,6 +183,12 @@ int aoa_engine_create(const aoa_params* p, aoa_engine** out) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
       throw AoaError(AOA_ERR_NO_DEVICE, "no CUDA device visible");
     AOA_CUDA(cudaGetDevice(&E.device));
+    {   // keep stream-ordered allocations cached across synchronisations
+      cudaMemPool_t pool;
+      AOA_CUDA(cudaDeviceGetDefaultMemPool(&pool, E.device));
+      uint64_t keep = ~0ull;
+      AOA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     E.log_n = p->log_n;
     E.N = 1L << p->log_n;
     E.log_c = p->log_n / 2;
@@ -257,6 +263,8 @@ int aoa_ctx_destroy(aoa_ctx* h) {
   int st = guarded([&] {
     if (h->c.scratch) AOA_CUDA(cudaFreeAsync(h->c.scratch, h->c.stream));
     if (h->c.plain) AOA_CUDA(cudaFreeAsync(h->c.plain, h->c.stream));
+    if (h->c.batch) AOA_CUDA(cudaFreeAsync(h->c.batch, h->c.stream));
+    if (h->c.conv) AOA_CUDA(cudaFreeAsync(h->c.conv, h->c.stream));
     AOA_CUDA(cudaStreamSynchronize(h->c.stream));
     if (h->c.own_stream) AOA_CUDA(cudaStreamDestroy(h->c.stream));
   });

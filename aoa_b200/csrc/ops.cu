@@ -123,6 +123,46 @@ __global__ void automorph_ntt(uint64_t* out, const uint64_t* in, long poly_strid
   out[off + p] = in[off + src];
 }
 
+// ---- batched variants (one launch for a batch of ciphertexts) ---------------------
+
+// tensor for op z = blockIdx.z: a = ptr.a[z], b = ptr.b[z] ([c0 | c1], stride half);
+// outputs to the blocks D0 = D, D1 = D + n*half, D2 = D + 2n*half, op stride half.
+__global__ void hmult_tensor_batch(CtPtrs ptr, long half, uint64_t* D, int n, const PrimeConst* pc, int log_n) {
+  const long N = 1L << log_n;
+  const int z = blockIdx.z;
+  const long off = (long)blockIdx.y * N + coef_index();
+  const PrimeConst& P = pc[blockIdx.y];
+  const uint64_t* a = ptr.a[z];
+  const uint64_t* b = ptr.b[z];
+  const uint64_t x0 = a[off], x1 = a[half + off], y0 = b[off], y1 = b[half + off];
+  const uint64_t q = P.q, qi = P.qinv_neg;
+  uint64_t m0 = mont_mul(x0, y0, q, qi);
+  uint64_t m1 = add_mod(mont_mul(x0, y1, q, qi), mont_mul(x1, y0, q, qi), q);
+  uint64_t m2 = mont_mul(x1, y1, q, qi);
+  const long nh = (long)n * half;
+  uint64_t* d = D + (long)z * half + off;
+  d[0] = mont_mul(m0, P.r2, q, qi);
+  d[nh] = mont_mul(m1, P.r2, q, qi);
+  d[2 * nh] = mont_mul(m2, P.r2, q, qi);
+}
+
+// key products for op z: x limbs (Q part at xq + z*xq_stride, B part at
+// xb + z*xb_stride) times the key; k0 of op z at k + z*k_stride, k1 at
+// k + (n + z)*k_stride.
+__global__ void keyswitch_mul_batch(const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                                    const uint64_t* key, long key_half, uint64_t* k, long k_stride, int n, int nq,
+                                    int K, const PrimeConst* pc, int log_n) {
+  const long N = 1L << log_n;
+  const long c = coef_index();
+  const int l = blockIdx.y, z = blockIdx.z;
+  const int prime = l < nq ? l : K + (l - nq);
+  const uint64_t x = l < nq ? xq[z * xq_stride + (long)l * N + c] : xb[z * xb_stride + (long)(l - nq) * N + c];
+  const PrimeConst& P = pc[prime];
+  const uint64_t kb = key[(long)prime * N + c], ka = key[key_half + (long)prime * N + c];
+  k[z * k_stride + (long)l * N + c] = mul_mod(x, kb, P);
+  k[(n + z) * k_stride + (long)l * N + c] = mul_mod(x, ka, P);
+}
+
 // ---- host wrappers -----------------------------------------------------------
 
 static dim3 ew_grid(const Engine& E, int nlimbs, int npolys) { return dim3(E.N / 256, nlimbs, npolys); }
@@ -154,6 +194,21 @@ void ew_muladd_op(const Engine& E, uint64_t* d, long ds, const uint64_t* a, long
 void tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
                uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st) {
   hmult_tensor<<<ew_grid(E, nlimbs, 1), 256, 0, st>>>(a, b, a_half, b_half, d0, d1, d2, E.d_pc, E.log_n); note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+void tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D, int n, int nlimbs, cudaStream_t st) {
+  hmult_tensor_batch<<<ew_grid(E, nlimbs, n), 256, 0, st>>>(ptr, half, D, n, E.d_pc, E.log_n);
+  note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                            const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st) {
+  const long half = (long)E.nprimes * E.N;
+  keyswitch_mul_batch<<<ew_grid(E, nq + E.kl, n), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
+                                                               n, nq, E.k, E.d_pc, E.log_n);
+  note_launch();
   AOA_CHECK_LAUNCH();
 }
 

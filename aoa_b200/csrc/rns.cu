@@ -275,6 +275,38 @@ __global__ void ks_combine_kernel(uint64_t* out, long out_stride, const uint64_t
   out[p * out_stride + off] = r;
 }
 
+// Same epilogue writing poly p to outp.p[p] (a list of output polys).
+__global__ void ks_combine_ptr_kernel(OutPtrs outp, const uint64_t* base, long base_stride, const uint64_t* k,
+                                      long k_stride, const uint64_t* y, long y_stride, const ShoupW* binv,
+                                      const ShoupW* resc, const PrimeConst* pc, int log_n) {
+  const long N = 1L << log_n;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y, p = blockIdx.z;
+  const long off = (long)i * N + c;
+  const uint64_t q = pc[i].q;
+  const uint64_t kv = k[p * k_stride + off], yv = y[p * y_stride + off];
+  const uint64_t bv = base ? base[p * base_stride + off] : 0;
+  uint64_t r;
+  if (resc) {
+    r = shoup(sub_mod(add_mod(bv, shoup(kv, binv[i], q), q), yv, q), resc[i], q);
+  } else {
+    r = add_mod(bv, shoup(sub_mod(kv, yv, q), binv[i], q), q);
+  }
+  outp.p[p][off] = r;
+}
+
+void ks_combine_ptr(const Engine& E, const OutPtrs& outp, const uint64_t* base, long base_stride, const uint64_t* k,
+                    long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys, int rescale_level,
+                    cudaStream_t st) {
+  if (nlimbs <= 0) return;
+  dim3 grid(E.N / 256, nlimbs, npolys);
+  const ShoupW* resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
+  ks_combine_ptr_kernel<<<grid, 256, 0, st>>>(outp, base, base_stride, k, k_stride, y, y_stride, E.rns.moddown_binv,
+                                              resc, E.d_pc, E.log_n);
+  note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
 void ks_combine(const Engine& E, uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
                 const uint64_t* k, long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys,
                 int rescale_level, cudaStream_t st, int prime0) {

@@ -156,6 +156,13 @@ int aoa_swk_destroy(aoa_ctx* c, aoa_swk* k);
 int aoa_hmult(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
 /* ckks_mul (ckks.cpp:334-347): HMult + relinearise + rescale.                */
 int aoa_hmult_relin_rescale(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
+/* Batched ckks_mul / ckks_mul_without_rescale (rescale != 0 / == 0) of n
+ * independent products out[i] = a[i] * b[i]: operands are grouped by level
+ * and every stage of the pipeline runs as one launch over a group of up to 64
+ * products.  No reference counterpart as one call (the reference runs the
+ * products one ckks_mul at a time); results equal n separate calls.          */
+int aoa_hmult_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b,
+                    const aoa_swk* evk, int rescale);
 /* The reference's per-call ckks_mul sequence (ckks.cpp:273-347 with the
  * poly_t.cpp domain rules: full-base transforms, unfused element-wise ops),
  * on this engine's kernels; same residues as aoa_hmult_relin_rescale, output

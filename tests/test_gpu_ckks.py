@@ -257,3 +257,61 @@ def test_encrypted_hmult_decodes_full_size():
     got = o.decode(m[0], slots, out.scale)
     err = np.abs(got - v1 * v2)
     assert err.max() < 2.0 ** -20, err.max()
+
+
+@pytest.mark.parametrize("rescale", [True, False])
+def test_hmult_batch_matches_single_calls(ref_table, rescale):
+    """Grouped batched HMult (mixed levels, aliased outputs) equals per-call HMult and the oracle."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=17)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(11)
+    N, k = E.N, E.k
+    levels = [4, 2, 4, 3, 2, 4]
+    pairs = [(_rand_ct(rng, Q, N, k), _rand_ct(rng, Q, N, k)) for _ in levels]
+    cts_a, cts_b, outs = [], [], []
+    for (a, b), lv in zip(pairs, levels):
+        ca = aoa.Ciphertext.from_residues(ctx, *a, slots=8, scale=1 << 35, domain=aoa.AOA_NTT)
+        cb = aoa.Ciphertext.from_residues(ctx, *b, slots=8, scale=1 << 36, domain=aoa.AOA_COEF)
+        ca.set(lv, 8, 1 << 35, aoa.AOA_NTT)
+        cb.set(lv, 8, 1 << 36, aoa.AOA_COEF)
+        cts_a.append(ca)
+        cts_b.append(cb)
+    outs = [aoa.Ciphertext(ctx) for _ in levels]
+    outs[1] = cts_a[1]                                   # output aliases an input
+    aoa.ckks_mul_batch(ctx, outs, cts_a, cts_b, evk, rescale=rescale)
+    for z, ((a, b), lv) in enumerate(zip(pairs, levels)):
+        pad = lambda x: np.concatenate([x[: lv + 1], np.zeros((k - lv - 1, N), dtype=np.uint64)])
+        w0, w1, wsc = o.hmult((pad(a[0]), pad(a[1])), (pad(b[0]), pad(b[1])), keys["evk"], lv, 1 << 35, 1 << 36,
+                              rescale=rescale, a_state=ST_NTT, b_state=ST_COEF)
+        nl = lv if rescale else lv + 1
+        g0, g1 = outs[z].download(nlimbs=nl)
+        assert outs[z].level == nl - 1 and outs[z].scale == wsc, z
+        assert np.array_equal(g0, w0[:nl]) and np.array_equal(g1, w1[:nl]), z
+
+
+def test_hmult_batch_full_size_equals_pipeline():
+    """N = 2^16, 30 + 31 primes: batched and per-call pipeline residues agree."""
+    require_gpu()
+    import aoa_b200 as aoa
+    ps = oracle.gen_ntt_primes(60, 1 << 17, 61)
+    E = aoa.Engine(16, ps[:30], ps[30:])
+    ctx = aoa.Context(E)
+    rng = np.random.default_rng(4)
+    N = E.N
+    evk = aoa.SwitchKey(ctx, uniform_residues(rng, ps, N), uniform_residues(rng, ps, N))
+    xs = [(_rand_ct(rng, ps, N, 30), _rand_ct(rng, ps, N, 30)) for _ in range(3)]
+    A = [aoa.Ciphertext.from_residues(ctx, *x[0], slots=4, scale=1 << 50, domain=aoa.AOA_NTT) for x in xs]
+    Bc = [aoa.Ciphertext.from_residues(ctx, *x[1], slots=4, scale=1 << 50, domain=aoa.AOA_NTT) for x in xs]
+    outs = [aoa.Ciphertext(ctx) for _ in xs]
+    aoa.ckks_mul_batch(ctx, outs, A, Bc, evk)
+    for z, x in enumerate(xs):
+        a1 = aoa.Ciphertext.from_residues(ctx, *x[0], slots=4, scale=1 << 50, domain=aoa.AOA_NTT)
+        b1 = aoa.Ciphertext.from_residues(ctx, *x[1], slots=4, scale=1 << 50, domain=aoa.AOA_NTT)
+        o1 = aoa.Ciphertext(ctx)
+        aoa.ckks_mul(ctx, o1, a1, b1, evk)
+        g = outs[z].download(nlimbs=29, domain=aoa.AOA_NTT)
+        w = o1.download(nlimbs=29, domain=aoa.AOA_NTT)
+        assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
