@@ -160,18 +160,13 @@ static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long hal
 // merged with the rescale (one forward transform per output limb).  The
 // result is left in the transform domain (the reference leaves coefficients;
 // the residues of every live limb are the same after a domain change).
-void hmult(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool do_rescale) {
+static void hmult_core(Ctx& C, const Workspace& w, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk,
+                       bool do_rescale) {
   const Engine& E = *C.E;
   const long N = E.N;
-  if (a->level == 0 || b->level == 0)
-    throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
-  if (a->slots != b->slots) throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
-  if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
-  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
   const int level = std::min(a->level, b->level);
   const int m = level + 1;
   const long half = (long)E.k * N;
-  Workspace w = get_ws(C);
   // operands to the transform domain, in place (poly_mul does the same, poly_t.cpp:201-220)
   to_domain(C, a, AOA_NTT, a->level + 1);
   if (b != a) to_domain(C, b, AOA_NTT, b->level + 1);
@@ -188,6 +183,26 @@ void hmult(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool d
   out->slots = slots;
   out->scale = scale_after_mult(E, sa, sb, level);
   out->domain = AOA_NTT;
+}
+
+static void hmult_check(const Engine& E, const aoa_ct* a, const aoa_ct* b, const aoa_swk* evk) {
+  if (a->level == 0 || b->level == 0)
+    throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
+  if (a->slots != b->slots) throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
+  if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
+  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
+}
+
+void hmult(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool do_rescale) {
+  hmult_check(*C.E, a, b, evk);
+  hmult_core(C, get_ws(C), out, a, b, evk, do_rescale);
+}
+
+// Same pipeline on caller-provided scratch of workspace_words(E) words.
+void hmult_with_scratch(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk, bool do_rescale,
+                        uint64_t* scratch) {
+  hmult_check(*C.E, a, b, evk);
+  hmult_core(C, carve(*C.E, scratch), out, a, b, evk, do_rescale);
 }
 
 // Galois automorphism X -> X^g followed by the key switch with `key`
