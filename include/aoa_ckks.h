@@ -168,6 +168,18 @@ int aoa_hmult_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* a, aoa
  * on this engine's kernels; same residues as aoa_hmult_relin_rescale, output
  * in coefficients.  The plain per-call baseline of the benchmarks.           */
 int aoa_hmult_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
+/* HMult + relinearise + rescale that allocates nothing.  No counterpart in the
+ * reference.  For callers that may not allocate device memory while they
+ * evaluate (an application that owns the whole device memory budget through
+ * its own allocator; a serving thread that cannot risk the device
+ * synchronisation and driver lock of cudaMalloc / cudaFree): the same kernels
+ * as aoa_hmult_relin_rescale, with their workspace in a fixed 32 MiB device
+ * array built into the library (held by every device that loads it until the
+ * process exits).  Parameter sets needing more workspace fail with
+ * AOA_ERR_BAD_PARAM.  The first call on a device looks the array up (make it
+ * with the engine's device current and before any stream capture).  All calls
+ * share the one array: calls whose work overlaps on the GPU race.            */
+int aoa_hmult_relin_rescale_noalloc(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
 /* ckks_rescale (ckks.cpp:220-230) */
 int aoa_rescale(aoa_ctx* c, aoa_ct* ct);
 /* ckks_add / ckks_sub (ckks.cpp:232-271) */
