@@ -10,9 +10,9 @@ import ctypes
 import numpy as np
 
 from . import capi
-from .capi import AoaError, AOA_COEF, AOA_NTT
+from .capi import AoaError, AOA_COEF, AOA_NTT, AOA_DGT
 
-__all__ = ["Engine", "Context", "DeviceArray", "AoaError", "AOA_COEF", "AOA_NTT"]
+__all__ = ["Engine", "Context", "DeviceArray", "AoaError", "AOA_COEF", "AOA_NTT", "AOA_DGT"]
 
 
 class Engine:
@@ -22,7 +22,7 @@ class Engine:
     src/cuda/manager.cu:762-800) with explicit prime lists.
     """
 
-    def __init__(self, log_n, q_primes, b_primes, scale_bits=0, generators=None):
+    def __init__(self, log_n, q_primes, b_primes, scale_bits=0, generators=None, dgt_roots=None):
         lib = capi.load()
         self.log_n, self.N = log_n, 1 << log_n
         self.q_primes = [int(q) for q in q_primes]
@@ -36,6 +36,9 @@ class Engine:
         p.primes = self._primes_arr.ctypes.data_as(capi.u64p)
         p.generators = None if self._gens_arr is None else self._gens_arr.ctypes.data_as(capi.u64p)
         p.scale_bits, p.dnum = scale_bits, 1
+        self._roots_arr = None if dgt_roots is None else np.array([int(v) for r in dgt_roots for v in r],
+                                                                   dtype=np.uint64)
+        p.dgt_roots = None if self._roots_arr is None else self._roots_arr.ctypes.data_as(capi.u64p)
         self.scale_bits = scale_bits
         h = ctypes.c_void_p()
         capi.check(lib.aoa_engine_create(ctypes.byref(p), ctypes.byref(h)))
@@ -100,6 +103,19 @@ class Context:
     def ntt_inv(self, d, npolys, first_prime, nlimbs, poly_stride=None):
         capi.check(capi.load().aoa_ntt_inv(self.handle, d.ptr, npolys, first_prime, nlimbs,
                                            poly_stride or nlimbs))
+
+    def dgt_fwd(self, d, npolys, first_prime, nlimbs, poly_stride=None):
+        """DGT of planar GI limbs (DGTEngine::execute_dgt FORWARD)."""
+        capi.check(capi.load().aoa_dgt_fwd(self.handle, d.ptr, npolys, first_prime, nlimbs,
+                                           poly_stride or nlimbs))
+
+    def dgt_inv(self, d, npolys, first_prime, nlimbs, poly_stride=None):
+        capi.check(capi.load().aoa_dgt_inv(self.handle, d.ptr, npolys, first_prime, nlimbs,
+                                           poly_stride or nlimbs))
+
+    def set_transform(self, domain):
+        """AOA_NTT (aoa-ntt) or AOA_DGT (aoa-dgt) for this context's evaluations."""
+        capi.check(capi.load().aoa_ctx_set_transform(self.handle, domain))
 
 
 class DeviceArray:
@@ -205,13 +221,37 @@ class Ciphertext:
 class SwitchKey:
     """SwitchKey {b, a} over the QB basis (relinearisation, rotation or conjugation key)."""
 
-    def __init__(self, ctx, b, a, domain=AOA_NTT):
+    def __init__(self, ctx, b, a, domain=AOA_NTT, handle=None):
         self.ctx = ctx
+        if handle is not None:
+            self.handle = handle
+            return
         b = np.ascontiguousarray(b, dtype=np.uint64)
         a = np.ascontiguousarray(a, dtype=np.uint64)
         h = ctypes.c_void_p()
         capi.check(capi.load().aoa_swk_create(ctx.handle, capi.ptr(b), capi.ptr(a), domain, ctypes.byref(h)))
         self.handle = h
+
+    @classmethod
+    def generate(cls, ctx, s1, s2, a, e, a_domain=AOA_COEF):
+        """Switching key for s1 under s2 (b = rho(s1) + e - a s2, a) from given
+        draws; s1 / s2 / a are [k+kl][N] device arrays (s1 may be None), e a
+        device array of N int64 (ckks_new_evk & co., ckkskeys.cpp:101-191)."""
+        h = ctypes.c_void_p()
+        capi.check(capi.load().aoa_swk_generate(ctx.handle, None if s1 is None else s1.ptr, s2.ptr, a.ptr, a_domain,
+                                                e.ptr, ctypes.byref(h)))
+        return cls(ctx, None, None, handle=h)
+
+    def numpy(self):
+        """(b, a, domain) copied to the host."""
+        d = ctypes.c_void_p()
+        dom = ctypes.c_int()
+        capi.check(capi.load().aoa_swk_data(self.handle, ctypes.byref(d), ctypes.byref(dom)))
+        E = self.ctx.engine
+        out = np.empty((2, len(E.primes), E.N), dtype=np.uint64)
+        capi.check(capi.load().aoa_memcpy_d2h(self.ctx.handle, capi.ptr(out), d, out.nbytes))
+        self.ctx.sync()
+        return out[0], out[1], dom.value
 
     def close(self):
         if getattr(self, "handle", None) and self.ctx.handle:
@@ -309,3 +349,110 @@ def ckks_mul_batch(ctx, outs, c1s, c2s, evk, rescale=True):
     a = arr(*[x.handle.value for x in c1s])
     b = arr(*[x.handle.value for x in c2s])
     capi.check(capi.load().aoa_hmult_batch(ctx.handle, n, o, a, b, _h(evk), 1 if rescale else 0))
+
+
+# ---- encoder and encryption (aoa-ntt src/ckks/encoder.cu, ckks.cpp:87-192) --------
+
+def ckks_encode(ctx, values, empty_slots=0, scale=None, nlimbs=None, domain=AOA_COEF, out=None):
+    """Encode complex `values` (+ `empty_slots` zeros) into a [nlimbs][N] device
+    polynomial (CKKSContext::encode, ckkscontext.cpp:5-19).  Returns (poly, scale)."""
+    eng = ctx.engine
+    if scale is None:
+        scale = 1 << eng.scale_bits
+    nlimbs = nlimbs or eng.k
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.complex128))
+    out = out if out is not None else ctx.alloc((nlimbs, eng.N))
+    capi.check(capi.load().aoa_encode(ctx.handle, capi.ptr(v) if v.size else None, v.size, empty_slots,
+                                      int(scale), nlimbs, domain, out.ptr))
+    return out, int(scale)
+
+
+def ckks_decode(ctx, poly, slots, scale, domain=AOA_COEF):
+    """Decode `slots` complex values from limb 0 of a device polynomial
+    (CKKSContext::decode, ckkscontext.cpp:21-38)."""
+    out = np.empty(slots, dtype=np.complex128)
+    capi.check(capi.load().aoa_decode(ctx.handle, poly.ptr, domain, slots, int(scale), capi.ptr(out)))
+    return out
+
+
+def ckks_encrypt(ctx, values, pk, u, e1, e2, empty_slots=0, scale=None, out=None):
+    """Encode and encrypt (ckks_encrypt, ckks.cpp:109-128) with the sampler's
+    draws given: u (ternary), e1, e2 (Gaussian) as N signed integers each."""
+    m, scale = ckks_encode(ctx, values, empty_slots, scale)
+    dv = [ctx.upload(np.ascontiguousarray(x, dtype=np.int64)) for x in (u, e1, e2)]
+    out = out if out is not None else Ciphertext(ctx)
+    slots = len(values) + empty_slots
+    capi.check(capi.load().aoa_encrypt(ctx.handle, out.handle, m.ptr, AOA_COEF, pk.handle, dv[0].ptr, dv[1].ptr,
+                                       dv[2].ptr, slots, int(scale)))
+    ctx.sync()
+    return out
+
+
+def ckks_decrypt_poly(ctx, ct, sk, sk_domain=AOA_COEF):
+    """m = c1 s + c0 (ckks_decrypt_poly, ckks.cpp:179-192) as a device array
+    [level+1][N] in coefficients; sk is a [k][N] device array."""
+    m = ctx.alloc((ct.level + 1, ctx.engine.N))
+    capi.check(capi.load().aoa_decrypt(ctx.handle, ct.handle, sk.ptr, sk_domain, m.ptr))
+    return m
+
+
+def ckks_decrypt(ctx, ct, sk, sk_domain=AOA_COEF):
+    """Decrypt and decode (ckks_decrypt, ckks.cpp:195-215)."""
+    m = ckks_decrypt_poly(ctx, ct, sk, sk_domain)
+    return ckks_decode(ctx, m, ct.slots, ct.scale)
+
+
+# ---- key generation (CKKSKeychain, aoa-ntt src/ckks/ckkskeys.cpp:20-191) ----------
+
+def galois_left(N, r):
+    """Galois element of a left rotation by r slots: 5^r mod 2N."""
+    return pow(5, r % (N // 2), 2 * N)
+
+
+def galois_conjugate(N):
+    return 2 * N - 1
+
+
+def ckks_pk_generate(ctx, s, a, e, a_domain=AOA_COEF, out=None):
+    """Public key (e - a s, a) over Q as a ciphertext (ckks_new_pk); s, a: [k][N]
+    device arrays, e: device array of N int64."""
+    out = out if out is not None else Ciphertext(ctx)
+    capi.check(capi.load().aoa_pk_generate(ctx.handle, out.handle, s.ptr, a.ptr, a_domain, e.ptr))
+    return out
+
+
+def ckks_secret_square(ctx, s, nlimbs):
+    out = ctx.alloc((nlimbs, ctx.engine.N))
+    capi.check(capi.load().aoa_secret_square(ctx.handle, s.ptr, out.ptr, nlimbs))
+    return out
+
+
+def ckks_secret_galois(ctx, s, galois, nlimbs):
+    out = ctx.alloc((nlimbs, ctx.engine.N))
+    capi.check(capi.load().aoa_secret_galois(ctx.handle, s.ptr, out.ptr, int(galois), nlimbs))
+    return out
+
+
+def ckks_keygen(ctx, s, draws, rotations=(), conjugation=False):
+    """All keys of a secret s ([k+kl][N] device residues, coefficients) from the
+    sampler draws `draws` (a dict of device arrays: "pk": (a, e), "evk": (a, e),
+    ("rtk", r): (a, e), "cjk": (a, e); a uniform [k+kl][N], e N int64), on the
+    device (ckks_new_keys, ckkskeys.cpp:20-73).  Returns a dict of keys."""
+    E = ctx.engine
+    nqb = len(E.primes)
+    keys = {}
+    a, e = draws["pk"]
+    keys["pk"] = ckks_pk_generate(ctx, s, a, e)
+    s2 = ckks_secret_square(ctx, s, nqb)
+    a, e = draws["evk"]
+    keys["evk"] = SwitchKey.generate(ctx, s2, s, a, e)
+    keys["rtk"] = {}
+    for r in rotations:
+        sr = ckks_secret_galois(ctx, s, galois_left(E.N, r), nqb)
+        a, e = draws[("rtk", r)]
+        keys["rtk"][r] = SwitchKey.generate(ctx, sr, s, a, e)
+    if conjugation:
+        sc = ckks_secret_galois(ctx, s, galois_conjugate(E.N), nqb)
+        a, e = draws["cjk"]
+        keys["cjk"] = SwitchKey.generate(ctx, sc, s, a, e)
+    return keys

@@ -39,7 +39,7 @@ def build(force=False, verbose=False, jobs=None):
         objs.append(obj)
         cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [NVCC] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
+            cmd = [NVCC] + ARCH + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((subprocess.Popen(cmd), cmd))

@@ -25,7 +25,7 @@ STATUS = {
     5: "AOA_ERR_CUDA", 6: "AOA_ERR_TIMEOUT", 7: "AOA_ERR_SLOT_MISMATCH", 8: "AOA_ERR_NOT_INITIALIZED",
     9: "AOA_ERR_NO_DEVICE",
 }
-AOA_COEF, AOA_NTT = 1, 2
+AOA_COEF, AOA_NTT, AOA_DGT = 1, 2, 3
 
 
 class AoaError(RuntimeError):
@@ -37,7 +37,7 @@ class AoaError(RuntimeError):
 
 class Params(ctypes.Structure):
     _fields_ = [("log_n", c_int), ("k", c_int), ("kl", c_int), ("primes", u64p),
-                ("generators", u64p), ("scale_bits", c_int), ("dnum", c_int)]
+                ("generators", u64p), ("scale_bits", c_int), ("dnum", c_int), ("dgt_roots", u64p)]
 
 
 # name -> (restype, argtypes); every function returns an aoa_status unless noted
@@ -85,6 +85,23 @@ SIGNATURES = {
     "aoa_sub": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_rotate": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "aoa_conjugate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_encode": (c_int, [c_void_p, c_void_p, c_int, c_int, c_u64, c_int, c_int, c_void_p]),
+    "aoa_decode": (c_int, [c_void_p, c_void_p, c_int, c_int, c_u64, c_void_p]),
+    "aoa_encrypt": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                            c_u64]),
+    "aoa_decrypt": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "aoa_dgt_fwd": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int]),
+    "aoa_dgt_inv": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int]),
+    "aoa_gi_mul": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int]),
+    "aoa_gi_to_planar": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "aoa_gi_from_planar": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "aoa_engine_dgt_roots": (c_int, [c_void_p, c_void_p]),
+    "aoa_ctx_set_transform": (c_int, [c_void_p, c_int]),
+    "aoa_swk_data": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "aoa_swk_generate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "aoa_pk_generate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "aoa_secret_square": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "aoa_secret_galois": (c_int, [c_void_p, c_void_p, c_void_p, c_long, c_int]),
 }
 
 _lib = None

@@ -76,6 +76,24 @@ struct Engine {
   // Device error word: kernels OR in kErr* bits instead of trapping (a bounded
   // wait that expired, ...); aoa_ctx_sync reads and clears it.
   unsigned* d_err = nullptr;
+  // Encoder tables: ksi[j] = exp(2 pi i j / M) for j <= M = 2N, as FP64 pairs
+  // computed on the host; rot[j] = 5^j mod M for j < N/2.
+  double2* d_ksi = nullptr;
+  uint32_t* d_rot = nullptr;
+  // DGT (folded Gaussian-integer transform of length N/2): cyclic merged
+  // tables per prime, constants with N/2 inverses, and the twist by powers of
+  // a root r of i (r^(N/2) = i) split as r^n = r^(n mod L) * r^(L floor(n/L)):
+  // GI entries {re, re', im, im'} (Shoup companions), [nprimes][L] and
+  // [nprimes][N/2/L], forward (r) and inverse (r^-1).
+  std::vector<uint64_t> dgt_roots;   // 2 per prime (re, im of r)
+  ShoupW* d_dtw = nullptr;
+  ShoupW* d_ditw = nullptr;
+  PrimeConst* d_dpc = nullptr;
+  uint64_t* d_twist_lo = nullptr;
+  uint64_t* d_twist_hi = nullptr;
+  uint64_t* d_untwist_lo = nullptr;
+  uint64_t* d_untwist_hi = nullptr;
+  int dgt_log_lo = 0;
   std::vector<void*> allocations;
 };
 
@@ -91,6 +109,9 @@ struct Ctx {
   size_t batch_bytes = 0;
   void* conv = nullptr;         // domain-conversion buffer for downloads
   size_t conv_bytes = 0;
+  void* enc = nullptr;          // encoder / key generation buffer
+  size_t enc_bytes = 0;
+  int transform = AOA_NTT;      // transform domain of this context's evaluations (AOA_NTT / AOA_DGT)
 };
 
 // Per-launch pointer lists for batched kernels (passed by value).
@@ -124,7 +145,19 @@ int guarded(F&& f) {
 }
 
 // ntt.cu
+// A family of limb transforms: merged Cooley-Tukey tables ([nprimes][2^log_n]
+// forward / inverse with Shoup companions) and per-prime constants.
+struct NttTables {
+  const ShoupW* tw = nullptr;
+  const ShoupW* itw = nullptr;
+  const PrimeConst* pc = nullptr;
+  int log_n = 0;
+  int prime_shift = 0;     // limb l uses prime first + (l >> prime_shift)
+  bool lazy = false;
+};
 void ntt_init(Engine& E);
+void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int npolys, int first_prime, int nlimbs,
+                      long poly_stride, bool forward, cudaStream_t st);
 void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
                long poly_stride, bool forward, cudaStream_t st);
 
@@ -143,6 +176,22 @@ void rescale_corrections(const Engine& E, const uint64_t* in_b, long in_stride, 
 void ks_combine(const Engine& E, uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
                 const uint64_t* k, long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys,
                 int rescale_level, cudaStream_t st, int prime0 = 0);
+
+// dgt.cu: folded Gaussian-integer transform.  A GI limb is N words: the
+// real plane (N/2) then the imaginary plane (N/2), which is also the
+// coefficient layout of the unfolded polynomial (a_j, a_{j+N/2}).
+void dgt_init(Engine& E, const uint64_t* roots);
+void dgt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs, long poly_stride,
+               bool forward, cudaStream_t st);
+void gi_mul_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as, const uint64_t* b, long bs,
+               int prime0, int nlimbs, int npolys, cudaStream_t st);
+void gi_tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
+                  uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st);
+void gi_keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
+                         uint64_t* k1, int nq, cudaStream_t st);
+// ckks.cu: limb transforms of a kind (AOA_NTT / AOA_DGT) and domain changes
+void xform(const Engine& E, int kind, uint64_t* d, int npolys, int first_prime, int nlimbs, long stride, bool fwd,
+           cudaStream_t st);
 
 // ops.cu  (op: 0 add, 1 sub, 2 mul, 3 neg)
 void ew_binary_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as, const uint64_t* b, long bs,
@@ -176,6 +225,23 @@ uint64_t h_shoup_companion(uint64_t w, uint64_t q);
 int h_search_primes(int bits, uint64_t modulus, int count, uint64_t* out);
 
 }  // namespace aoa
+
+// Ciphertext (cipher_t, aoa-ntt include/newckks/ckks/cipher_t.h:17-22):
+// d = [c0 | c1], each k limbs of N words.
+struct aoa_ct {
+  uint64_t* d = nullptr;
+  int level = 0;
+  int slots = 0;
+  uint64_t scale = 0;
+  int domain = AOA_COEF;
+};
+
+// Switching key (SwitchKey, aoa-ntt include/newckks/defines.h:85-90):
+// d = [b | a], each k + kl limbs, in the transform domain `domain`.
+struct aoa_swk {
+  uint64_t* d = nullptr;
+  int domain = AOA_NTT;     // AOA_NTT or AOA_DGT
+};
 
 struct aoa_engine { aoa::Engine e; };
 struct aoa_ctx { aoa::Ctx c; };

@@ -12,22 +12,6 @@
 
 using namespace aoa;
 
-// Ciphertext (cipher_t, aoa-ntt include/newckks/ckks/cipher_t.h:17-22):
-// d = [c0 | c1], each k limbs of N words.
-struct aoa_ct {
-  uint64_t* d = nullptr;
-  int level = 0;
-  int slots = 0;
-  uint64_t scale = 0;
-  int domain = AOA_COEF;
-};
-
-// Switching key (SwitchKey, aoa-ntt include/newckks/defines.h:85-90):
-// d = [b | a], each k + kl limbs, transform domain.
-struct aoa_swk {
-  uint64_t* d = nullptr;
-};
-
 namespace aoa {
 
 // Workspace for one key switch / HMult at the engine's largest level (words):
@@ -77,12 +61,24 @@ static Workspace get_ws(Ctx& C) {
   return carve(*C.E, (uint64_t*)C.scratch);
 }
 
-static void to_domain(Ctx& C, aoa_ct* ct, int domain, int nlimbs) {
+// Limb transforms of the given kind (AOA_NTT: negacyclic NTT of aoa-ntt;
+// AOA_DGT: folded Gaussian-integer DGT of aoa-dgt) on [npolys][stride][N].
+void xform(const Engine& E, int kind, uint64_t* d, int npolys, int first_prime, int nlimbs, long stride, bool fwd,
+           cudaStream_t st) {
+  if (kind == AOA_DGT) dgt_batch(E, d, npolys, first_prime, nlimbs, stride, fwd, st);
+  else ntt_batch(E, d, npolys, first_prime, nlimbs, stride, fwd, st);
+}
+
+// Brings limbs 0..nlimbs-1 of both polys of ct to `domain` in place.
+void ct_to_domain(Ctx& C, aoa_ct* ct, int domain, int nlimbs) {
   const Engine& E = *C.E;
   if (ct->domain == domain) return;
-  ntt_batch(E, ct->d, 2, 0, nlimbs, E.k, domain == AOA_NTT, C.stream);
+  if (ct->domain != AOA_COEF) xform(E, ct->domain, ct->d, 2, 0, nlimbs, E.k, false, C.stream);
+  if (domain != AOA_COEF) xform(E, domain, ct->d, 2, 0, nlimbs, E.k, true, C.stream);
   ct->domain = domain;
 }
+
+static void to_domain(Ctx& C, aoa_ct* ct, int domain, int nlimbs) { ct_to_domain(C, ct, domain, nlimbs); }
 
 static void copy_limbs(Ctx& C, uint64_t* dst, const uint64_t* src, long words) {
   AOA_CUDA(cudaMemcpyAsync(dst, src, (size_t)words * 8, cudaMemcpyDeviceToDevice, C.stream));
@@ -97,10 +93,13 @@ static void keyswitch_core(Ctx& C, const Workspace& w, const uint64_t* x_coef, c
   const Engine& E = *C.E;
   const long N = E.N;
   const int m = level + 1;
+  const int tk = C.transform;
+  if (key->domain != tk) throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
   modup(E, x_coef, 0, w.UB, 0, 1, level, C.stream);
-  ntt_batch(E, w.UB, 1, E.k, E.kl, E.kl, true, C.stream);
-  keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + (long)(E.k + E.kl) * N, m, C.stream);
-  ntt_batch(E, w.KS + (long)m * N, 2, E.k, E.kl, E.k + E.kl, false, C.stream);
+  xform(E, tk, w.UB, 1, E.k, E.kl, E.kl, true, C.stream);
+  if (tk == AOA_DGT) gi_keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + (long)(E.k + E.kl) * N, m, C.stream);
+  else keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + (long)(E.k + E.kl) * N, m, C.stream);
+  xform(E, tk, w.KS + (long)m * N, 2, E.k, E.kl, E.k + E.kl, false, C.stream);
 }
 
 static uint64_t scale_after_mult(const Engine& E, uint64_t sa, uint64_t sb, int level) {
@@ -132,9 +131,9 @@ static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long hal
       ks_combine(E, U + N, 0, b1 ? b1 + (long)level * N : nullptr, 0, w.KS + ks_stride + (long)level * N, 0,
                  nullptr, 0, 1, 1, 0, C.stream, level);
     }
-    ntt_batch(E, U, 2, level, 1, 1, false, C.stream);
+    xform(E, C.transform, U, 2, level, 1, 1, false, C.stream);
     rescale_corrections(E, kb, ks_stride, U, N, w.CL, N, w.Y, (long)E.k * N, 2, level, C.stream);
-    ntt_batch(E, w.Y, 2, 0, level, E.k, true, C.stream);
+    xform(E, C.transform, w.Y, 2, 0, level, E.k, true, C.stream);
     if (b0 && b1 == b0 + half) {
       ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, level, 2, level, C.stream);
     } else {
@@ -143,7 +142,7 @@ static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long hal
     }
   } else {
     moddown_conv(E, kb, ks_stride, w.Y, (long)E.k * N, 2, m, C.stream);
-    ntt_batch(E, w.Y, 2, 0, m, E.k, true, C.stream);
+    xform(E, C.transform, w.Y, 2, 0, m, E.k, true, C.stream);
     if (b0 && b1 == b0 + half) {
       ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, m, 2, 0, C.stream);
     } else {
@@ -168,21 +167,23 @@ static void hmult_core(Ctx& C, const Workspace& w, aoa_ct* out, aoa_ct* a, aoa_c
   const int m = level + 1;
   const long half = (long)E.k * N;
   // operands to the transform domain, in place (poly_mul does the same, poly_t.cpp:201-220)
-  to_domain(C, a, AOA_NTT, a->level + 1);
-  if (b != a) to_domain(C, b, AOA_NTT, b->level + 1);
+  const int tk = C.transform;
+  to_domain(C, a, tk, a->level + 1);
+  if (b != a) to_domain(C, b, tk, b->level + 1);
   uint64_t* D0 = w.D;
   uint64_t* D2 = w.D + 2 * half;
-  tensor_op(E, a->d, half, b->d, half, D0, D0 + half, D2, m, C.stream);
+  if (tk == AOA_DGT) gi_tensor_op(E, a->d, half, b->d, half, D0, D0 + half, D2, m, C.stream);
+  else tensor_op(E, a->d, half, b->d, half, D0, D0 + half, D2, m, C.stream);
   const uint64_t sa = a->scale, sb = b->scale;
   const int slots = a->slots;
   copy_limbs(C, w.T, D2, (long)m * N);
-  ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  xform(E, tk, w.T, 1, 0, m, m, false, C.stream);
   keyswitch_core(C, w, w.T, D2, evk, level);
   keyswitch_finish(C, w, out->d, half, D0, D0 + half, level, do_rescale);
   out->level = do_rescale ? level - 1 : level;
   out->slots = slots;
   out->scale = scale_after_mult(E, sa, sb, level);
-  out->domain = AOA_NTT;
+  out->domain = tk;
 }
 
 static void hmult_check(const Engine& E, const aoa_ct* a, const aoa_ct* b, const aoa_swk* evk) {
@@ -217,20 +218,33 @@ void apply_galois(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* k
   const int level = in->level, m = level + 1;
   const long half = (long)E.k * N;
   Workspace w = get_ws(C);
-  to_domain(C, in, AOA_NTT, m);
   uint64_t* X = w.D + 2 * half;
-  automorph_ntt_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
-  automorph_ntt_op(E, X, in->d + half, 0, galois, m, 1, C.stream);
   const int slots = in->slots;
   const uint64_t scale = in->scale;
-  copy_limbs(C, w.T, X, (long)m * N);
-  ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  const int tk = C.transform;
+  if (tk == AOA_DGT) {
+    // Galois maps do not permute the DGT's evaluation points: apply X -> X^g
+    // to the coefficients (as the reference does, aoa-dgt src/tool/encoder.cu:
+    // 338-470) and transform the results.
+    to_domain(C, in, AOA_COEF, m);
+    automorph_coef_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
+    automorph_coef_op(E, w.T, in->d + half, 0, galois, m, 1, C.stream);
+    copy_limbs(C, X, w.T, (long)m * N);
+    xform(E, tk, X, 1, 0, m, m, true, C.stream);
+    xform(E, tk, w.R0, 1, 0, m, m, true, C.stream);
+  } else {
+    to_domain(C, in, AOA_NTT, m);
+    automorph_ntt_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
+    automorph_ntt_op(E, X, in->d + half, 0, galois, m, 1, C.stream);
+    copy_limbs(C, w.T, X, (long)m * N);
+    ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+  }
   keyswitch_core(C, w, w.T, X, key, level);
   keyswitch_finish(C, w, out->d, half, w.R0, nullptr, level, false);
   out->level = level;
   out->slots = slots;
   out->scale = scale;
-  out->domain = AOA_NTT;
+  out->domain = tk;
 }
 
 // Batched HMult (+ relinearise + rescale) of n <= kMaxBatch independent
@@ -316,6 +330,8 @@ static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* 
 void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b, const aoa_swk* evk,
                  bool do_rescale) {
   const Engine& E = *C.E;
+  if (C.transform != AOA_NTT || (evk && evk->domain != AOA_NTT))
+    throw AoaError(AOA_ERR_BAD_PARAM, "batched HMult runs on the NTT transform only");
   if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
   if (n == 0) return;
   if (!out || !a || !b) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
@@ -367,6 +383,10 @@ void hmult_plain(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) 
     throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
   if (a->slots != b->slots) throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
   if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
+  if (C.transform != AOA_NTT || evk->domain != AOA_NTT)
+    throw AoaError(AOA_ERR_BAD_PARAM, "the reference-structured path runs on the NTT transform only");
+  if (a->domain == AOA_DGT) to_domain(C, a, AOA_COEF, a->level + 1);
+  if (b->domain == AOA_DGT) to_domain(C, b, AOA_COEF, b->level + 1);
   const int k = E.k, nqb = E.k + E.kl;
   const int level = std::min(a->level, b->level);
   const long half = (long)k * N, qb = (long)nqb * N;
@@ -460,7 +480,7 @@ int aoa_ct_destroy(aoa_ctx* c, aoa_ct* ct) {
 }
 
 int aoa_ct_set(aoa_ct* ct, int level, int slots, uint64_t scale, int domain) {
-  if (!ct || (domain != AOA_COEF && domain != AOA_NTT)) return fail(AOA_ERR_BAD_PARAM, "bad argument");
+  if (!ct || (domain != AOA_COEF && domain != AOA_NTT && domain != AOA_DGT)) return fail(AOA_ERR_BAD_PARAM, "bad argument");
   ct->level = level; ct->slots = slots; ct->scale = scale; ct->domain = domain;
   return AOA_OK;
 }
@@ -486,6 +506,7 @@ int aoa_ct_upload(aoa_ctx* c, aoa_ct* ct, const uint64_t* host, int nlimbs, int 
   return guarded([&] {
     const Engine& E = *c->c.E;
     if (nlimbs < 1 || nlimbs > E.k) throw AoaError(AOA_ERR_BAD_PARAM, "nlimbs out of range");
+    if (domain != AOA_COEF && domain != AOA_NTT && domain != AOA_DGT) throw AoaError(AOA_ERR_BAD_PARAM, "bad domain");
     const size_t limb = (size_t)E.N * 8;
     for (int p = 0; p < 2; p++)
       AOA_CUDA(cudaMemcpyAsync(ct->d + (size_t)p * E.k * E.N, host + (size_t)p * nlimbs * E.N, nlimbs * limb,
@@ -502,6 +523,7 @@ int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, in
     Ctx& C = c->c;
     const Engine& E = *C.E;
     if (nlimbs < 1 || nlimbs > E.k) throw AoaError(AOA_ERR_BAD_PARAM, "nlimbs out of range");
+    if (domain != AOA_COEF && domain != AOA_NTT && domain != AOA_DGT) throw AoaError(AOA_ERR_BAD_PARAM, "bad domain");
     const size_t limb = (size_t)E.N * 8;
     const uint64_t* src = ct->d;
     uint64_t* tmp = nullptr;
@@ -515,7 +537,8 @@ int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, in
       tmp = (uint64_t*)C.conv;
       AOA_CUDA(cudaMemcpy2DAsync(tmp, E.k * limb, ct->d, E.k * limb, nlimbs * limb, 2, cudaMemcpyDeviceToDevice,
                                  C.stream));
-      ntt_batch(E, tmp, 2, 0, nlimbs, E.k, domain == AOA_NTT, C.stream);
+      if (ct->domain != AOA_COEF) xform(E, ct->domain, tmp, 2, 0, nlimbs, E.k, false, C.stream);
+      if (domain != AOA_COEF) xform(E, domain, tmp, 2, 0, nlimbs, E.k, true, C.stream);
       src = tmp;
     }
     for (int p = 0; p < 2; p++)
@@ -528,6 +551,7 @@ int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, in
 // Switching key from host residues b, a ([k+kl][N] each) in `domain`.
 int aoa_swk_create(aoa_ctx* c, const uint64_t* host_b, const uint64_t* host_a, int domain, aoa_swk** out) {
   if (!c || !host_b || !host_a || !out) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  if (domain != AOA_COEF && domain != AOA_NTT && domain != AOA_DGT) return fail(AOA_ERR_BAD_PARAM, "bad domain");
   return guarded([&] {
     Ctx& C = c->c;
     const Engine& E = *C.E;
@@ -540,10 +564,19 @@ int aoa_swk_create(aoa_ctx* c, const uint64_t* host_b, const uint64_t* host_a, i
     }
     AOA_CUDA(cudaMemcpyAsync(k->d, host_b, half * 8, cudaMemcpyHostToDevice, C.stream));
     AOA_CUDA(cudaMemcpyAsync(k->d + half, host_a, half * 8, cudaMemcpyHostToDevice, C.stream));
-    if (domain == AOA_COEF) ntt_batch(E, k->d, 2, 0, E.nprimes, E.nprimes, true, C.stream);
+    // a coefficient-domain key goes to the context's transform domain
+    k->domain = domain == AOA_COEF ? C.transform : domain;
+    if (domain == AOA_COEF) xform(E, k->domain, k->d, 2, 0, E.nprimes, E.nprimes, true, C.stream);
     AOA_CUDA(cudaStreamSynchronize(C.stream));
     *out = k;
   });
+}
+
+int aoa_swk_data(aoa_swk* k, uint64_t** device_ptr, int* domain) {
+  if (!k || !device_ptr) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  *device_ptr = k->d;
+  if (domain) *domain = k->domain;
+  return AOA_OK;
 }
 
 int aoa_swk_destroy(aoa_ctx* c, aoa_swk* k) {

@@ -84,6 +84,28 @@ static void build_prime_tables(Engine& E) {
   E.d_err = dev_upload(E, std::vector<unsigned>(1, 0u));
 }
 
+// Encoder tables (the reference computes them on the host per call,
+// aoa-ntt src/ckks/encoder.cu:33-124).  ksi[j] = (cos(2 pi j / M), sin(2 pi j / M))
+// with M = 2N, evaluated by the host libm exactly as written so that the
+// device FFT uses the same doubles; rot[j] = 5^j mod M.
+static void build_encoder_tables(Engine& E) {
+  const long M = 2 * E.N;
+  std::vector<double2> ksi(M + 1);
+  for (long j = 0; j < M; ++j) {
+    const double angle = 2.0 * M_PI * j / M;
+    ksi[j] = make_double2(cos(angle), sin(angle));
+  }
+  ksi[M] = ksi[0];
+  std::vector<uint32_t> rot(std::max<long>(1, E.N / 2));
+  uint64_t v = 1;
+  for (long j = 0; j < E.N / 2; ++j) {
+    rot[j] = (uint32_t)v;
+    v = (v * 5) % (uint64_t)M;
+  }
+  E.d_ksi = dev_upload(E, ksi);
+  E.d_rot = dev_upload(E, rot);
+}
+
 // Basis-conversion and rescale constants (manager.cu:566-759).
 static void build_rns_tables(Engine& E) {
   const int k = E.k, kl = E.kl;
@@ -209,6 +231,8 @@ int aoa_engine_create(const aoa_params* p, aoa_engine** out) {
       E.gens[i] = p->generators ? p->generators[i] : h_smallest_primitive_root(E.primes[i]);
     build_prime_tables(E);
     build_rns_tables(E);
+    build_encoder_tables(E);
+    dgt_init(E, p->dgt_roots);
     rns_init(E);
     ntt_init(E);
     AOA_CUDA(cudaDeviceSynchronize());
@@ -265,6 +289,7 @@ int aoa_ctx_destroy(aoa_ctx* h) {
     if (h->c.plain) AOA_CUDA(cudaFreeAsync(h->c.plain, h->c.stream));
     if (h->c.batch) AOA_CUDA(cudaFreeAsync(h->c.batch, h->c.stream));
     if (h->c.conv) AOA_CUDA(cudaFreeAsync(h->c.conv, h->c.stream));
+    if (h->c.enc) AOA_CUDA(cudaFreeAsync(h->c.enc, h->c.stream));
     AOA_CUDA(cudaStreamSynchronize(h->c.stream));
     if (h->c.own_stream) AOA_CUDA(cudaStreamDestroy(h->c.stream));
   });

@@ -301,6 +301,7 @@ struct NttBatch {
   unsigned* err;           // device error word
   int log_n, log_r, log_c; // N = R * C
   int first_prime;
+  int prime_shift;         // limb l uses prime first_prime + (l >> prime_shift)
   long poly_stride;        // limbs between consecutive polys
   int npolys, nitems;      // nitems = nlimbs * npolys
 };
@@ -355,7 +356,7 @@ ntt_cols(NttBatch b) {
   if ((int)blockIdx.y < b.nitems) issue(blockIdx.y, 0);
   for (int j = blockIdx.y, it = 0; j < b.nitems; j += G, it++) {
     const int bi = it & 1;
-    const int limb = j / b.npolys, prime = b.first_prime + limb;
+    const int limb = j / b.npolys, prime = b.first_prime + (limb >> b.prime_shift);
     if (j + G < b.nitems) issue(j + G, bi ^ 1);
     if (limb != cur_limb) {                // previous users of tws passed the barrier below
       const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
@@ -464,7 +465,7 @@ ntt_rows(NttBatch b) {
     const int limb = j / b.npolys;
     if (threadIdx.x == 0 && j + G < b.nitems) issue(j + G, bi ^ 1);
     if (limb != cur_limb) {
-      const int prime = b.first_prime + limb;
+      const int prime = b.first_prime + (limb >> b.prime_shift);
       const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
       for (int e = threadIdx.x; e < ROWS * NT1; e += blockDim.x) {
         const int r = e / NT1, jj = e % NT1;
@@ -639,26 +640,82 @@ void ntt_init(Engine& E) {
   E.num_sms = sms;
 }
 
-// Transform limbs [0, nlimbs) of npolys polys (layout [npolys][poly_stride][N]),
-// limb l under prime first_prime + l.  Work is split into chunks of whole polys
+// Small transforms (N < 1024): one CTA per item, the whole limb in shared
+// memory, one radix-2 stage per step, canonical (strict) butterflies with the
+// same merged tables as the large kernels.
+__global__ void ntt_small(NttBatch b, bool fwd) {
+  extern __shared__ __align__(16) uint64_t xs[];
+  const int N = 1 << b.log_n;
+  for (int j = blockIdx.x; j < b.nitems; j += gridDim.x) {
+    const int limb = j / b.npolys, p = j % b.npolys;
+    const int prime = b.first_prime + (limb >> b.prime_shift);
+    uint64_t* x = b.data + ((long)p * b.poly_stride + limb) * N;
+    const PrimeConst& P = b.pc[prime];
+    const uint64_t q = P.q;
+    const ShoupW* tw = (fwd ? b.tw : b.itw) + (long)prime * N;
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += blockDim.x) xs[i] = x[i];
+    __syncthreads();
+    if (fwd) {
+      for (int m = 1; m < N; m <<= 1) {
+        const int t = N / (2 * m);
+        for (int bf = threadIdx.x; bf < N / 2; bf += blockDim.x) {
+          const int g = bf / t, l = bf % t, i0 = 2 * g * t + l;
+          const uint64_t u = xs[i0], v = shoup(xs[i0 + t], tw[m + g], q);
+          xs[i0] = add_mod(u, v, q);
+          xs[i0 + t] = sub_mod(u, v, q);
+        }
+        __syncthreads();
+      }
+      for (int i = threadIdx.x; i < N; i += blockDim.x) x[i] = xs[i];
+    } else {
+      for (int m = N / 2; m >= 1; m >>= 1) {
+        const int t = N / (2 * m);
+        for (int bf = threadIdx.x; bf < N / 2; bf += blockDim.x) {
+          const int g = bf / t, l = bf % t, i0 = 2 * g * t + l;
+          const uint64_t u = xs[i0], v = xs[i0 + t];
+          xs[i0] = add_mod(u, v, q);
+          xs[i0 + t] = shoup(sub_mod(u, v, q), tw[m + g], q);
+        }
+        __syncthreads();
+      }
+      for (int i = threadIdx.x; i < N; i += blockDim.x) x[i] = shoup(xs[i], P.ninv, P.ninv_sh, q);
+    }
+  }
+}
+
+// Transform limbs [0, nlimbs) of npolys polys (layout [npolys][poly_stride][N],
+// N = 2^T.log_n) with the tables T; limb l under prime first_prime +
+// (l >> T.prime_shift).  Large transforms are split into chunks of whole polys
 // whose total size stays within the L2 budget, column and row pass per chunk.
-void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
-               long poly_stride, bool forward, cudaStream_t st) {
+void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int npolys, int first_prime, int nlimbs,
+                      long poly_stride, bool forward, cudaStream_t st) {
   if (npolys <= 0 || nlimbs <= 0) return;
-  if (first_prime < 0 || first_prime + nlimbs > E.nprimes)
+  if (first_prime < 0 || first_prime + ((nlimbs - 1) >> T.prime_shift) >= E.nprimes)
     throw AoaError(AOA_ERR_BAD_PARAM, "ntt: prime range out of bounds");
   NttBatch b;
-  b.tw = E.d_tw; b.itw = E.d_itw; b.pc = E.d_pc; b.err = E.d_err;
-  b.log_n = E.log_n; b.log_c = E.log_c; b.log_r = E.log_n - E.log_c;
-  b.first_prime = first_prime; b.poly_stride = poly_stride;
-  const long limb_bytes = (8L << E.log_n);
+  b.tw = T.tw; b.itw = T.itw; b.pc = T.pc; b.err = E.d_err;
+  b.log_n = T.log_n; b.log_c = T.log_n / 2; b.log_r = T.log_n - b.log_c;
+  b.first_prime = first_prime; b.prime_shift = T.prime_shift; b.poly_stride = poly_stride;
+  if (T.log_n < 10) {
+    b.npolys = npolys;
+    b.nitems = npolys * nlimbs;
+    b.data = data;
+    const int n = 1 << T.log_n;
+    const int grid = std::min(b.nitems, 8 * E.num_sms);
+    ntt_small<<<grid, std::max(32, std::min(n / 2, 256)), n * 8, st>>>(b, forward);
+    note_launch();
+    AOA_CHECK_LAUNCH();
+    return;
+  }
+  const long limb_bytes = (8L << T.log_n);
   const long chunk = std::max(1L, E.tune.ntt_chunk_bytes / (limb_bytes * nlimbs));
   for (long c0 = 0; c0 < npolys; c0 += chunk) {
     const int np = (int)std::min<long>(chunk, npolys - c0);
     b.npolys = np;
     b.nitems = np * nlimbs;
-    b.data = data + c0 * poly_stride * (1L << E.log_n);
-    if (E.lazy) {
+    b.data = data + c0 * poly_stride * (1L << T.log_n);
+    if (T.lazy) {
       if (forward) { run_cols<true>(E, b, true, st); run_rows<true>(E, b, true, st); }
       else { run_rows<true>(E, b, false, st); run_cols<true>(E, b, false, st); }
     } else {
@@ -667,6 +724,15 @@ void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
     }
   }
   AOA_CHECK_LAUNCH();
+}
+
+// Negacyclic limb transforms of the engine's ring (psi^bitrev tables).
+void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
+               long poly_stride, bool forward, cudaStream_t st) {
+  NttTables T;
+  T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
+  T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
+  ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st);
 }
 
 }  // namespace aoa

@@ -318,6 +318,48 @@ def main():
             traffic = tj["ntt_fwd_bytes_per_coef"] * npolys * K * N
     del buf
 
+    # ---- DGT variant: transform rate and per-call HMult on a DGT context -----------
+    ctxd = aoa.Context(E)
+    ctxd.set_transform(aoa.AOA_DGT)
+    streamd = torch.cuda.ExternalStream(ctxd.stream)
+
+    def timed_on(st, c, fn, steps):
+        fn()
+        c.sync()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(st)
+        for _ in range(steps):
+            fn()
+        s1.record(st)
+        c.sync()
+        torch.cuda.synchronize()
+        return maxt(s0.elapsed_time(s1)) / steps
+
+    dbuf = ctxd.alloc((8, K, N))
+    dgt_fwd_ms = timed_on(streamd, ctxd, lambda: ctxd.dgt_fwd(dbuf, 8, 0, K), 5)
+    dgt_inv_ms = timed_on(streamd, ctxd, lambda: ctxd.dgt_inv(dbuf, 8, 0, K), 5)
+    dgt_bytes = 16 * 8 * K * N
+    del dbuf
+    evk_d = aoa.SwitchKey(ctxd, rr(ps), rr(ps), domain=aoa.AOA_COEF)
+
+    def dgt_step():
+        for (a, b), o in zip(cts, outs):
+            a.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_DGT)
+            b.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_DGT)
+            aoa.ckks_mul(ctxd, o, a, b, evk_d)
+    dgt_hmult_ms = timed_on(streamd, ctxd, dgt_step, max(2, args.steps // 2))
+    # encoder: N/2 slots encoded into K limbs and decoded from limb 0
+    vals = rng.uniform(-1, 1, N // 2) + 1j * rng.uniform(-1, 1, N // 2)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        m_enc, _ = aoa.ckks_encode(ctx, vals, scale=1 << SCALE_BITS)
+        ctx.sync()
+    enc_ms = (time.perf_counter() - t0) / 5 * 1000.0
+    t0 = time.perf_counter()
+    for _ in range(5):
+        aoa.ckks_decode(ctx, m_enc, N // 2, 1 << SCALE_BITS)
+    dec_ms = (time.perf_counter() - t0) / 5 * 1000.0
+
     # ---- end to end through the C ABI with host buffers -----------------------------
     pin_in = [aoa.PinnedArray((2, K, N)) for _ in range(2 * B)]
     for i, x in enumerate(host_in):
@@ -392,6 +434,13 @@ def main():
             "ntt": {"fwd_ms": fwd_ms, "inv_ms": inv_ms, "polys": npolys, "limbs": K,
                     "fwd_gbs": achieved, "inv_gbs": algo_bytes / (inv_ms / 1000.0) / 1e9,
                     "hbm_frac": achieved / peak},
+            "dgt": {"fwd_ms": dgt_fwd_ms, "inv_ms": dgt_inv_ms, "polys": 8, "limbs": K,
+                    "fwd_gbs": dgt_bytes / (dgt_fwd_ms / 1000.0) / 1e9,
+                    "inv_gbs": dgt_bytes / (dgt_inv_ms / 1000.0) / 1e9,
+                    "hmult_per_call_ops_per_s": world * B / (dgt_hmult_ms / 1000.0),
+                    "path": "aoa-dgt ckks_mul on a DGT context (GI tensor and key products), inputs in the DGT domain"},
+            "encoder": {"slots": N // 2, "limbs": K, "encode_ms_host_to_device": enc_ms,
+                        "decode_ms_device_to_host": dec_ms},
             "roofline": {"kernel": "ntt forward (column + row kernel pair), N=2^16", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_src, "algorithmic_bytes": algo_bytes, "traffic": traffic},

@@ -44,8 +44,10 @@ typedef enum {
   AOA_ERR_NO_DEVICE = 9
 } aoa_status;
 
-/* Domain of a polynomial's residues (reference poly_states, defines.h:56-60). */
-typedef enum { AOA_COEF = 1, AOA_NTT = 2 } aoa_domain;
+/* Domain of a polynomial's residues (reference poly_states, defines.h:56-60):
+ * coefficients (RNSSTATE), the negacyclic NTT domain of aoa-ntt (TRANSSTATE)
+ * or the folded Gaussian-integer DGT domain of aoa-dgt (its TRANSSTATE).     */
+typedef enum { AOA_COEF = 1, AOA_NTT = 2, AOA_DGT = 3 } aoa_domain;
 
 typedef struct aoa_engine aoa_engine;
 typedef struct aoa_ctx aoa_ctx;
@@ -58,6 +60,9 @@ typedef struct {
   const uint64_t* generators; /* optional primitive roots (NULL: smallest root)    */
   int scale_bits;             /* default scale 2^scale_bits (cipher_init)          */
   int dnum;                   /* key-switching decomposition; must be 1            */
+  const uint64_t* dgt_roots;  /* optional, 2 per prime: r = re + i im with r^(N/2) = i
+                                 (the DGT twist root, aoa-dgt NTHROOT[p][N/2]); NULL:
+                                 a root derived from the generator                  */
 } aoa_params;
 
 /* Last error message of this thread ("" if none). */
@@ -113,6 +118,35 @@ int aoa_memcpy_d2d(aoa_ctx* c, void* dst, const void* src, size_t bytes);
 int aoa_ntt_fwd(aoa_ctx* c, uint64_t* d_data, int npolys, int first_prime, int nlimbs, int poly_stride);
 int aoa_ntt_inv(aoa_ctx* c, uint64_t* d_data, int npolys, int first_prime, int nlimbs, int poly_stride);
 
+/* --- the DGT variant (aoa-dgt = library AOADGT).  A Gaussian-integer (GI)
+ *     limb is N words, planar: the N/2 real parts then the N/2 imaginary parts
+ *     of the folded polynomial a_j + i a_{j+N/2}, which is the same memory as
+ *     the limb's N coefficients, so folding is free (poly_copy_to_device /
+ *     poly_copy_to_host fold and unfold on the host, aoa-dgt
+ *     src/arithmetic/polynomial.cu:92-154).
+ *     aoa_dgt_fwd / aoa_dgt_inv replace DGTEngine::execute_dgt (aoa-dgt
+ *     src/cuda/dgt.cu:1055-1096, kernels hdgt_tr/hidgt/hidgt_tr/dgt/idgt
+ *     dgt.cu:805-1053): position p holds the folded polynomial at r w^bitrev(p),
+ *     r the engine's twist root (aoa_params.dgt_roots), w = g^((q-1)/(N/2)).  */
+int aoa_dgt_fwd(aoa_ctx* c, uint64_t* d_data, int npolys, int first_prime, int nlimbs, int poly_stride);
+int aoa_dgt_inv(aoa_ctx* c, uint64_t* d_data, int npolys, int first_prime, int nlimbs, int poly_stride);
+/* mul_dgt<GaussianInteger> (dgt.cu:1327-1341): element-wise GIMul (Karatsuba,
+ * dgt.cu:530-553) of nlimbs transform-domain GI limbs, primes first_prime..  */
+int aoa_gi_mul(aoa_ctx* c, uint64_t* d_out, const uint64_t* d_a, const uint64_t* d_b, int first_prime, int nlimbs);
+/* The reference's GaussianInteger arrays ({re, im} pairs, [nlimbs][N/2]) to
+ * planar GI limbs and back; no reference counterpart (the layout change the
+ * planar format needs at the boundary).  Buffers must not overlap.          */
+int aoa_gi_to_planar(aoa_ctx* c, uint64_t* d_dst, const uint64_t* d_src, int nlimbs);
+int aoa_gi_from_planar(aoa_ctx* c, uint64_t* d_dst, const uint64_t* d_src, int nlimbs);
+/* The engine's DGT twist roots, 2 words (re, im) per prime (compute_nthroot
+ * inputs NTHROOT[p][N/2], dgt.cu:1612-1662).                                */
+int aoa_engine_dgt_roots(const aoa_engine* e, uint64_t* roots_out);
+/* Which library's transform the context's evaluations use: AOA_NTT (aoa-ntt,
+ * default) or AOA_DGT (aoa-dgt: HMult tensor and key products as GIMul,
+ * rotations through the coefficient domain).  Ciphertexts and keys carry
+ * their domain; operands are converted on demand like poly_t states.       */
+int aoa_ctx_set_transform(aoa_ctx* c, int domain);
+
 /* --- RNS basis conversion and rescale on device buffers (coefficient domain).
  *     aoa_modup replaces CUDAManager::execute_modup / fast_conv_Q_to_B_opt
  *     (src/cuda/manager.cu:180-249): reads Q limbs 0..level of in_q ([k][N]),
@@ -147,6 +181,24 @@ int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, in
 typedef struct aoa_swk aoa_swk;
 int aoa_swk_create(aoa_ctx* c, const uint64_t* host_b, const uint64_t* host_a, int domain, aoa_swk** out);
 int aoa_swk_destroy(aoa_ctx* c, aoa_swk* k);
+/* device data [b | a], each (k+kl) limbs, and its transform domain */
+int aoa_swk_data(aoa_swk* k, uint64_t** device_ptr, int* domain);
+/* Key generation from given randomness (CKKSKeychain, src/ckks/ckkskeys.cpp:
+ * 101-191, with the sampler's draws passed in), in the context's transform
+ * domain.  Switching key for s1 under s2: b = rho(s1) + e - a s2, a over QB
+ * (rho: ckks_rho, src/cuda/manager.cu:149-176; s1 NULL means 0).  d_s1, d_s2:
+ * [k+kl][N] coefficient residues; d_a: [k+kl][N] uniform residues in a_domain;
+ * d_e: N signed noise values.                                               */
+int aoa_swk_generate(aoa_ctx* c, const uint64_t* d_s1, const uint64_t* d_s2, const uint64_t* d_a, int a_domain,
+                     const int64_t* d_e, aoa_swk** out);
+/* Public key (ckks_new_pk): out = (e - a s, a) over the Q primes, level k-1. */
+int aoa_pk_generate(aoa_ctx* c, aoa_ct* out, const uint64_t* d_s, const uint64_t* d_a, int a_domain,
+                    const int64_t* d_e);
+/* Secrets of the evaluation, rotation and conjugation keys from s (nlimbs
+ * coefficient-domain limbs): s^2 (ckks_new_mtk) and s(X^g) for odd g
+ * (rotation by r: g = 5^r mod 2N; conjugation: g = 2N - 1).                  */
+int aoa_secret_square(aoa_ctx* c, const uint64_t* d_s, uint64_t* d_out, int nlimbs);
+int aoa_secret_galois(aoa_ctx* c, const uint64_t* d_s, uint64_t* d_out, long galois, int nlimbs);
 
 /* --- CKKS evaluation (src/ckks/ckks.cpp; include/newckks/ckks/ckks.h:23-319).
  *     Outputs may alias inputs.  Like the reference, operands are brought to
@@ -190,6 +242,28 @@ int aoa_sub(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b);
 int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk);
 /* ckks_conjugate (ckks.cpp:1011-1040) */
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk);
+
+/* --- encoder and encryption (src/ckks/encoder.cu:12-298, ckks.cpp:87-192,
+ *     CKKSContext::encode/decode ckkscontext.cpp:5-38).  Complex values are
+ *     (re, im) double pairs (the layout of std::complex<double>).             */
+/* ckks_encode (encoder.cu:166-221): `filled` values then `empty` zero slots
+ * (filled + empty a power of two <= N/2), scaled by `scale`, into limbs
+ * 0..nlimbs-1 of d_out ([nlimbs][N]) in `domain`.  Identical residues.        */
+int aoa_encode(aoa_ctx* c, const double* host_vals, int filled, int empty, uint64_t scale, int nlimbs,
+               int domain, uint64_t* d_out);
+/* CKKSContext::decode + ckks_decode (ckkscontext.cpp:21-38, encoder.cu:259-298):
+ * `slots` values from limb 0 of d_m (in `domain`) into host memory; identical
+ * doubles.  Synchronises.                                                    */
+int aoa_decode(aoa_ctx* c, const uint64_t* d_m, int domain, int slots, uint64_t scale, double* host_vals);
+/* ckks_encrypt_poly (ckks.cpp:87-105) with the sampler's draws passed in:
+ * d_u, d_e1, d_e2 hold N signed coefficients each (the Z0 and DG samples);
+ * pk = (b, a) as a ciphertext over all Q primes.  d_m: [k][N] message in
+ * m_domain.  Output in the NTT domain at level k-1.                          */
+int aoa_encrypt(aoa_ctx* c, aoa_ct* out, const uint64_t* d_m, int m_domain, aoa_ct* pk, const int64_t* d_u,
+                const int64_t* d_e1, const int64_t* d_e2, int slots, uint64_t scale);
+/* ckks_decrypt_poly (ckks.cpp:179-192): m = c1 s + c0 over limbs 0..level,
+ * coefficient domain, into d_m_out ([level+1][N]).  d_s: [k][N] secret.     */
+int aoa_decrypt(aoa_ctx* c, aoa_ct* ct, const uint64_t* d_s, int s_domain, uint64_t* d_m_out);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,12 @@ def lib():
             "oc_decode": (None, [vp, u64p, c_int, u64, f64p, f64p]),
             "oc_fft_special_inv": (None, [c_int, f64p, f64p, c_int]),
             "oc_fft_special": (None, [c_int, f64p, f64p, c_int]),
+            "oc_dgt_create": (vp, [c_int, c_int, u64p, u64p, u64p]),
+            "oc_dgt_destroy": (None, [vp]),
+            "oc_dgt_fwd": (None, [vp, u64p, c_int, c_int]),
+            "oc_dgt_inv": (None, [vp, u64p, c_int, c_int]),
+            "oc_gi_mul": (None, [vp, u64p, u64p, u64p, c_int, c_int]),
+            "oc_dgt_twist": (None, [vp, c_int, u64p, u64p]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -306,3 +312,80 @@ def reference_prime_set(table, k, kl, prec):
 
 def reference_proots(table, primes):
     return [int(table["proots"][str(q)]) for q in primes]
+
+
+class DgtOracle:
+    """The reference's DGT (aoa-dgt src/cuda/dgt.cu) for folded length N = n/2
+    over `primes`, with generators `proots` and roots r (r^N = i) given as
+    (re, im) pairs.  Arrays are [nres][N][2] uint64 (re, im interleaved, the
+    reference's GaussianInteger layout)."""
+
+    def __init__(self, N, primes, proots, roots):
+        self.N = N
+        self.primes = [int(q) for q in primes]
+        pa = np.array(self.primes, dtype=np.uint64)
+        ga = np.array([int(g) for g in proots], dtype=np.uint64)
+        ra = np.array([int(v) for r in roots for v in r], dtype=np.uint64)
+        self._h = lib().oc_dgt_create(N, len(self.primes), P(pa), P(ga), P(ra))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().oc_dgt_destroy(self._h)
+            self._h = None
+
+    def fwd(self, x, first=0):
+        y = u64(x).copy()
+        lib().oc_dgt_fwd(self._h, P(y), first, y.shape[0])
+        return y
+
+    def inv(self, x, first=0):
+        y = u64(x).copy()
+        lib().oc_dgt_inv(self._h, P(y), first, y.shape[0])
+        return y
+
+    def gi_mul(self, a, b, first=0):
+        a, b = u64(a), u64(b)
+        c = np.zeros_like(a)
+        lib().oc_gi_mul(self._h, P(a), P(b), P(c), first, a.shape[0])
+        return c
+
+    def twist(self, rid):
+        nth = np.zeros((self.N, 2), dtype=np.uint64)
+        inv = np.zeros_like(nth)
+        lib().oc_dgt_twist(self._h, rid, P(nth), P(inv))
+        return nth, inv
+
+
+def fold(coeffs):
+    """[nres][2N] coefficients -> [nres][N][2] Gaussian integers a_j + i a_{j+N}
+    (poly_copy_to_device, aoa-dgt src/arithmetic/polynomial.cu:92-116)."""
+    c = u64(coeffs)
+    n2 = c.shape[-1] // 2
+    return np.ascontiguousarray(np.stack([c[..., :n2], c[..., n2:]], axis=-1))
+
+
+def unfold(gi):
+    """Inverse of fold (poly_copy_to_host, polynomial.cu:118-154)."""
+    g = u64(gi)
+    return np.ascontiguousarray(np.concatenate([g[..., 0], g[..., 1]], axis=-1))
+
+
+def dgt_prime_set(table, k, kl, prec):
+    """Q and B primes as the DGT variant's fill_ckks_coprimes_bucket picks them
+    (aoa-dgt src/cuda/cudaengine.cu:545-583): B continues the 55-bit bucket at
+    index k-1 for every precision but 45."""
+    b = table["buckets"]
+    q0 = b["63"][0]
+    if prec == 45:
+        return [q0] + b["45"][:k - 1], b["45"][k - 1:k - 1 + kl]
+    if prec in (48, 52, 55):
+        return [q0] + b[str(prec)][:k - 1], b["55"][k - 1:k - 1 + kl]
+    raise ValueError("the DGT variant supports prec 45/48/52/55 only")
+
+
+def dgt_roots(table, primes, N):
+    """(generators, roots r with r^N = i) of `primes` from the fixture
+    (tests/golden/dgt_roots.json)."""
+    g = [int(table["proots"][str(q)]) for q in primes]
+    r = [tuple(int(v) for v in table["nthroot"][str(q)][str(N)]) for q in primes]
+    return g, r

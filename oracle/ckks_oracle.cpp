@@ -1167,3 +1167,245 @@ void oc_fft_special(int N, double* re, double* im, int size) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// DGT variant (aoa-dgt): folded Gaussian-integer transform.
+//
+// A degree-n polynomial is folded into N = n/2 Gaussian integers
+// a_j + i a_{j+N} (poly_copy_to_device, aoa-dgt src/arithmetic/polynomial.cu:
+// 92-116), twisted by powers of r, r^N = i (NTHROOT[p][N], aoa-dgt
+// src/arithmetic/coprimes.cu), and transformed by a length-N DIF transform
+// over GF(p)[i] with Z_p twiddles; N >= 1024 uses the two-kernel hierarchical
+// form (Na x Nb, DGTFACT*, aoa-dgt include/AOADGT/cuda/dgt.h:26-35).  Data
+// layout as in the reference: [residue][N] of {re, im} (16 bytes).
+// ===========================================================================
+namespace {
+
+struct GI { uint64_t re, im; };
+
+struct DgtPrime {
+  uint64_t q; int nbits; uint64_t mu;
+  uint64_t mul(uint64_t a, uint64_t b) const { return ref_mod((u128)a * b, q, nbits, mu); }
+  uint64_t add(uint64_t a, uint64_t b) const { uint64_t s = a + b; return s >= q ? s - q : s; }   // addmod
+  uint64_t sub(uint64_t a, uint64_t b) const { return a < b ? a + (q - b) : a - b; }             // submod
+  GI gadd(GI a, GI b) const { return {add(a.re, b.re), add(a.im, b.im)}; }     // GIAdd, dgt.cu:486-495
+  GI gsub(GI a, GI b) const { return {sub(a.re, b.re), sub(a.im, b.im)}; }     // GISub, dgt.cu:498-508
+  // GIMul (Karatsuba), aoa-dgt src/cuda/dgt.cu:530-553
+  GI gmul(GI a, GI b) const {
+    uint64_t s1 = mul(a.re, b.re), s2 = mul(a.im, b.im);
+    uint64_t s3 = mul(add(a.re, a.im), add(b.re, b.im));
+    return {sub(s1, s2), sub(s3, add(s1, s2))};
+  }
+  std::vector<uint64_t> gjk_n, inv_n, gjk_a, inv_a, gjk_b, inv_b;   // compute_gjk
+  std::vector<GI> nth, invnth;                                      // compute_nthroot
+  std::vector<uint64_t> gN, ginvN;                                  // DGTEngine::init, dgt.cu:1918-1941
+};
+
+struct DgtCtx {
+  int N = 0, Na = 0, Nb = 0;
+  bool hier = false;
+  std::vector<DgtPrime> P;
+};
+
+// DGTFACT* (aoa-dgt include/AOADGT/cuda/dgt.h:26-35): hierarchical from N = 1024.
+static void dgt_fact(int N, int& Na, int& Nb) {
+  switch (N) {
+    case 1024: Na = 32; Nb = 32; break;
+    case 2048: Na = 64; Nb = 32; break;
+    case 4096: Na = 64; Nb = 64; break;
+    case 8192: Na = 128; Nb = 64; break;
+    case 16384: Na = 128; Nb = 128; break;
+    case 32768: Na = 256; Nb = 128; break;
+    default: Na = Nb = 0;
+  }
+}
+
+// compute_gjk (aoa-dgt src/cuda/dgt.cu:1511-1560), one residue:
+// g = proot^((p-1)/(2S)); gjk[s][j] = g^(j 2^(s+1)); inv[s][j] = g^((2S - j) 2^(s+1)).
+static void dgt_gjk(const DgtPrime& P, uint64_t proot, int S, std::vector<uint64_t>& gjk, std::vector<uint64_t>& inv) {
+  int L = ilog2i(S);
+  gjk.assign((size_t)L * S, 0);
+  inv.assign((size_t)L * S, 0);
+  uint64_t g = oc_powmod(proot, (P.q - 1) / (2 * (uint64_t)S), P.q);
+  for (int s = 0; s < L; s++)
+    for (int j = 0; j < S; j++) {
+      gjk[(size_t)s * S + j] = oc_powmod(g, (uint64_t)j * ((2ull * S) >> (L - s)), P.q);
+      inv[(size_t)s * S + j] = oc_powmod(g, (uint64_t)(2 * S - j) * ((2ull * S) >> (L - s)), P.q);
+    }
+}
+
+// dgttransform (dgt.cu:667-700) over all butterflies of stage s, inside the
+// stage loop of doDGT (dgt.cu:741-765): DIF, natural in, bit-reversed out.
+static void dgt_do(const DgtPrime& P, GI* d, int S, const std::vector<uint64_t>& gjk) {
+  int L = ilog2i(S);
+  for (int s = 0; s < L; s++) {
+    int m = S / (2 << s);
+    for (int cid = 0; cid < S / 2; cid++) {
+      int j = cid * 2 * m / S;
+      int i = j + (cid % (S / (2 * m))) * 2 * m;
+      GI xi = d[i], xim = d[i + m];
+      uint64_t a = gjk[(size_t)s * S + j];
+      d[i] = P.gadd(xi, xim);
+      GI t = P.gsub(xi, xim);
+      d[i + m] = {P.mul(a, t.re), P.mul(a, t.im)};
+    }
+  }
+}
+
+// idgttransform (dgt.cu:702-739) + doIDGT (dgt.cu:768-790): DIT, stages L-1..0.
+static void dgt_undo(const DgtPrime& P, GI* d, int S, const std::vector<uint64_t>& inv) {
+  int L = ilog2i(S);
+  for (int s = L - 1; s >= 0; s--) {
+    int m = S / (2 << s);
+    for (int cid = 0; cid < S / 2; cid++) {
+      int j = cid * 2 * m / S;
+      int i = j + (cid % (S / (2 * m))) * 2 * m;
+      GI xi = d[i], xim = d[i + m];
+      uint64_t a = inv[(size_t)s * S + j];
+      GI axim = {P.mul(a, xim.re), P.mul(a, xim.im)};
+      d[i] = P.gadd(xi, axim);
+      d[i + m] = P.gsub(xi, axim);
+    }
+  }
+}
+
+static void dgt_forward(const DgtCtx& D, const DgtPrime& P, GI* x) {
+  const int N = D.N;
+  if (!D.hier) {                                     // dgt<N> (dgt.cu:995-1024)
+    for (int t = 0; t < N; t++) x[t] = P.gmul(x[t], P.nth[t]);
+    dgt_do(P, x, N, P.gjk_n);
+    return;
+  }
+  const int Na = D.Na, Nb = D.Nb;
+  std::vector<GI> tmp(N), s(std::max(Na, Nb));
+  // hdgt_tr<Nb> with the GI twist (dgt.cu:805-848): column c of the Nb x Na
+  // matrix, written transposed to row c.
+  for (int c = 0; c < Na; c++) {
+    for (int t = 0; t < Nb; t++) s[t] = P.gmul(x[t * Na + c], P.nth[t * Na + c]);
+    dgt_do(P, s.data(), Nb, P.gjk_b);
+    for (int t = 0; t < Nb; t++) tmp[c * Nb + t] = s[t];
+  }
+  // hdgt_tr<Na> with the integer twist gN (dgt.cu:850-901).
+  for (int c = 0; c < Nb; c++) {
+    for (int t = 0; t < Na; t++) {
+      GI v = tmp[t * Nb + c];
+      uint64_t w = P.gN[t * Nb + c];
+      s[t] = {P.mul(w, v.re), P.mul(w, v.im)};
+    }
+    dgt_do(P, s.data(), Na, P.gjk_a);
+    for (int t = 0; t < Na; t++) x[c * Na + t] = s[t];
+  }
+}
+
+static void dgt_inverse(const DgtCtx& D, const DgtPrime& P, GI* x) {
+  const int N = D.N;
+  if (!D.hier) {                                     // idgt<N> (dgt.cu:1026-1053)
+    dgt_undo(P, x, N, P.inv_n);
+    for (int t = 0; t < N; t++) x[t] = P.gmul(x[t], P.invnth[t]);
+    return;
+  }
+  const int Na = D.Na, Nb = D.Nb;
+  std::vector<GI> tmp(N), s(std::max(Na, Nb));
+  // hidgt<Na> (dgt.cu:903-949): rows of Na, untwist by ginvN (N^-1 inside).
+  for (int r = 0; r < Nb; r++) {
+    for (int t = 0; t < Na; t++) s[t] = x[r * Na + t];
+    dgt_undo(P, s.data(), Na, P.inv_a);
+    for (int t = 0; t < Na; t++) {
+      uint64_t w = P.ginvN[r * Na + t];
+      tmp[r * Na + t] = {P.mul(w, s[t].re), P.mul(w, s[t].im)};
+    }
+  }
+  // hidgt_tr<Nb> (dgt.cu:951-993): columns, untwist by r^-n, not transposed.
+  for (int c = 0; c < Na; c++) {
+    for (int t = 0; t < Nb; t++) s[t] = tmp[t * Na + c];
+    dgt_undo(P, s.data(), Nb, P.inv_b);
+    for (int t = 0; t < Nb; t++) x[t * Na + c] = P.gmul(s[t], P.invnth[t * Na + c]);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+typedef void* oc_dgt;
+
+// DGTEngine::init (aoa-dgt src/cuda/dgt.cu:1696-1945) for one folded length N:
+// primes[i] with generator proots[i] and root roots[2i] + i roots[2i+1]
+// (NTHROOT[p][N]); the inverse root is the GF(p)[i] inverse of r (what
+// INVNTHROOT[p][N] holds, asserted by compute_nthroot, dgt.cu:1640-1644).
+oc_dgt oc_dgt_create(int N, int nprimes, const uint64_t* primes, const uint64_t* proots, const uint64_t* roots) {
+  DgtCtx* D = new DgtCtx();
+  D->N = N;
+  dgt_fact(N, D->Na, D->Nb);
+  D->hier = D->Na > 0;
+  D->P.resize(nprimes);
+  for (int i = 0; i < nprimes; i++) {
+    DgtPrime& P = D->P[i];
+    P.q = primes[i]; P.nbits = nbits64(P.q); P.mu = oc_ref_barrett_mu(P.q);
+    GI r = {roots[2 * i], roots[2 * i + 1]};
+    uint64_t norm = (uint64_t)(((u128)r.re * r.re + (u128)r.im * r.im) % P.q);
+    uint64_t ninv_norm = oc_invmod(norm, P.q);
+    GI rinv = {oc_mulmod_exact(r.re, ninv_norm, P.q), oc_mulmod_exact(r.im ? P.q - r.im : 0, ninv_norm, P.q)};
+    P.nth.resize(N); P.invnth.resize(N);
+    uint64_t ninv = oc_invmod((uint64_t)N % P.q, P.q);
+    GI a = {1, 0}, b = {1, 0};
+    for (int t = 0; t < N; t++) {                      // compute_nthroot, dgt.cu:1646-1662
+      P.nth[t] = a;
+      P.invnth[t] = D->hier ? b : P.gmul(b, GI{ninv, 0});
+      a = P.gmul(a, r);
+      b = P.gmul(b, rinv);
+    }
+    if (!D->hier) {
+      dgt_gjk(P, proots[i], N, P.gjk_n, P.inv_n);
+    } else {
+      dgt_gjk(P, proots[i], D->Na, P.gjk_a, P.inv_a);
+      dgt_gjk(P, proots[i], D->Nb, P.gjk_b, P.inv_b);
+      uint64_t g = oc_powmod(proots[i], (P.q - 1) / (uint64_t)N, P.q), ginv = oc_invmod(g, P.q);
+      P.gN.resize(N); P.ginvN.resize(N);
+      int lb = ilog2i(D->Nb);
+      for (int cid = 0; cid < N; cid++) {
+        P.gN[cid] = oc_powmod(g, (uint64_t)(cid / D->Nb) * bitrev(cid % D->Nb, lb), P.q);
+        P.ginvN[cid] = oc_mulmod_exact(oc_powmod(ginv, (uint64_t)bitrev(cid / D->Na, lb) * (cid % D->Na), P.q), ninv,
+                                       P.q);
+      }
+    }
+  }
+  return D;
+}
+
+void oc_dgt_destroy(oc_dgt h) { delete (DgtCtx*)h; }
+
+// execute_dgt (dgt.cu:1055-1096) on residues first..first+nres-1 of x
+// ([nres][N] Gaussian integers, interleaved re/im), in place.
+void oc_dgt_fwd(oc_dgt h, uint64_t* x, int first, int nres) {
+  DgtCtx& D = *(DgtCtx*)h;
+  #pragma omp parallel for schedule(static)
+  for (int r = 0; r < nres; r++) dgt_forward(D, D.P[first + r], (GI*)x + (size_t)r * D.N);
+}
+
+void oc_dgt_inv(oc_dgt h, uint64_t* x, int first, int nres) {
+  DgtCtx& D = *(DgtCtx*)h;
+  #pragma omp parallel for schedule(static)
+  for (int r = 0; r < nres; r++) dgt_inverse(D, D.P[first + r], (GI*)x + (size_t)r * D.N);
+}
+
+// Element-wise GI product (mul_dgt<GaussianInteger>, dgt.cu:1327-1341): c = a * b.
+void oc_gi_mul(oc_dgt h, const uint64_t* a, const uint64_t* b, uint64_t* c, int first, int nres) {
+  DgtCtx& D = *(DgtCtx*)h;
+  for (int r = 0; r < nres; r++) {
+    const DgtPrime& P = D.P[first + r];
+    for (int t = 0; t < D.N; t++) {
+      size_t i = (size_t)r * D.N + t;
+      ((GI*)c)[i] = P.gmul(((const GI*)a)[i], ((const GI*)b)[i]);
+    }
+  }
+}
+
+// The twist tables, for inspection by the tests: nth[t] = r^t, invnth[t].
+void oc_dgt_twist(oc_dgt h, int rid, uint64_t* nth, uint64_t* invnth) {
+  DgtCtx& D = *(DgtCtx*)h;
+  std::memcpy(nth, D.P[rid].nth.data(), (size_t)D.N * 16);
+  std::memcpy(invnth, D.P[rid].invnth.data(), (size_t)D.N * 16);
+}
+
+}  // extern "C"
