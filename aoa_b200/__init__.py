@@ -44,6 +44,10 @@ class Engine:
         capi.check(lib.aoa_engine_create(ctypes.byref(p), ctypes.byref(h)))
         self.handle = h
 
+    def tune(self, knob, value):
+        """Set a launch-shape knob ("ntt_chunk_bytes", "ntt_waves")."""
+        capi.check(capi.load().aoa_engine_tune(self.handle, knob.encode(), float(value)))
+
     def close(self):
         if getattr(self, "handle", None):
             capi.load().aoa_engine_destroy(self.handle)
@@ -173,6 +177,19 @@ class Ciphertext:
         ct.set(level if level is not None else nl - 1, slots,
                scale if scale is not None else (1 << E.scale_bits if E.scale_bits else 1), domain)
         return ct
+
+    def copy(self):
+        """A new ciphertext with a device copy of this one's data and metadata."""
+        out = Ciphertext(self.ctx)
+        E = self.ctx.engine
+        lib = capi.load()
+        src, dst = ctypes.c_void_p(), ctypes.c_void_p()
+        capi.check(lib.aoa_ct_data(self.handle, ctypes.byref(src)))
+        capi.check(lib.aoa_ct_data(out.handle, ctypes.byref(dst)))
+        capi.check(lib.aoa_memcpy_d2d(self.ctx.handle, dst, src, 2 * E.k * E.N * 8))
+        level, slots, scale, domain = self._get()
+        out.set(level, slots, scale, domain)
+        return out
 
     def upload(self, c0, c1, domain=AOA_COEF):
         host = np.ascontiguousarray(np.stack([np.asarray(c0, dtype=np.uint64), np.asarray(c1, dtype=np.uint64)]))
@@ -456,3 +473,90 @@ def ckks_keygen(ctx, s, draws, rotations=(), conjugation=False):
         a, e = draws["cjk"]
         keys["cjk"] = SwitchKey.generate(ctx, sc, s, a, e)
     return keys
+
+
+# ---- plaintext / constant operations (aoa-ntt src/ckks/ckks.cpp:423-690) ----------
+
+def ckks_mul_pt(ctx, out, ct, pt, pt_scale, pt_domain=AOA_COEF, rescale=True):
+    """out = ct * pt for an encoded plaintext device array pt ([k][N])."""
+    capi.check(capi.load().aoa_mul_plaintext(ctx.handle, out.handle, ct.handle, pt.ptr, pt_domain, int(pt_scale),
+                                             1 if rescale else 0))
+
+
+def ckks_mul_values(ctx, out, ct, values, rescale=True):
+    """ckks_mul(ctx, c2, c1, complex*) (ckks.cpp:610-632): encode at the
+    ciphertext's scale and slot count, multiply, rescale."""
+    v = np.asarray(values, dtype=np.complex128)
+    pt, scale = ckks_encode(ctx, v, empty_slots=ct.slots - v.size, scale=ct.scale)
+    ckks_mul_pt(ctx, out, ct, pt, scale, rescale=rescale)
+
+
+def ckks_mul_const(ctx, out, ct, val, rescale=True):
+    capi.check(capi.load().aoa_mul_const(ctx.handle, out.handle, ct.handle, float(val), 1 if rescale else 0))
+
+
+def ckks_add_const(ctx, out, ct, val):
+    capi.check(capi.load().aoa_add_const(ctx.handle, out.handle, ct.handle, float(val)))
+
+
+def ckks_sumslots(ctx, out, ct, rtks):
+    """Rotate-and-sum over the slots (ckks_sumslots); rtks maps each power-of-two
+    step 2^j to its left-rotation SwitchKey."""
+    n = max((s.bit_length() for s in rtks), default=0)
+    arr = (ctypes.c_void_p * max(n, 1))()
+    for step, key in rtks.items():
+        arr[step.bit_length() - 1] = key.handle.value
+    capi.check(capi.load().aoa_sumslots(ctx.handle, out.handle, ct.handle, arr, n))
+
+
+def ckks_batch_inner_prod(ctx, out, ct, other, rtks):
+    """ckks_batch_inner_prod (ckks.cpp:470-482): multiply (by a ciphertext, a
+    SwitchKey-relinearised product needs evk in `rtks["evk"]`, or by complex
+    values) then sum the slots."""
+    if isinstance(other, Ciphertext):
+        ckks_mul(ctx, out, ct, other, rtks["evk"])
+    else:
+        ckks_mul_values(ctx, out, ct, other)
+    ckks_sumslots(ctx, out, out, {k: v for k, v in rtks.items() if isinstance(k, int)})
+
+
+# ---- CUDA graphs ------------------------------------------------------------------
+
+class Graph:
+    """A captured sequence of a context's asynchronous work, replayed with one launch."""
+
+    def __init__(self, ctx, handle):
+        self.ctx, self.handle = ctx, handle
+
+    @classmethod
+    def capture(cls, ctx, fn):
+        """Run fn() under stream capture on ctx and instantiate the result."""
+        lib = capi.load()
+        capi.check(lib.aoa_ctx_capture_begin(ctx.handle))
+        try:
+            fn()
+        finally:
+            h = ctypes.c_void_p()
+            st = lib.aoa_ctx_capture_end(ctx.handle, ctypes.byref(h))
+        capi.check(st)
+        return cls(ctx, h)
+
+    @property
+    def nodes(self):
+        n = ctypes.c_long()
+        capi.check(capi.load().aoa_graph_nodes(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def launch(self):
+        capi.check(capi.load().aoa_graph_launch(self.ctx.handle, self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            capi.load().aoa_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -97,6 +97,16 @@ SIGNATURES = {
     "aoa_gi_from_planar": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "aoa_engine_dgt_roots": (c_int, [c_void_p, c_void_p]),
     "aoa_ctx_set_transform": (c_int, [c_void_p, c_int]),
+    "aoa_engine_tune": (c_int, [c_void_p, c_char_p, c_double]),
+    "aoa_mul_plaintext": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_u64, c_int]),
+    "aoa_mul_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int]),
+    "aoa_add_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double]),
+    "aoa_sumslots": (c_int, [c_void_p, c_void_p, c_void_p, vpp, c_int]),
+    "aoa_ctx_capture_begin": (c_int, [c_void_p]),
+    "aoa_ctx_capture_end": (c_int, [c_void_p, c_void_p]),
+    "aoa_graph_launch": (c_int, [c_void_p, c_void_p]),
+    "aoa_graph_nodes": (c_int, [c_void_p, c_void_p]),
+    "aoa_graph_destroy": (c_int, [c_void_p]),
     "aoa_swk_data": (c_int, [c_void_p, c_void_p, c_void_p]),
     "aoa_swk_generate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "aoa_pk_generate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),

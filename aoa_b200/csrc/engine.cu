@@ -256,6 +256,19 @@ int aoa_engine_destroy(aoa_engine* h) {
   return st;
 }
 
+// Launch-shape knobs of the engine's kernels (the reference fixes its kernel
+// shapes at compile time): "ntt_chunk_bytes" (limbs per transform launch
+// pair, kept within L2) and "ntt_waves" (transform CTAs per pass, in resident
+// waves).  Set before the engine is used from several streams at once.
+int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
+  if (!h || !knob) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  const std::string k(knob);
+  if (k == "ntt_chunk_bytes" && value >= (1 << 20) && value <= 4e9) h->e.tune.ntt_chunk_bytes = (long)value;
+  else if (k == "ntt_waves" && value > 0 && value <= 64) h->e.tune.ntt_waves = value;
+  else return fail(AOA_ERR_BAD_PARAM, "unknown knob or value out of range: " + k);
+  return AOA_OK;
+}
+
 int aoa_engine_info(const aoa_engine* h, int* log_n, int* k, int* kl, uint64_t* primes_out) {
   if (!h) return fail(AOA_ERR_BAD_PARAM, "null engine");
   if (log_n) *log_n = h->e.log_n;

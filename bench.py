@@ -163,6 +163,65 @@ def profile_case(args, aoa, ctx, rr, ps):
     print("profile case done")
 
 
+def systems_workloads(aoa, torch):
+    """Batched uneven mix (512 ops, N in {2^14, 2^15, 2^16}, live limbs 4..30,
+    50% HMult+relin+rescale / 30% rotate by 2^j / 20% add): grouped launches
+    captured in CUDA graphs vs the plain per-call path; then the serving loop
+    (plaintext-weight multiply + rescale, rotate-and-sum, rescale; N in
+    {2^15, 2^16}, live limbs 6..30) at 5 Poisson rates relative to its measured
+    saturation throughput."""
+    from aoa_b200.workloads import UnevenBatch, Server
+    wb = UnevenBatch(n_ops=512, seed=4)
+
+    def timed_multi(fn):
+        wb.sync()
+        torch.cuda.synchronize()
+        evs = {ln: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for ln in wb.ctx}
+        st = {ln: torch.cuda.ExternalStream(c.stream) for ln, c in wb.ctx.items()}
+        first = next(iter(wb.ctx))
+        evs[first][0].record(st[first])
+        for ln in wb.ctx:
+            if ln != first:
+                evs[ln][0].record(st[ln])
+        fn()
+        for ln in wb.ctx:
+            evs[ln][1].record(st[ln])
+        wb.sync()
+        torch.cuda.synchronize()
+        return max(evs[first][0].elapsed_time(evs[ln][1]) for ln in wb.ctx)
+
+    wb.run_plain()
+    plain_ms = timed_multi(wb.run_plain)
+    nodes = wb.capture()
+    wb.launch_graphs()
+    graph_ms = min(timed_multi(wb.launch_graphs) for _ in range(3))
+    grouped_ms = timed_multi(lambda: [wb.run_grouped(ln) for ln in wb.ctx])
+    n_ops = len(wb.ops)
+    mix = {k: sum(1 for op in wb.ops if op["kind"] == k) for k in ("mul", "rot", "add")}
+    uneven = {"ops": n_ops, "mix": mix, "seed": 4,
+              "graph_ops_per_s": n_ops / (graph_ms / 1000.0), "grouped_ops_per_s": n_ops / (grouped_ms / 1000.0),
+              "plain_ops_per_s": n_ops / (plain_ms / 1000.0), "speedup_vs_plain": plain_ms / graph_ms,
+              "graph_nodes": nodes, "algorithmic_bytes": wb.bytes,
+              "achieved_gbs": wb.bytes / (graph_ms / 1000.0) / 1e9,
+              "schedule": "one stream per N, HMults grouped by limb count (<=64 per launch), CUDA graph per stream"}
+    del wb
+    srv = Server(log_ns=(15, 16), slots_per_degree=4, hbm_budget=8 << 30)
+    reqs = srv.make_requests(48, seed=6)
+    srv.run(reqs[:8], rate=None)                         # warm the contexts' workspaces
+    lat, wall = srv.run(reqs, rate=None)
+    sat = len(reqs) / wall
+    rates = []
+    for f in (0.25, 0.5, 0.75, 0.9, 1.1):
+        lat, wall = srv.run(reqs, rate=f * sat)
+        rates.append({"rate_factor": f, "offered_req_per_s": f * sat, "served_req_per_s": len(reqs) / wall,
+                      "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000)})
+    serving = {"saturation_req_per_s": sat, "requests_per_rate": len(reqs), "streams_per_degree": 4,
+               "hbm_budget_bytes": 8 << 30, "rates": rates,
+               "request": "ct*w (plaintext, rescale) + rotate-and-sum over N/2 slots + rescale; N in {2^15,2^16}, "
+                          "live limbs 6..30; latency = arrival to completion (host clock)"}
+    return uneven, serving
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -171,6 +230,7 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--impl", default="aoa", choices=["aoa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-systems", action="store_true", help="skip the uneven-batch and serving measurements")
     ap.add_argument("--profile-case", choices=["ntt", "hmult"],
                     help="run a small fixed case for ncu captures (no timing, no JSON)")
     ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt")
@@ -284,8 +344,8 @@ def main():
         lat.append(s0.elapsed_time(s1))
     lat = np.array(lat)
 
-    # ---- NTT roofline (forward transform over 64 polys x 30 limbs) ----------------
-    npolys = 64
+    # ---- transform throughput: 256 polys x 30 limbs, forward then inverse ----------
+    npolys = 256
     buf = ctx.alloc((npolys, K, N))
     xs = rr(ps[:K])
     for p in range(npolys):
@@ -306,6 +366,46 @@ def main():
     barrier()
     fwd_ms = t0.elapsed_time(t1) / reps
     inv_ms = t1.elapsed_time(t2) / reps
+    # inverse(forward(x)) == x on the first and last poly, forward == oracle on one poly
+    lib_ = aoa.capi.load()
+    chk = np.empty((K, N), dtype=np.uint64)
+    roundtrip_ok = True
+    for p in (0, npolys - 1):
+        aoa.capi.check(lib_.aoa_memcpy_d2h(ctx.handle, aoa.capi.ptr(chk), buf.offset(p * K * N), chk.nbytes))
+        ctx.sync()
+        roundtrip_ok = roundtrip_ok and bool(np.array_equal(chk, xs))
+    ctx.ntt_fwd(buf, 1, 0, K)
+    aoa.capi.check(lib_.aoa_memcpy_d2h(ctx.handle, aoa.capi.ptr(chk), buf.ptr, chk.nbytes))
+    ctx.sync()
+    ntt_cpu = None
+    fwd_matches_oracle = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        from oracle import Oracle
+        oracle.lib().oc_set_threads(os.cpu_count() or 1)
+        o_ntt = Oracle(N, ps[:K], ps[K:])
+        tc = time.perf_counter()
+        want = o_ntt.ntt_fwd(xs)
+        tc = time.perf_counter() - tc
+        fwd_matches_oracle = bool(np.array_equal(chk, want))
+        ntt_cpu = {"value": 16 * K * N / tc / 1e9, "unit": "GB/s", "cores": os.cpu_count() or 1, "kind": "port",
+                   "sample": "forward transform of one 30-limb poly (oracle, OpenMP)"}
+    ctx.ntt_inv(buf, 1, 0, K)
+    # the DGT on the same data (folded to 2^15 Gaussian integers per limb)
+    d0, d1, d2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    ctx.dgt_fwd(buf, npolys, 0, K)
+    ctx.dgt_inv(buf, npolys, 0, K)
+    barrier()
+    d0.record(stream)
+    ctx.dgt_fwd(buf, npolys, 0, K)
+    d1.record(stream)
+    ctx.dgt_inv(buf, npolys, 0, K)
+    d2.record(stream)
+    barrier()
+    dgt256_fwd_ms, dgt256_inv_ms = d0.elapsed_time(d1), d1.elapsed_time(d2)
+    aoa.capi.check(lib_.aoa_memcpy_d2h(ctx.handle, aoa.capi.ptr(chk), buf.offset((npolys - 1) * K * N), chk.nbytes))
+    ctx.sync()
+    dgt_roundtrip_ok = bool(np.array_equal(chk, xs))
     algo_bytes = 16 * npolys * K * N          # read + write every coefficient once
     achieved = algo_bytes / (fwd_ms / 1000.0) / 1e9
     peak, peak_src = measured_peaks()
@@ -359,6 +459,11 @@ def main():
     for _ in range(5):
         aoa.ckks_decode(ctx, m_enc, N // 2, 1 << SCALE_BITS)
     dec_ms = (time.perf_counter() - t0) / 5 * 1000.0
+
+    # ---- batched uneven workload and serving loop ----------------------------------
+    uneven = serving = None
+    if not args.no_systems and world == 1:
+        uneven, serving = systems_workloads(aoa, torch)
 
     # ---- end to end through the C ABI with host buffers -----------------------------
     pin_in = [aoa.PinnedArray((2, K, N)) for _ in range(2 * B)]
@@ -433,7 +538,11 @@ def main():
             "batched_coefficient_inputs_ops_per_s": world * B / (coef_ms / 1000.0),
             "ntt": {"fwd_ms": fwd_ms, "inv_ms": inv_ms, "polys": npolys, "limbs": K,
                     "fwd_gbs": achieved, "inv_gbs": algo_bytes / (inv_ms / 1000.0) / 1e9,
-                    "hbm_frac": achieved / peak},
+                    "hbm_frac": achieved / peak, "inverse_of_forward_is_identity": roundtrip_ok,
+                    "forward_equals_oracle": fwd_matches_oracle, "cpu_baseline": ntt_cpu,
+                    "dgt_fwd_gbs": algo_bytes / (dgt256_fwd_ms / 1000.0) / 1e9,
+                    "dgt_inv_gbs": algo_bytes / (dgt256_inv_ms / 1000.0) / 1e9,
+                    "dgt_inverse_of_forward_is_identity": dgt_roundtrip_ok},
             "dgt": {"fwd_ms": dgt_fwd_ms, "inv_ms": dgt_inv_ms, "polys": 8, "limbs": K,
                     "fwd_gbs": dgt_bytes / (dgt_fwd_ms / 1000.0) / 1e9,
                     "inv_gbs": dgt_bytes / (dgt_inv_ms / 1000.0) / 1e9,
@@ -441,6 +550,8 @@ def main():
                     "path": "aoa-dgt ckks_mul on a DGT context (GI tensor and key products), inputs in the DGT domain"},
             "encoder": {"slots": N // 2, "limbs": K, "encode_ms_host_to_device": enc_ms,
                         "decode_ms_device_to_host": dec_ms},
+            "uneven_batch": uneven,
+            "serving": serving,
             "roofline": {"kernel": "ntt forward (column + row kernel pair), N=2^16", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_src, "algorithmic_bytes": algo_bytes, "traffic": traffic},

@@ -90,6 +90,11 @@ uint64_t aoa_primitive_root(uint64_t q);
  *     coexist (one per parameter set).  The engine binds the current device.   */
 int aoa_engine_create(const aoa_params* params, aoa_engine** out);
 int aoa_engine_destroy(aoa_engine* e);
+/* Launch-shape knobs, no reference counterpart (its kernel shapes are
+ * compile-time constants): "ntt_chunk_bytes" (bytes of limbs per transform
+ * launch pair, default 48 MiB so the column pass output stays in L2) and
+ * "ntt_waves" (transform CTAs per pass in resident waves, default 1).      */
+int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
 /* ring degree, prime count, primes (out may be NULL) */
 int aoa_engine_info(const aoa_engine* e, int* log_n, int* k, int* kl, uint64_t* primes_out);
 
@@ -242,6 +247,33 @@ int aoa_sub(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b);
 int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk);
 /* ckks_conjugate (ckks.cpp:1011-1040) */
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk);
+
+/* --- CUDA-graph capture of a context's asynchronous work (no reference
+ *     counterpart: the reference launches every kernel from the host).  Only
+ *     asynchronous calls may sit between begin and end, after each work size
+ *     has run once on the context (so nothing is allocated while capturing);
+ *     a synchronising call ends the capture with an error.                    */
+typedef struct aoa_graph aoa_graph;
+int aoa_ctx_capture_begin(aoa_ctx* c);
+int aoa_ctx_capture_end(aoa_ctx* c, aoa_graph** out);
+int aoa_graph_launch(aoa_ctx* c, aoa_graph* g);
+int aoa_graph_nodes(const aoa_graph* g, long* nodes);
+int aoa_graph_destroy(aoa_graph* g);
+
+/* --- plaintext / constant operations and slot sums (ckks.cpp:484-690).   */
+/* ckks_mul / ckks_mul_without_rescale by an encoded plaintext (ckks.cpp:
+ * 610-676): out = in * pt, scale = floor(in.scale * pt_scale / q_level),
+ * rescaled when `rescale` != 0.  d_pt: [k][N] in pt_domain.                */
+int aoa_mul_plaintext(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const uint64_t* d_pt, int pt_domain, uint64_t pt_scale,
+                      int rescale);
+/* ckks_mul(_without_rescale) by a double (ckks.cpp:540-592): x = lrint(|val|
+ * scale), negated for val < 0, scale = floor(scale^2 / q_level).            */
+int aoa_mul_const(aoa_ctx* c, aoa_ct* out, aoa_ct* in, double val, int rescale);
+/* ckks_add(ctx, c2, c1, double) (ckks.cpp:512-530): c0 +/- (uint64)(|val| scale). */
+int aoa_add_const(aoa_ctx* c, aoa_ct* out, aoa_ct* in, double val);
+/* ckks_sumslots (ckks.cpp:484-500): rotate-and-add over slots/2 .. 1;
+ * rtks[j] is the left-rotation key for 2^j.                                */
+int aoa_sumslots(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* const* rtks, int nkeys);
 
 /* --- encoder and encryption (src/ckks/encoder.cu:12-298, ckks.cpp:87-192,
  *     CKKSContext::encode/decode ckkscontext.cpp:5-38).  Complex values are
