@@ -37,6 +37,7 @@ constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration
 struct Tune {
   long ntt_chunk_bytes = 48L << 20;   // per NTT launch pair: stays inside L2
   double ntt_waves = 1.0;             // transform CTAs per pass, in resident waves
+  bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
 };
 
 // Device copy of the basis-conversion / rescale constants.
@@ -57,6 +58,12 @@ struct RnsTables {
   ShoupW* resc_inv = nullptr;
   // B mod q_i for rho (manager.cu:149-160), Shoup form; zero on B primes
   ShoupW* bmodq = nullptr;
+  // Tensor-core conversion images (k <= 32 and kl <= 32): for each table
+  // (ModUp at level l, then ModDown) a 128 KiB byte matrix in the shared-memory
+  // layout of the conversion's int8 MMA: [k-chunk 16][n 512][16 bytes], row
+  // n = out*16 + d, byte k = in*8 + a holding byte (d - a) of the table entry.
+  uint8_t* tc_modup = nullptr;     // [k][131072]
+  uint8_t* tc_moddown = nullptr;   // [131072]
 };
 
 struct Engine {

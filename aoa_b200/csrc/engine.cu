@@ -156,6 +156,25 @@ static void build_rns_tables(Engine& E) {
   std::vector<ShoupW> resc((size_t)k * k, ShoupW{0, 0});
   for (int l = 1; l < k; l++)
     for (int i = 0; i < l; i++) resc[(size_t)l * k + i] = sh(h_invmod(P[l] % P[i], P[i]), P[i]);
+  if (k <= 32 && kl >= 1 && kl <= 32 && E.N % 128 == 0) {
+    constexpr size_t kImg = 131072;
+    auto image = [](const uint64_t* mat, int ld, int nin, int nout, uint8_t* img) {
+      for (int in = 0; in < nin; in++)
+        for (int out = 0; out < nout; out++) {
+          const uint64_t h = mat[(size_t)in * ld + out];
+          for (int a = 0; a < 8; a++)
+            for (int b = 0; b < 8; b++) {
+              const int kb = in * 8 + a, n = out * 16 + a + b;
+              img[((size_t)(kb / 16) * 512 + n) * 16 + kb % 16] = (uint8_t)(h >> (8 * b));
+            }
+        }
+    };
+    std::vector<uint8_t> up((size_t)k * kImg, 0), down(kImg, 0);
+    for (int l = 0; l < k; l++) image(modup_hat.data() + (size_t)l * k * kl, kl, l + 1, kl, up.data() + l * kImg);
+    image(moddown_hat.data(), k, kl, k, down.data());
+    E.rns.tc_modup = dev_upload(E, up);
+    E.rns.tc_moddown = dev_upload(E, down);
+  }
   E.rns.modup_inv = dev_upload(E, modup_inv);
   E.rns.modup_hat = dev_upload(E, modup_hat);
   E.rns.moddown_inv = dev_upload(E, moddown_inv);
@@ -265,6 +284,7 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   const std::string k(knob);
   if (k == "ntt_chunk_bytes" && value >= (1 << 20) && value <= 4e9) h->e.tune.ntt_chunk_bytes = (long)value;
   else if (k == "ntt_waves" && value > 0 && value <= 64) h->e.tune.ntt_waves = value;
+  else if (k == "conv_tensor_cores" && (value == 0 || value == 1)) h->e.tune.conv_tensor_cores = value != 0;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob or value out of range: " + k);
   return AOA_OK;
 }

@@ -22,6 +22,7 @@
 // sized so that the column-pass output is still in L2 when the row pass reads
 // it.
 #include "aoa_internal.h"
+#include "async.cuh"
 
 namespace aoa {
 
@@ -102,7 +103,6 @@ struct Bf<true> {
 // ---- explicit shared-memory accessors --------------------------------------------
 // (ld.shared / st.shared: keeps every on-chip access on the short-latency path)
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ uint64_t lds64(uint32_t a) {
   uint64_t v;
@@ -240,50 +240,6 @@ __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
     }
   }
 }
-
-// ---- asynchronous bulk copies (TMA engine) and mbarriers --------------------------
-
-constexpr int kSpinLimit = 1 << 20;     // bounded mbarrier waits
-
-__device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init_fence() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)), "r"(bytes)
-               : "memory");
-}
-
-// global -> shared bulk copy; bytes % 16 == 0, both addresses 16-byte aligned
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, unsigned bytes, uint64_t* mb) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-      "l"(src), "r"(bytes), "r"(smem_u32(mb))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* mb, unsigned parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(mb)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Waits for phase `parity` of the barrier; gives up after kSpinLimit tries.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
-  for (int i = 0; i < kSpinLimit; i++)
-    if (mbar_try_wait(mb, parity)) return true;
-  return false;
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // ---- kernels ---------------------------------------------------------------
 // Work items: limb l of poly p (item j = l * npolys + p) lives at

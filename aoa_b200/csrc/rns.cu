@@ -1,5 +1,6 @@
-// RNS basis conversion (ModUp / ModDown), rescale and the key-switch epilogues,
-// sm_100a CUDA cores.
+// RNS basis conversion (ModUp / ModDown), rescale and the key-switch epilogues.
+// The conversion runs on the int8 tensor cores (basis_convert_tc) when both
+// bases have at most 32 primes, else on the CUDA cores (basis_convert).
 //
 // Both conversions are small dense modular matrix products per coefficient:
 //   ModUp   (fast_conv_Q_to_B_opt, aoa-ntt src/cuda/manager.cu:180-223)
@@ -23,6 +24,7 @@
 //   kRescaleFused  both in one pass when all outputs 0..l fit one launch: the
 //               thread owning output l shares c_l through shared memory
 #include "aoa_internal.h"
+#include "async.cuh"
 
 namespace aoa {
 
@@ -53,7 +55,25 @@ struct ConvArgs {
   const PrimeConst* pc;
   int log_n;
   int mode;
+  const uint8_t* tc_b;      // tensor-core image of `mat` (null: CUDA-core kernel only)
+  unsigned* err;            // device error word
+  int npolys;
 };
+
+// Epilogue of the non-fused modes for output jj with the reduced sum r.
+__device__ __forceinline__ void conv_store(const ConvArgs& a, int jj, uint64_t r, uint64_t dv, uint64_t* out, long c,
+                                           long N, long poly) {
+  const PrimeConst& P = a.pc[a.out_prime0 + jj];
+  if (a.mode == kModDown) {
+    const uint64_t x = a.x[poly * a.x_poly_stride + (long)(jj - a.x_shift) * N + c];
+    r = shoup(sub_mod(x, r, P.q), a.binv[jj], P.q);
+  } else if (a.mode == kRescaleTop) {
+    r = sub_mod(dv, shoup(r, a.binv[jj], P.q), P.q);
+  } else if (a.mode == kRescaleY) {
+    r = add_mod(shoup(r, a.binv[jj], P.q), shoup(dv, 1, P.one_sh, P.q), P.q);
+  }
+  out[(long)(jj - a.out_shift) * N] = r;
+}
 
 __global__ void __launch_bounds__(kConvThreads, 2)
 basis_convert(ConvArgs a, int j_first, int j_end) {
@@ -115,19 +135,195 @@ basis_convert(ConvArgs a, int j_first, int j_end) {
     const int j = half * kConvAcc + jl;
     if (j < nout) {
       const int jj = j_first + j;
-      const PrimeConst& P = a.pc[a.out_prime0 + jj];
-      uint64_t r = reduce128(lo[jl], hi[jl], P);
-      if (a.mode == kModDown) {
-        const uint64_t x = a.x[blockIdx.y * a.x_poly_stride + (long)(jj - a.x_shift) * N + c];
-        r = shoup(sub_mod(x, r, P.q), a.binv[jj], P.q);
-      } else if (a.mode == kRescaleTop) {
-        r = sub_mod(dv, shoup(r, a.binv[jj], P.q), P.q);
-      } else if (a.mode == kRescaleY) {
-        r = add_mod(shoup(r, a.binv[jj], P.q), shoup(dv, 1, P.one_sh, P.q), P.q);
-      }
-      out[(long)(jj - a.out_shift) * N] = r;
+      conv_store(a, jj, reduce128(lo[jl], hi[jl], a.pc[a.out_prime0 + jj]), dv, out, c, N, blockIdx.y);
     }
   }
+}
+
+// ---- tensor-core variant ------------------------------------------------------------
+// The conversion as one int8 GEMM per 128-coefficient tile on the 5th-generation
+// tensor cores.  With the scaled inputs z_i split into their 8 bytes z_i[a]
+// and the table entries h_ij into bytes h_ij[b], the sum over i of z_i h_ij
+// is sum_d 2^(8d) S_jd with the diagonal sums S_jd = sum_i sum_(a+b=d)
+// z_i[a] h_ij[b] < 2^24 (at most 32 inputs).  That is C = A B with
+//   A[row][8i + a] = z_i[a]           (the bytes of z_i: just z_i stored as u64)
+//   B[8i + a][16j + d] = h_ij[d - a]  (0 outside 0 <= d - a < 8; precomputed image)
+// so one tcgen05.mma kind::i8 (M = 128, N = 256, K = 32 per instruction,
+// u8 x u8 -> s32 in tensor memory) computes 16 diagonal sums per output, for
+// two N halves and 8 K steps.  The epilogue reads each thread's 16 columns of
+// an output from tensor memory (tcgen05.ld), combines them into the exact
+// 128-bit sum and reduces it once, as the CUDA-core kernel does.
+// Shared memory (no swizzle, K-major "core matrices" of 8 rows x 16 bytes):
+//   A: [16 k-chunks][128 rows][16 B]   = 32 KiB, descriptor LBO 2048, SBO 128
+//   B: [16 k-chunks][512 rows][16 B]   = 128 KiB, descriptor LBO 8192, SBO 128
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 256;
+constexpr size_t kTcA = 16 * kTcRows * 16;
+constexpr size_t kTcB = 131072;
+constexpr size_t kTcSmem = kTcA + kTcB + 1024;
+constexpr uint32_t kTcCols = 512;
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);   // version 1, no swizzle
+}
+
+// instruction descriptor: s32 accumulator, u8 x u8, both K-major, M = 128, N = 256
+constexpr uint32_t kTcIdesc = (2u << 4) | (uint32_t(256 >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* mb) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mb))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// the exact sum of one output: sum_d S_d 2^(8d), d < 15, reduced mod P
+__device__ __forceinline__ uint64_t tc_combine(const uint32_t (&v)[16], const PrimeConst& P) {
+  uint64_t p[3];
+#pragma unroll
+  for (int g = 0; g < 3; g++) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int t = 0; t < 5; t++) acc += (uint64_t)v[5 * g + t] << (8 * t);
+    p[g] = acc;                                            // < 2^57
+  }
+  const unsigned __int128 t = (unsigned __int128)p[0] + ((unsigned __int128)p[1] << 40) +
+                              ((unsigned __int128)p[2] << 80);
+  return reduce128((uint64_t)t, (uint64_t)(t >> 64), P);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+basis_convert_tc(ConvArgs a, int j_first, int j_end) {
+  extern __shared__ __align__(1024) uint8_t tcs[];
+  __shared__ __align__(8) uint64_t mbar[2];                // [0] image loaded, [1] MMA done
+  __shared__ uint32_t tmem_slot;
+  uint8_t* As = tcs;
+  uint8_t* Bs = tcs + kTcA;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const long N = 1L << a.log_n;
+  const long tiles_per_poly = N / kTcRows;
+  const long ntiles = tiles_per_poly * a.npolys;
+  // zero A (inputs beyond nin stay zero), barriers, tensor memory, the table image
+  for (int e = threadIdx.x; e < (int)(kTcA / 16); e += blockDim.x) ((uint4*)As)[e] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    mbar_init_fence();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(kTcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&mbar[0], (unsigned)kTcB);
+    for (int c = 0; c < 8; c++) bulk_g2s(smem_u32(Bs + c * 16384), a.tc_b + c * 16384, 16384, &mbar[0]);
+  }
+  bool ok = __syncthreads_and(mbar_wait(&mbar[0], 0));
+  bool in_flight = false;                                  // an MMA group not yet waited for
+  const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
+  const int ksteps = (a.nin + 3) / 4;                      // 4 inputs (32 bytes) per MMA K step
+  const int nout = j_end - j_first;
+  uint32_t phase = 0;
+  for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const long poly = tile / tiles_per_poly;
+    const long c0 = (tile % tiles_per_poly) * kTcRows;
+    // A: row r, inputs 2p and 2p+1 as one 16-byte store at chunk p
+    {
+      const int r = threadIdx.x % kTcRows;
+      const uint64_t* in = a.in + poly * a.in_poly_stride + c0 + r;
+      for (int p = threadIdx.x / kTcRows; p < (a.nin + 1) / 2; p += kTcThreads / kTcRows) {
+        const int i0 = 2 * p, i1 = 2 * p + 1;
+        const uint64_t z0 = shoup(in[(long)i0 * N], a.zc[i0], a.pc[a.in_prime0 + i0].q);
+        const uint64_t z1 = i1 < a.nin ? shoup(in[(long)i1 * N], a.zc[i1], a.pc[a.in_prime0 + i1].q) : 0;
+        *(uint4*)(As + (size_t)p * (kTcRows * 16) + r * 16) =
+            make_uint4((uint32_t)z0, (uint32_t)(z0 >> 32), (uint32_t)z1, (uint32_t)(z1 >> 32));
+      }
+    }
+    fence_proxy_async();                                   // generic smem writes -> tensor-core reads
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      for (int st = 0; st < ksteps; st++) {
+        const uint64_t ad = umma_desc(a_base + st * 2 * (kTcRows * 16), kTcRows * 16, 128);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const uint64_t bd = umma_desc(b_base + st * 2 * (512 * 16) + h * 256 * 16, 512 * 16, 128);
+          tc_mma(tmem + h * 256, ad, bd, st > 0);
+        }
+      }
+      tc_commit(&mbar[1]);
+    }
+    in_flight = true;
+    ok = !__syncthreads_or(!mbar_wait(&mbar[1], phase));
+    if (!ok) break;
+    in_flight = false;
+    phase ^= 1;
+    tc_fence_after();
+    // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 = tile rows;
+    // warps w and w + 4 split the outputs (even / odd)
+    const int g = warp % 4, par = warp / 4;
+    const int r = g * 32 + lane;
+    const long c = c0 + r;
+    const uint32_t t_lane = tmem + ((uint32_t)(g * 32) << 16);
+    uint64_t* out = a.out + poly * a.out_poly_stride + c;
+    uint64_t dv = 0;
+    if (a.mode >= kRescaleTop) dv = a.d[poly * a.d_poly_stride + c];
+    uint32_t v[16];
+    if (a.mode == kRescaleFused) {
+      const int l = j_end - 1;
+      tc_ld16(t_lane + l * 16, v);
+      const PrimeConst& Pl = a.pc[a.out_prime0 + l];
+      const uint64_t cl = sub_mod(dv, shoup(tc_combine(v, Pl), a.binv[l], Pl.q), Pl.q);
+      for (int j = par; j < l; j += 2) {
+        tc_ld16(t_lane + j * 16, v);
+        const PrimeConst& P = a.pc[a.out_prime0 + j];
+        out[(long)(j - a.out_shift) * N] =
+            add_mod(shoup(tc_combine(v, P), a.binv[j], P.q), shoup(cl, 1, P.one_sh, P.q), P.q);
+      }
+    } else {
+      for (int j = par; j < nout; j += 2) {
+        const int jj = j_first + j;
+        tc_ld16(t_lane + jj * 16, v);
+        conv_store(a, jj, tc_combine(v, a.pc[a.out_prime0 + jj]), dv, out, c, N, poly);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (!ok && threadIdx.x == 0) {
+    atomicOr(a.err, kErrWaitTimeout);
+    // let copies and MMAs in flight finish (bounded) before the memory is released
+    mbar_wait(&mbar[0], 0);
+    if (in_flight) mbar_wait(&mbar[1], phase);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
 }
 
 static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_begin, int j_end, cudaStream_t st) {
@@ -136,6 +332,16 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
   const size_t smem = (size_t)a.nin * kConvOut * sizeof(uint64_t);
   if (smem > 200 * 1024) throw AoaError(AOA_ERR_BAD_PARAM, "basis conversion: too many input limbs");
   dim3 grid(N / kConvCoefs, npolys);
+  if (a.tc_b && E.tune.conv_tensor_cores && a.nin <= 32 && j_end <= 32 && N % kTcRows == 0) {
+    ConvArgs t = a;
+    t.err = E.d_err;
+    t.npolys = npolys;
+    const long tiles = (N / kTcRows) * npolys;
+    basis_convert_tc<<<(unsigned)std::min<long>(tiles, E.num_sms), kTcThreads, kTcSmem, st>>>(t, j_begin, j_end);
+    note_launch();
+    AOA_CHECK_LAUNCH();
+    return;
+  }
   for (int j0 = j_begin; j0 < j_end; j0 += kConvOut) {
     basis_convert<<<grid, kConvThreads, smem, st>>>(a, j0, j_end);
     note_launch();
@@ -147,6 +353,7 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
 // conversion kernel needs, and check the 128-bit accumulation bound.
 void rns_init(Engine& E) {
   AOA_CUDA(cudaFuncSetAttribute(basis_convert, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
   auto bits = [](uint64_t x) { int b = 0; while (x) { b++; x >>= 1; } return b; };
   uint64_t mq = 0, mb = 0;
   for (int i = 0; i < E.k; i++) mq = std::max(mq, E.primes[i]);
@@ -168,6 +375,7 @@ void modup(const Engine& E, const uint64_t* in, long in_stride, uint64_t* out_b,
   a.in_prime0 = 0; a.out_prime0 = E.k;
   a.zc = E.rns.modup_inv + (long)level * E.k;
   a.mat = E.rns.modup_hat + (long)level * E.k * E.kl;
+  a.tc_b = E.rns.tc_modup ? E.rns.tc_modup + (size_t)level * 131072 : nullptr;
   a.pc = E.d_pc; a.log_n = E.log_n; a.mode = kRaw;
   run_convert(E, a, npolys, 0, E.kl, st);
 }
@@ -180,6 +388,7 @@ static ConvArgs moddown_args(const Engine& E, const uint64_t* in_b, long in_stri
   a.in_prime0 = E.k; a.out_prime0 = 0;
   a.zc = E.rns.moddown_inv;
   a.mat = E.rns.moddown_hat;
+  a.tc_b = E.rns.tc_moddown;
   a.binv = E.rns.moddown_binv; a.pc = E.d_pc; a.log_n = E.log_n;
   return a;
 }
