@@ -244,10 +244,11 @@ __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
 // ---- kernels ---------------------------------------------------------------
 // Work items: limb l of poly p (item j = l * npolys + p) lives at
 // data + (p * poly_stride + l) * N under prime first_prime + l.  grid =
-// (tiles per limb, G): CTA (x, y) handles tile x of items y, y + G, ... and
-// streams them through two shared-memory buffers filled by bulk copies, so the
-// next item's tile arrives while the current one is transformed.  Twiddles are
-// reloaded only when the limb changes.
+// (tiles per limb, G): CTA (x, y) handles tile x of the contiguous item range
+// [y * nitems / G, (y + 1) * nitems / G) — consecutive polys of one limb share
+// their twiddles, which are reloaded only when the limb changes — and streams
+// the items through two shared-memory buffers filled by bulk copies, so the
+// next item's tile arrives while the current one is transformed.
 
 struct NttBatch {
   uint64_t* data;
@@ -309,11 +310,12 @@ ntt_cols(NttBatch b) {
     }
   };
   int cur_limb = -1;
-  if ((int)blockIdx.y < b.nitems) issue(blockIdx.y, 0);
-  for (int j = blockIdx.y, it = 0; j < b.nitems; j += G, it++) {
+  const int j_lo = (int)((long)blockIdx.y * b.nitems / G), j_hi = (int)((long)(blockIdx.y + 1) * b.nitems / G);
+  if (j_lo < j_hi) issue(j_lo, 0);
+  for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
     const int bi = it & 1;
     const int limb = j / b.npolys, prime = b.first_prime + (limb >> b.prime_shift);
-    if (j + G < b.nitems) issue(j + G, bi ^ 1);
+    if (j + 1 < j_hi) issue(j + 1, bi ^ 1);
     if (limb != cur_limb) {                // previous users of tws passed the barrier below
       const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
       for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[e] = tw[e];
@@ -322,7 +324,7 @@ ntt_cols(NttBatch b) {
     const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
-      if (j + G < b.nitems) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);   // drain the copy in flight
+      if (j + 1 < j_hi) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);   // drain the copy in flight
       return;
     }
     const PrimeConst& P = b.pc[prime];
@@ -415,11 +417,12 @@ ntt_rows(NttBatch b) {
   ShoupW w2[D::G][D::L - 1];
   int cur_limb = -1;
   uint64_t q = 0;
-  if (threadIdx.x == 0 && (int)blockIdx.y < b.nitems) issue(blockIdx.y, 0);
-  for (int j = blockIdx.y, it = 0; j < b.nitems; j += G, it++) {
+  const int j_lo = (int)((long)blockIdx.y * b.nitems / G), j_hi = (int)((long)(blockIdx.y + 1) * b.nitems / G);
+  if (threadIdx.x == 0 && j_lo < j_hi) issue(j_lo, 0);
+  for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
     const int bi = it & 1;
     const int limb = j / b.npolys;
-    if (threadIdx.x == 0 && j + G < b.nitems) issue(j + G, bi ^ 1);
+    if (threadIdx.x == 0 && j + 1 < j_hi) issue(j + 1, bi ^ 1);
     if (limb != cur_limb) {
       const int prime = b.first_prime + (limb >> b.prime_shift);
       const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
@@ -435,7 +438,7 @@ ntt_rows(NttBatch b) {
     const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
-      if (j + G < b.nitems) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);
+      if (j + 1 < j_hi) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);
       return;
     }
     const uint32_t s = sbuf + (bi * TILE + rho * D::S) * 8;

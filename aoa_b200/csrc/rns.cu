@@ -157,7 +157,7 @@ basis_convert(ConvArgs a, int j_first, int j_end) {
 //   A: [16 k-chunks][128 rows][16 B]   = 32 KiB, descriptor LBO 2048, SBO 128
 //   B: [16 k-chunks][512 rows][16 B]   = 128 KiB, descriptor LBO 8192, SBO 128
 constexpr int kTcRows = 128;
-constexpr int kTcThreads = 256;
+constexpr int kTcThreads = 512;
 constexpr size_t kTcA = 16 * kTcRows * 16;
 constexpr size_t kTcB = 131072;
 constexpr size_t kTcSmem = kTcA + kTcB + 1024;
@@ -196,20 +196,38 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// the exact sum of one output: sum_d S_d 2^(8d), d < 15, reduced mod P
+// The exact sum of one output, sum_d S_d 2^(8d) (d < 15, S_d < 2^24), reduced
+// mod P.  Groups of four diagonals W_m = sum_t S_(4m+t) 2^(8t) < 2^51 are
+// formed with 32 x 32 -> 64-bit multiply-adds, then added at 32-bit offsets
+// 32m into the 128-bit total (below 2^126, so W_3 < 2^30 fits word 3).
 __device__ __forceinline__ uint64_t tc_combine(const uint32_t (&v)[16], const PrimeConst& P) {
-  uint64_t p[3];
+  uint64_t W[4];
 #pragma unroll
-  for (int g = 0; g < 3; g++) {
-    uint64_t acc = 0;
-#pragma unroll
-    for (int t = 0; t < 5; t++) acc += (uint64_t)v[5 * g + t] << (8 * t);
-    p[g] = acc;                                            // < 2^57
+  for (int m = 0; m < 4; m++) {
+    uint64_t w = v[4 * m];
+    asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(w) : "r"(v[4 * m + 1]));
+    asm("mad.wide.u32 %0, %1, 65536, %0;" : "+l"(w) : "r"(v[4 * m + 2]));
+    if (m < 3) asm("mad.wide.u32 %0, %1, 16777216, %0;" : "+l"(w) : "r"(v[4 * m + 3]));
+    W[m] = w;
   }
-  const unsigned __int128 t = (unsigned __int128)p[0] + ((unsigned __int128)p[1] << 40) +
-                              ((unsigned __int128)p[2] << 80);
-  return reduce128((uint64_t)t, (uint64_t)(t >> 64), P);
+  uint32_t r1, r2, r3;
+  asm("add.cc.u32 %0, %3, %4;\n\t"
+      "addc.cc.u32 %1, %5, %6;\n\t"
+      "addc.u32 %2, %7, %8;"
+      : "=r"(r1), "=r"(r2), "=r"(r3)
+      : "r"((uint32_t)(W[0] >> 32)), "r"((uint32_t)W[1]), "r"((uint32_t)(W[1] >> 32)), "r"((uint32_t)W[2]),
+        "r"((uint32_t)(W[2] >> 32)), "r"((uint32_t)W[3]));
+  const uint64_t lo = ((uint64_t)r1 << 32) | (uint32_t)W[0];
+  const uint64_t hi = ((uint64_t)r3 << 32) | r2;
+  return reduce128(lo, hi, P);
 }
+
+// Persistent: CTA b handles tiles b, b + grid, ...  Per tile: the inputs (loaded
+// into registers during the previous tile's MMA and epilogue) are scaled and
+// written to A, one thread issues the MMAs and commits them to an mbarrier,
+// and all 16 warps read tensor memory: warp w owns lanes 32 (w % 4) .. + 31
+// (tile rows) and every fourth output starting at w / 4.
+constexpr int kTcPairs = 32 / 2 / (kTcThreads / kTcRows);   // input pairs per thread (nin <= 32)
 
 __global__ void __launch_bounds__(kTcThreads, 1)
 basis_convert_tc(ConvArgs a, int j_first, int j_end) {
@@ -222,6 +240,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   const long N = 1L << a.log_n;
   const long tiles_per_poly = N / kTcRows;
   const long ntiles = tiles_per_poly * a.npolys;
+  const int npairs = (a.nin + 1) / 2;
   // zero A (inputs beyond nin stay zero), barriers, tensor memory, the table image
   for (int e = threadIdx.x; e < (int)(kTcA / 16); e += blockDim.x) ((uint4*)As)[e] = make_uint4(0, 0, 0, 0);
   if (threadIdx.x == 0) {
@@ -243,6 +262,20 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     mbar_expect_tx(&mbar[0], (unsigned)kTcB);
     for (int c = 0; c < 8; c++) bulk_g2s(smem_u32(Bs + c * 16384), a.tc_b + c * 16384, 16384, &mbar[0]);
   }
+  // this thread's A rows / input pairs, and its prefetched inputs
+  const int ar = threadIdx.x % kTcRows, ap = threadIdx.x / kTcRows;
+  uint64_t xa[kTcPairs], xb[kTcPairs];
+  auto load_inputs = [&](long tile) {
+    const long poly = tile / tiles_per_poly, c0 = (tile % tiles_per_poly) * kTcRows;
+    const uint64_t* in = a.in + poly * a.in_poly_stride + c0 + ar;
+#pragma unroll
+    for (int m = 0; m < kTcPairs; m++) {
+      const int p = ap + m * (kTcThreads / kTcRows);
+      xa[m] = p < npairs ? in[(long)(2 * p) * N] : 0;
+      xb[m] = 2 * p + 1 < a.nin ? in[(long)(2 * p + 1) * N] : 0;
+    }
+  };
+  if (blockIdx.x < ntiles) load_inputs(blockIdx.x);
   bool ok = __syncthreads_and(mbar_wait(&mbar[0], 0));
   bool in_flight = false;                                  // an MMA group not yet waited for
   const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
@@ -252,15 +285,15 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
     const long poly = tile / tiles_per_poly;
     const long c0 = (tile % tiles_per_poly) * kTcRows;
-    // A: row r, inputs 2p and 2p+1 as one 16-byte store at chunk p
-    {
-      const int r = threadIdx.x % kTcRows;
-      const uint64_t* in = a.in + poly * a.in_poly_stride + c0 + r;
-      for (int p = threadIdx.x / kTcRows; p < (a.nin + 1) / 2; p += kTcThreads / kTcRows) {
+    // A: row ar, inputs 2p and 2p + 1 as one 16-byte store at chunk p
+#pragma unroll
+    for (int m = 0; m < kTcPairs; m++) {
+      const int p = ap + m * (kTcThreads / kTcRows);
+      if (p < npairs) {
         const int i0 = 2 * p, i1 = 2 * p + 1;
-        const uint64_t z0 = shoup(in[(long)i0 * N], a.zc[i0], a.pc[a.in_prime0 + i0].q);
-        const uint64_t z1 = i1 < a.nin ? shoup(in[(long)i1 * N], a.zc[i1], a.pc[a.in_prime0 + i1].q) : 0;
-        *(uint4*)(As + (size_t)p * (kTcRows * 16) + r * 16) =
+        const uint64_t z0 = shoup(xa[m], a.zc[i0], a.pc[a.in_prime0 + i0].q);
+        const uint64_t z1 = i1 < a.nin ? shoup(xb[m], a.zc[i1], a.pc[a.in_prime0 + i1].q) : 0;
+        *(uint4*)(As + (size_t)p * (kTcRows * 16) + ar * 16) =
             make_uint4((uint32_t)z0, (uint32_t)(z0 >> 32), (uint32_t)z1, (uint32_t)(z1 >> 32));
       }
     }
@@ -279,16 +312,14 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       tc_commit(&mbar[1]);
     }
     in_flight = true;
+    if (tile + gridDim.x < ntiles) load_inputs(tile + gridDim.x);   // overlaps the MMAs and the epilogue
     ok = !__syncthreads_or(!mbar_wait(&mbar[1], phase));
     if (!ok) break;
     in_flight = false;
     phase ^= 1;
     tc_fence_after();
-    // epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 = tile rows;
-    // warps w and w + 4 split the outputs (even / odd)
     const int g = warp % 4, par = warp / 4;
-    const int r = g * 32 + lane;
-    const long c = c0 + r;
+    const long c = c0 + g * 32 + lane;
     const uint32_t t_lane = tmem + ((uint32_t)(g * 32) << 16);
     uint64_t* out = a.out + poly * a.out_poly_stride + c;
     uint64_t dv = 0;
@@ -299,14 +330,14 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       tc_ld16(t_lane + l * 16, v);
       const PrimeConst& Pl = a.pc[a.out_prime0 + l];
       const uint64_t cl = sub_mod(dv, shoup(tc_combine(v, Pl), a.binv[l], Pl.q), Pl.q);
-      for (int j = par; j < l; j += 2) {
+      for (int j = par; j < l; j += kTcThreads / 128) {
         tc_ld16(t_lane + j * 16, v);
         const PrimeConst& P = a.pc[a.out_prime0 + j];
         out[(long)(j - a.out_shift) * N] =
             add_mod(shoup(tc_combine(v, P), a.binv[j], P.q), shoup(cl, 1, P.one_sh, P.q), P.q);
       }
     } else {
-      for (int j = par; j < nout; j += 2) {
+      for (int j = par; j < nout; j += kTcThreads / 128) {
         const int jj = j_first + j;
         tc_ld16(t_lane + jj * 16, v);
         conv_store(a, jj, tc_combine(v, a.pc[a.out_prime0 + jj]), dv, out, c, N, poly);
