@@ -45,8 +45,17 @@ class Engine:
         self.handle = h
 
     def tune(self, knob, value):
-        """Set a launch-shape knob ("ntt_chunk_bytes", "ntt_waves")."""
+        """Set a launch-shape knob ("ntt_chunk_bytes", "ntt_waves", "ntt_split",
+        "ntt_cols_div", "ntt_rows_div", "conv_tensor_cores")."""
         capi.check(capi.load().aoa_engine_tune(self.handle, knob.encode(), float(value)))
+
+    def autotune(self, limbs=0):
+        """Time candidate transform shapes on this engine's ring and keep the
+        fastest; returns the tuner's report (choice, timings in ms)."""
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        capi.check(capi.load().aoa_engine_autotune(self.handle, int(limbs), buf, len(buf)))
+        return json.loads(buf.value.decode())
 
     def close(self):
         if getattr(self, "handle", None):

@@ -38,6 +38,9 @@ struct Tune {
   long ntt_chunk_bytes = 48L << 20;   // per NTT launch pair: stays inside L2
   double ntt_waves = 1.0;             // transform CTAs per pass, in resident waves
   bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
+  int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split
+  int ntt_cols_div = 0;               // column-pass tile width: widest >> div (0..2)
+  int ntt_rows_div = 0;               // row-pass tile height: tallest >> div (0..2)
 };
 
 // Device copy of the basis-conversion / rescale constants.

@@ -263,24 +263,35 @@ struct NttBatch {
   int npolys, nitems;      // nitems = nlimbs * npolys
 };
 
-template <int LOG_S>
-constexpr int tile_words() { return Sub<LOG_S>::PER_CTA * Sub<LOG_S>::S; }
+// Tile widths: a column-pass CTA takes W = PER_CTA >> DIV columns (at least 2,
+// so that a row segment is a multiple of 16 bytes), a row-pass CTA takes
+// PER_CTA >> DIV rows (at least 1).  DIV is a tuning choice (0, 1, 2).
+template <int LOG_S, int DIV>
+struct ColTile {
+  static constexpr int W0 = Sub<LOG_S>::PER_CTA >> DIV;
+  static constexpr int W = W0 < 2 ? 2 : W0;
+  static constexpr int THREADS = Sub<LOG_S>::T * W;
+  static constexpr int MIN_BLOCKS = 768 / THREADS < 1 ? 1 : (768 / THREADS > 32 ? 32 : 768 / THREADS);
+  static constexpr size_t SMEM = 2 * (size_t)Sub<LOG_S>::S * W * 8 + (size_t)Sub<LOG_S>::S * sizeof(ShoupW);
+};
 
-template <int LOG_R>
-constexpr size_t cols_smem() { return 2 * tile_words<LOG_R>() * 8 + (size_t)Sub<LOG_R>::S * sizeof(ShoupW); }
-
-template <int LOG_C>
-constexpr size_t rows_smem() {
-  return 2 * tile_words<LOG_C>() * 8 + (size_t)Sub<LOG_C>::PER_CTA * (Sub<LOG_C>::E - 1) * sizeof(ShoupW);
-}
+template <int LOG_S, int DIV>
+struct RowTile {
+  static constexpr int R0 = Sub<LOG_S>::PER_CTA >> DIV;
+  static constexpr int ROWS = R0 < 1 ? 1 : R0;
+  static constexpr int THREADS = Sub<LOG_S>::T * ROWS;
+  static constexpr int MIN_BLOCKS = 512 / THREADS < 1 ? 1 : (512 / THREADS > 32 ? 32 : 512 / THREADS);
+  static constexpr size_t SMEM =
+      2 * (size_t)ROWS * Sub<LOG_S>::S * 8 + (size_t)ROWS * (Sub<LOG_S>::E - 1) * sizeof(ShoupW);
+};
 
 // Column pass.  Tile = S rows x W columns of one limb; its load is S bulk copies
 // of W*8 bytes (one per row) issued by warp 0.  Shared layout [S][W].
-template <int LOG_R, bool LAZY, bool FWD>
-__global__ void __launch_bounds__(Sub<LOG_R>::T * Sub<LOG_R>::PER_CTA, 3)
+template <int LOG_R, int DIV, bool LAZY, bool FWD>
+__global__ void __launch_bounds__(ColTile<LOG_R, DIV>::THREADS, ColTile<LOG_R, DIV>::MIN_BLOCKS)
 ntt_cols(NttBatch b) {
   using D = Sub<LOG_R>;
-  constexpr int W = D::PER_CTA;
+  constexpr int W = ColTile<LOG_R, DIV>::W;
   constexpr int TILE = D::S * W;
   extern __shared__ __align__(128) uint64_t dyn[];
   __shared__ __align__(8) uint64_t mbar[2];
@@ -383,11 +394,11 @@ __device__ __forceinline__ int swz(int hi, int lo) {
 }
 
 // Row pass.  Tile = ROWS contiguous rows of one limb: one bulk copy.
-template <int LOG_C, bool LAZY, bool FWD>
-__global__ void __launch_bounds__(Sub<LOG_C>::T * Sub<LOG_C>::PER_CTA, 2)
+template <int LOG_C, int DIV, bool LAZY, bool FWD>
+__global__ void __launch_bounds__(RowTile<LOG_C, DIV>::THREADS, RowTile<LOG_C, DIV>::MIN_BLOCKS)
 ntt_rows(NttBatch b) {
   using D = Sub<LOG_C>;
-  constexpr int ROWS = D::PER_CTA;
+  constexpr int ROWS = RowTile<LOG_C, DIV>::ROWS;
   constexpr int TILE = ROWS * D::S;
   constexpr int NT1 = D::E - 1;                           // high-digit twiddles per row
   extern __shared__ __align__(128) uint64_t dyn[];
@@ -514,61 +525,68 @@ ntt_rows(NttBatch b) {
 
 // ---- host launchers ----------------------------------------------------------
 
-template <int LOG_R, bool LAZY>
-static void launch_cols(const NttBatch& b, int ctas_per_tile, bool fwd, cudaStream_t st) {
-  constexpr int T = Sub<LOG_R>::T;
-  constexpr int W = Sub<LOG_R>::PER_CTA;
-  const int C = 1 << b.log_c;
-  if (C % W) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: column tile does not divide C");
-  dim3 grid(C / W, ctas_per_tile);
-  constexpr size_t smem = cols_smem<LOG_R>();
-  if (fwd) ntt_cols<LOG_R, LAZY, true><<<grid, T * W, smem, st>>>(b);
-  else ntt_cols<LOG_R, LAZY, false><<<grid, T * W, smem, st>>>(b);
-  note_launch();
-}
-
-template <int LOG_C, bool LAZY>
-static void launch_rows(const NttBatch& b, int ctas_per_tile, bool fwd, cudaStream_t st) {
-  constexpr int T = Sub<LOG_C>::T;
-  constexpr int ROWS = Sub<LOG_C>::PER_CTA;
-  const int R = 1 << b.log_r;
-  if (R % ROWS) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: row tile does not divide R");
-  dim3 grid(R / ROWS, ctas_per_tile);
-  constexpr size_t smem = rows_smem<LOG_C>();
-  if (fwd) ntt_rows<LOG_C, LAZY, true><<<grid, T * ROWS, smem, st>>>(b);
-  else ntt_rows<LOG_C, LAZY, false><<<grid, T * ROWS, smem, st>>>(b);
-  note_launch();
-}
-
-#define AOA_NTT_SIZES(X) X(5) X(6) X(7) X(8) X(9) X(10)
-
 // CTAs per tile column: about one resident wave of CTAs (blocks_per_sm per SM)
 static int ctas_per_tile(const Engine& E, int tiles, int items, int blocks_per_sm) {
   const int target = std::max(1, (int)(E.tune.ntt_waves * E.num_sms * blocks_per_sm) / std::max(1, tiles));
   return std::max(1, std::min(items, target));
 }
 
+template <int LOG_R, int DIV, bool LAZY>
+static void launch_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+  using Tl = ColTile<LOG_R, DIV>;
+  const int C = 1 << b.log_c;
+  if (C % Tl::W) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: column tile does not divide C");
+  dim3 grid(C / Tl::W, ctas_per_tile(E, C / Tl::W, b.nitems, Tl::MIN_BLOCKS));
+  if (fwd) ntt_cols<LOG_R, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  else ntt_cols<LOG_R, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  note_launch();
+}
+
+template <int LOG_C, int DIV, bool LAZY>
+static void launch_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+  using Tl = RowTile<LOG_C, DIV>;
+  const int R = 1 << b.log_r;
+  if (R % Tl::ROWS) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: row tile does not divide R");
+  dim3 grid(R / Tl::ROWS, ctas_per_tile(E, R / Tl::ROWS, b.nitems, Tl::MIN_BLOCKS));
+  if (fwd) ntt_rows<LOG_C, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  else ntt_rows<LOG_C, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  note_launch();
+}
+
+#define AOA_NTT_SIZES(X) X(5) X(6) X(7) X(8) X(9) X(10)
+
+// Tile width choice (DIV) for a launch: the engine's tuning for lazy
+// transforms; strict transforms (primes of 62 bits or more) use the widest.
+template <bool LAZY>
+static int tile_div(int knob) { return LAZY ? std::max(0, std::min(2, knob)) : 0; }
+
 template <bool LAZY>
 static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
-  const int tiles = (1 << b.log_c) / (1 << 4);
+  const int div = tile_div<LAZY>(E.tune.ntt_cols_div);
   switch (b.log_r) {
-#define AOA_CASE(s)                                                                                     \
-  case s:                                                                                               \
-    launch_cols<s, LAZY>(b, ctas_per_tile(E, (1 << b.log_c) / Sub<s>::PER_CTA, b.nitems, 3), fwd, st); \
+#define AOA_CASE(s)                                                \
+  case s:                                                          \
+    if constexpr (!LAZY) launch_cols<s, 0, false>(E, b, fwd, st);    \
+    else if (div == 0) launch_cols<s, 0, true>(E, b, fwd, st);      \
+    else if (div == 1) launch_cols<s, 1, true>(E, b, fwd, st);      \
+    else launch_cols<s, 2, true>(E, b, fwd, st);                    \
     break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
     default: throw AoaError(AOA_ERR_BAD_PARAM, "ntt: unsupported column size");
   }
-  (void)tiles;
 }
 
 template <bool LAZY>
 static void run_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+  const int div = tile_div<LAZY>(E.tune.ntt_rows_div);
   switch (b.log_c) {
-#define AOA_CASE(s)                                                                                     \
-  case s:                                                                                               \
-    launch_rows<s, LAZY>(b, ctas_per_tile(E, (1 << b.log_r) / Sub<s>::PER_CTA, b.nitems, 2), fwd, st); \
+#define AOA_CASE(s)                                                \
+  case s:                                                          \
+    if constexpr (!LAZY) launch_rows<s, 0, false>(E, b, fwd, st);    \
+    else if (div == 0) launch_rows<s, 0, true>(E, b, fwd, st);      \
+    else if (div == 1) launch_rows<s, 1, true>(E, b, fwd, st);      \
+    else launch_rows<s, 2, true>(E, b, fwd, st);                    \
     break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
@@ -581,17 +599,23 @@ static void allow_smem(K kernel, size_t bytes) {
   AOA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
+template <int S, int DIV>
+static void allow_size() {
+  allow_smem(ntt_cols<S, DIV, true, true>, ColTile<S, DIV>::SMEM);
+  allow_smem(ntt_cols<S, DIV, true, false>, ColTile<S, DIV>::SMEM);
+  allow_smem(ntt_rows<S, DIV, true, true>, RowTile<S, DIV>::SMEM);
+  allow_smem(ntt_rows<S, DIV, true, false>, RowTile<S, DIV>::SMEM);
+  if (DIV == 0) {
+    allow_smem(ntt_cols<S, 0, false, true>, ColTile<S, 0>::SMEM);
+    allow_smem(ntt_cols<S, 0, false, false>, ColTile<S, 0>::SMEM);
+    allow_smem(ntt_rows<S, 0, false, true>, RowTile<S, 0>::SMEM);
+    allow_smem(ntt_rows<S, 0, false, false>, RowTile<S, 0>::SMEM);
+  }
+}
+
 // Once per engine: opt every transform kernel in to its dynamic shared memory.
 void ntt_init(Engine& E) {
-#define AOA_ALLOW(s)                                                         \
-  allow_smem(ntt_cols<s, true, true>, cols_smem<s>());                       \
-  allow_smem(ntt_cols<s, true, false>, cols_smem<s>());                      \
-  allow_smem(ntt_cols<s, false, true>, cols_smem<s>());                      \
-  allow_smem(ntt_cols<s, false, false>, cols_smem<s>());                     \
-  allow_smem(ntt_rows<s, true, true>, rows_smem<s>());                       \
-  allow_smem(ntt_rows<s, true, false>, rows_smem<s>());                      \
-  allow_smem(ntt_rows<s, false, true>, rows_smem<s>());                      \
-  allow_smem(ntt_rows<s, false, false>, rows_smem<s>());
+#define AOA_ALLOW(s) allow_size<s, 0>(); allow_size<s, 1>(); allow_size<s, 2>();
   AOA_NTT_SIZES(AOA_ALLOW)
 #undef AOA_ALLOW
   int sms = 0;
@@ -654,7 +678,10 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
     throw AoaError(AOA_ERR_BAD_PARAM, "ntt: prime range out of bounds");
   NttBatch b;
   b.tw = T.tw; b.itw = T.itw; b.pc = T.pc; b.err = E.d_err;
-  b.log_n = T.log_n; b.log_c = T.log_n / 2; b.log_r = T.log_n - b.log_c;
+  b.log_n = T.log_n;
+  b.log_c = T.log_n / 2 + E.tune.ntt_split;
+  b.log_c = std::max(std::max(5, T.log_n - 10), std::min(std::min(10, T.log_n - 5), b.log_c));
+  b.log_r = T.log_n - b.log_c;
   b.first_prime = first_prime; b.prime_shift = T.prime_shift; b.poly_stride = poly_stride;
   if (T.log_n < 10) {
     b.npolys = npolys;

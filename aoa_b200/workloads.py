@@ -41,13 +41,15 @@ class UnevenBatch:
     limbs uniform in [min_limbs, k], op mix mul / rot / add."""
 
     def __init__(self, n_ops=512, seed=4, log_ns=(14, 15, 16), k=30, kl=31, min_limbs=4, mix=(0.5, 0.3, 0.2),
-                 inputs_per_n=4, scale_bits=50):
+                 inputs_per_n=4, scale_bits=50, autotune=False):
         rng = np.random.default_rng(seed)
         self.k, self.kl = k, kl
         primes = params.ntt_primes(60, 2 << max(log_ns), k + kl)
         self.engines, self.ctx, self.evk, self.rtk, self.inputs = {}, {}, {}, {}, {}
         for ln in log_ns:
             E = Engine(ln, primes[:k], primes[k:], scale_bits=scale_bits)
+            if autotune:
+                E.autotune()                  # transform launch shapes picked per ring degree
             ctx = Context(E)
             N = 1 << ln
             self.engines[ln], self.ctx[ln] = E, ctx
@@ -145,7 +147,7 @@ class Server:
     and the HBM budget holds its ciphertext buffers."""
 
     def __init__(self, log_ns=(15, 16), k=30, kl=31, slots_per_degree=4, hbm_budget=8 << 30, seed=5,
-                 scale_bits=50, n_slots_used=None):
+                 scale_bits=50, n_slots_used=None, autotune=False):
         rng = np.random.default_rng(seed)
         self.k, self.kl, self.log_ns = k, kl, log_ns
         primes = params.ntt_primes(60, 2 << max(log_ns), k + kl)
@@ -153,6 +155,8 @@ class Server:
         self.hbm_budget, self.hbm_used = hbm_budget, 0
         for ln in log_ns:
             E = Engine(ln, primes[:k], primes[k:], scale_bits=scale_bits)
+            if autotune:
+                E.autotune()
             N = 1 << ln
             self.engines[ln] = E
             ctxs = [Context(E) for _ in range(slots_per_degree)]

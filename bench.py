@@ -171,7 +171,7 @@ def systems_workloads(aoa, torch):
     {2^15, 2^16}, live limbs 6..30) at 5 Poisson rates relative to its measured
     saturation throughput."""
     from aoa_b200.workloads import UnevenBatch, Server
-    wb = UnevenBatch(n_ops=512, seed=4)
+    wb = UnevenBatch(n_ops=512, seed=4, autotune=True)
 
     def timed_multi(fn):
         wb.sync()
@@ -205,7 +205,7 @@ def systems_workloads(aoa, torch):
               "achieved_gbs": wb.bytes / (graph_ms / 1000.0) / 1e9,
               "schedule": "one stream per N, HMults grouped by limb count (<=64 per launch), CUDA graph per stream"}
     del wb
-    srv = Server(log_ns=(15, 16), slots_per_degree=4, hbm_budget=8 << 30)
+    srv = Server(log_ns=(15, 16), slots_per_degree=4, hbm_budget=8 << 30, autotune=True)
     reqs = srv.make_requests(48, seed=6)
     srv.run(reqs[:8], rate=None)                         # warm the contexts' workspaces
     lat, wall = srv.run(reqs, rate=None)
@@ -234,6 +234,8 @@ def main():
     ap.add_argument("--profile-case", choices=["ntt", "hmult"],
                     help="run a small fixed case for ncu captures (no timing, no JSON)")
     ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default transform launch shapes")
+    ap.add_argument("--knobs", default="", help="engine knobs name=value,... applied instead of the autotuner")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -252,6 +254,14 @@ def main():
 
     ps = primes()
     E = aoa.Engine(LOG_N, ps[:K], ps[K:], scale_bits=SCALE_BITS)
+    tuning = None
+    if args.knobs:
+        for kv in args.knobs.split(","):
+            k, v = kv.split("=")
+            E.tune(k, float(v))
+        tuning = {"knobs": args.knobs}
+    elif not args.no_autotune and not args.profile_case:
+        tuning = E.autotune()["choice"]
     ctx = aoa.Context(E)
     stream = torch.cuda.ExternalStream(ctx.stream)
     N = 1 << LOG_N
@@ -528,7 +538,8 @@ def main():
                        "dnum": 1, "level": K - 1, "prime_bits": 60, "scale_bits": SCALE_BITS,
                        "batch_per_gpu": B, "input_domain": "transform (state left by the previous HMult)",
                        "parallelism": "replicas",
-                       "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % B},
+                       "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % B,
+                       "transform_tuning": tuning},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "single_op_ops_per_s": float(1000.0 / np.mean(lat))},
             "plain_per_call": {"ops_per_s": world * B / (plain_ms / 1000.0),

@@ -88,3 +88,39 @@ def test_ntt_edge_values(ref_table):
     d = ctx.upload(x)
     ctx.ntt_fwd(d, 1, 0, 3)
     assert np.array_equal(d.numpy(), o.ntt_fwd(x))
+
+
+@pytest.mark.parametrize("log_n", [12, 15, 16])
+@pytest.mark.parametrize("shape", [(s, c, r) for s in (-2, -1, 0, 1, 2) for c, r in ((0, 0), (1, 2), (2, 1))])
+def test_ntt_launch_shapes_bit_exact(log_n, shape):
+    """Every split and tile shape the autotuner may pick gives the oracle's transform."""
+    require_gpu()
+    split, cdiv, rdiv = shape
+    ps = oracle.gen_ntt_primes(60, 2 << log_n, 3)
+    E, ctx, o = _engine_and_oracle(log_n, ps[:2], ps[2:])
+    E.tune("ntt_split", split)
+    E.tune("ntt_cols_div", cdiv)
+    E.tune("ntt_rows_div", rdiv)
+    rng = np.random.default_rng(log_n + 7 * (split + 2))
+    x = _rand(rng, ps, 1 << log_n, npolys=3)
+    d = ctx.upload(x)
+    ctx.ntt_fwd(d, 3, 0, 3)
+    X = d.numpy()
+    assert np.array_equal(X[2], o.ntt_fwd(x[2])), "forward mismatch"
+    ctx.ntt_inv(d, 3, 0, 3)
+    assert np.array_equal(d.numpy(), x), "inverse(forward(x)) != x"
+
+
+def test_autotune_keeps_results_bit_exact():
+    require_gpu()
+    ps = oracle.gen_ntt_primes(60, 1 << 15, 6)
+    E, ctx, o = _engine_and_oracle(14, ps[:4], ps[4:])
+    rep = E.autotune(limbs=64)
+    ch = rep["choice"]
+    assert -2 <= ch["ntt_split"] <= 2 and 0 <= ch["ntt_cols_div"] <= 2 and 0 <= ch["ntt_rows_div"] <= 2
+    assert rep["best_ms"] <= rep["start_ms"] * 1.0001 and len(rep["trials"]) >= 10
+    rng = np.random.default_rng(11)
+    x = _rand(rng, ps, 1 << 14, npolys=2)
+    d = ctx.upload(x)
+    ctx.ntt_fwd(d, 2, 0, 6)
+    assert np.array_equal(d.numpy()[1], o.ntt_fwd(x[1]))
