@@ -41,6 +41,10 @@ struct Tune {
   int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split
   int ntt_cols_div = 0;               // column-pass tile width: widest >> div (0..2)
   int ntt_rows_div = 0;               // row-pass tile height: tallest >> div (0..2)
+  // transform ends fused with their neighbours (bit mask): 1 out-of-place
+  // inverse instead of a copy, 2 key products in the special-limb forward
+  // transform, 4 key-switch combine in the corrections' forward transform
+  int fuse = 1;
 };
 
 // Device copy of the basis-conversion / rescale constants.
@@ -165,9 +169,47 @@ struct NttTables {
   int prime_shift = 0;     // limb l uses prime first + (l >> prime_shift)
   bool lazy = false;
 };
+// Fused ends of a limb transform.  NttIo::src: the first pass reads item
+// (p, l) from src + p * src_poly_stride + l * N instead of the data (an
+// out-of-place transform; the data is written).  NttIo::epi: what the last
+// pass of a FORWARD transform does with the finished value v of coefficient c
+// of item (p, l) under prime pr (p counts from the first poly of the call):
+//   kEpiStore       data = v
+//   kEpiKeyProduct  out + p*out_stride + l*N       = v * key[pr]           (b part)
+//                   (same) + out_poly1             = v * key[key_half + pr] (a part)
+//                   (the data is not written)
+//   kEpiCombine     the key-switch epilogue with y = v (ks_combine):
+//                   rescale: ((base + ks B^-1 - v) q_l^-1), else base + (ks - v) B^-1,
+//                   base = 0 for p >= base_polys; written to outp.p[p] (use_ptrs)
+//                   or out + p*out_stride, at l*N + c
+enum { kEpiStore = 0, kEpiKeyProduct = 1, kEpiCombine = 2 };
+enum { kFuseSource = 1, kFuseKeyProduct = 2, kFuseCombine = 4 };
+struct NttEpi {
+  int mode = kEpiStore;
+  uint64_t* out = nullptr;
+  long out_stride = 0, out_poly1 = 0;
+  const uint64_t* key = nullptr;
+  long key_half = 0;
+  const uint64_t* base = nullptr;
+  long base_stride = 0;
+  int base_polys = 0;
+  const uint64_t* ks = nullptr;
+  long ks_stride = 0;
+  const ShoupW* binv = nullptr;
+  const ShoupW* resc = nullptr;
+  int use_ptrs = 0;
+  OutPtrs outp;
+};
+struct NttIo {
+  const uint64_t* src = nullptr;
+  long src_poly_stride = 0;
+  NttEpi epi;
+};
 void ntt_init(Engine& E);
+void ntt_batch_io(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs, long poly_stride,
+                  bool forward, const NttIo& io, cudaStream_t st);
 void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int npolys, int first_prime, int nlimbs,
-                      long poly_stride, bool forward, cudaStream_t st);
+                      long poly_stride, bool forward, cudaStream_t st, const NttIo* io = nullptr);
 void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs,
                long poly_stride, bool forward, cudaStream_t st);
 
@@ -214,12 +256,12 @@ void tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* 
                uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st);
 void tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D, int n, int nlimbs, cudaStream_t st);
 void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
-                            const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st);
+                            const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st, int nb = -1);
 void ks_combine_ptr(const Engine& E, const OutPtrs& outp, const uint64_t* base, long base_stride, const uint64_t* k,
                     long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys, int rescale_level,
                     cudaStream_t st);
 void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
-                      uint64_t* k1, int nq, cudaStream_t st);
+                      uint64_t* k1, int nq, cudaStream_t st, int nb = -1);
 void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,
                        int nlimbs, int npolys, cudaStream_t st);
 void automorph_ntt_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,

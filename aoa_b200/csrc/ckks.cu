@@ -88,6 +88,36 @@ static void copy_limbs(Ctx& C, uint64_t* dst, const uint64_t* src, long words) {
 // (x_coef, x_ntt).  Leaves in w.KS = [x*b | x*a] (stride k + kl limbs): the Q
 // limbs in the transform domain, the kl B limbs back in coefficients.
 // (ModUp poly_modup, key products poly_mul, ckks.cpp:309-314.)
+// Fused transform ends (out-of-place inverse, key products, key-switch
+// combine; engine knob "fuse", a bit mask) on NTT contexts; DGT contexts take
+// the separate kernels.
+static bool fused(const Ctx& C, int what) { return C.transform == AOA_NTT && (C.E->tune.fuse & what); }
+
+// Forward transform of the corrections Y (npolys polys of stride k limbs,
+// limbs 0..nlimbs-1) with the key-switch combine as its epilogue.
+static void combine_into(Ctx& C, uint64_t* Y, int npolys, int nlimbs, const uint64_t* base, long base_stride,
+                         int base_polys, const uint64_t* KS, long ks_stride, int rescale_level, uint64_t* out,
+                         long out_stride, const OutPtrs* outp) {
+  const Engine& E = *C.E;
+  NttIo io;
+  io.epi.mode = kEpiCombine;
+  io.epi.base = base;
+  io.epi.base_stride = base_stride;
+  io.epi.base_polys = base ? base_polys : 0;
+  io.epi.ks = KS;
+  io.epi.ks_stride = ks_stride;
+  io.epi.binv = E.rns.moddown_binv;
+  io.epi.resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
+  if (outp) {
+    io.epi.use_ptrs = 1;
+    io.epi.outp = *outp;
+  } else {
+    io.epi.out = out;
+    io.epi.out_stride = out_stride;
+  }
+  ntt_batch_io(E, Y, npolys, 0, nlimbs, E.k, true, io, C.stream);
+}
+
 static void keyswitch_core(Ctx& C, const Workspace& w, const uint64_t* x_coef, const uint64_t* x_ntt,
                            const aoa_swk* key, int level) {
   const Engine& E = *C.E;
@@ -96,9 +126,22 @@ static void keyswitch_core(Ctx& C, const Workspace& w, const uint64_t* x_coef, c
   const int tk = C.transform;
   if (key->domain != tk) throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
   modup(E, x_coef, 0, w.UB, 0, 1, level, C.stream);
-  xform(E, tk, w.UB, 1, E.k, E.kl, E.kl, true, C.stream);
-  if (tk == AOA_DGT) gi_keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + (long)(E.k + E.kl) * N, m, C.stream);
-  else keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + (long)(E.k + E.kl) * N, m, C.stream);
+  const long ks = (long)(E.k + E.kl) * N;
+  if (fused(C, kFuseKeyProduct)) {
+    // forward transform of the special limbs with the key products as its epilogue
+    NttIo io;
+    io.epi.mode = kEpiKeyProduct;
+    io.epi.out = w.KS + (long)m * N;
+    io.epi.out_poly1 = ks;
+    io.epi.key = key->d;
+    io.epi.key_half = (long)E.nprimes * N;
+    ntt_batch_io(E, w.UB, 1, E.k, E.kl, E.kl, true, io, C.stream);
+    keyswitch_mul_op(E, x_ntt, nullptr, key->d, w.KS, w.KS + ks, m, C.stream, 0);
+  } else {
+    xform(E, tk, w.UB, 1, E.k, E.kl, E.kl, true, C.stream);
+    if (tk == AOA_DGT) gi_keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + ks, m, C.stream);
+    else keyswitch_mul_op(E, x_ntt, w.UB, key->d, w.KS, w.KS + ks, m, C.stream);
+  }
   xform(E, tk, w.KS + (long)m * N, 2, E.k, E.kl, E.k + E.kl, false, C.stream);
 }
 
@@ -133,6 +176,10 @@ static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long hal
     }
     xform(E, C.transform, U, 2, level, 1, 1, false, C.stream);
     rescale_corrections(E, kb, ks_stride, U, N, w.CL, N, w.Y, (long)E.k * N, 2, level, C.stream);
+    if (fused(C, kFuseCombine) && (!b1 || b1 == b0 + half)) {
+      combine_into(C, w.Y, 2, level, b0, half, b1 ? 2 : 1, w.KS, ks_stride, level, out, half, nullptr);
+      return;
+    }
     xform(E, C.transform, w.Y, 2, 0, level, E.k, true, C.stream);
     if (b0 && b1 == b0 + half) {
       ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, level, 2, level, C.stream);
@@ -142,6 +189,10 @@ static void keyswitch_finish(Ctx& C, const Workspace& w, uint64_t* out, long hal
     }
   } else {
     moddown_conv(E, kb, ks_stride, w.Y, (long)E.k * N, 2, m, C.stream);
+    if (fused(C, kFuseCombine) && (!b1 || b1 == b0 + half)) {
+      combine_into(C, w.Y, 2, m, b0, half, b1 ? 2 : 1, w.KS, ks_stride, 0, out, half, nullptr);
+      return;
+    }
     xform(E, C.transform, w.Y, 2, 0, m, E.k, true, C.stream);
     if (b0 && b1 == b0 + half) {
       ks_combine(E, out, half, b0, half, w.KS, ks_stride, w.Y, (long)E.k * N, m, 2, 0, C.stream);
@@ -176,8 +227,15 @@ static void hmult_core(Ctx& C, const Workspace& w, aoa_ct* out, aoa_ct* a, aoa_c
   else tensor_op(E, a->d, half, b->d, half, D0, D0 + half, D2, m, C.stream);
   const uint64_t sa = a->scale, sb = b->scale;
   const int slots = a->slots;
-  copy_limbs(C, w.T, D2, (long)m * N);
-  xform(E, tk, w.T, 1, 0, m, m, false, C.stream);
+  if (fused(C, kFuseSource)) {
+    NttIo io;                                  // inverse of d2 read in place of a copy
+    io.src = D2;
+    io.src_poly_stride = m;
+    ntt_batch_io(E, w.T, 1, 0, m, m, false, io, C.stream);
+  } else {
+    copy_limbs(C, w.T, D2, (long)m * N);
+    xform(E, tk, w.T, 1, 0, m, m, false, C.stream);
+  }
   keyswitch_core(C, w, w.T, D2, evk, level);
   keyswitch_finish(C, w, out->d, half, D0, D0 + half, level, do_rescale);
   out->level = do_rescale ? level - 1 : level;
@@ -236,8 +294,15 @@ void apply_galois(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* k
     to_domain(C, in, AOA_NTT, m);
     automorph_ntt_op(E, w.R0, in->d, 0, galois, m, 1, C.stream);
     automorph_ntt_op(E, X, in->d + half, 0, galois, m, 1, C.stream);
-    copy_limbs(C, w.T, X, (long)m * N);
-    ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+    if (fused(C, kFuseSource)) {
+      NttIo io;                                // inverse read out of place
+      io.src = X;
+      io.src_poly_stride = m;
+      ntt_batch_io(E, w.T, 1, 0, m, m, false, io, C.stream);
+    } else {
+      copy_limbs(C, w.T, X, (long)m * N);
+      ntt_batch(E, w.T, 1, 0, m, m, false, C.stream);
+    }
   }
   keyswitch_core(C, w, w.T, X, key, level);
   keyswitch_finish(C, w, out->d, half, w.R0, nullptr, level, false);
@@ -297,11 +362,31 @@ static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* 
   }
   tensor_batch_op(E, ptr, half, D, n, m, st);
   uint64_t* D2 = D + 2L * n * half;
-  AOA_CUDA(cudaMemcpy2DAsync(T, half * 8, D2, half * 8, (size_t)m * N * 8, n, cudaMemcpyDeviceToDevice, st));
-  ntt_batch(E, T, n, 0, m, k, false, st);
+  const int fuse = E.tune.fuse;
+  if (fuse & kFuseSource) {
+    NttIo io;                                  // inverse of d2 read in place of a copy
+    io.src = D2;
+    io.src_poly_stride = k;
+    ntt_batch_io(E, T, n, 0, m, k, false, io, st);
+  } else {
+    AOA_CUDA(cudaMemcpy2DAsync(T, half * 8, D2, half * 8, (size_t)m * N * 8, n, cudaMemcpyDeviceToDevice, st));
+    ntt_batch(E, T, n, 0, m, k, false, st);
+  }
   modup(E, T, half, UB, (long)kl * N, n, level, st);
-  ntt_batch(E, UB, n, k, kl, kl, true, st);
-  keyswitch_mul_batch_op(E, D2, half, UB, (long)kl * N, evk->d, KS, ks, n, m, st);
+  if (fuse & kFuseKeyProduct) {
+    NttIo io;                                  // special-limb transform with the key products fused
+    io.epi.mode = kEpiKeyProduct;
+    io.epi.out = KS + (long)m * N;
+    io.epi.out_stride = ks;
+    io.epi.out_poly1 = (long)n * ks;
+    io.epi.key = evk->d;
+    io.epi.key_half = (long)E.nprimes * N;
+    ntt_batch_io(E, UB, n, k, kl, kl, true, io, st);
+    keyswitch_mul_batch_op(E, D2, half, nullptr, 0, evk->d, KS, ks, n, m, st, 0);
+  } else {
+    ntt_batch(E, UB, n, k, kl, kl, true, st);
+    keyswitch_mul_batch_op(E, D2, half, UB, (long)kl * N, evk->d, KS, ks, n, m, st);
+  }
   ntt_batch(E, KS + (long)m * N, 2 * n, k, kl, k + kl, false, st);
   OutPtrs outp;
   for (int z = 0; z < n; z++) {
@@ -312,12 +397,20 @@ static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* 
     ks_combine(E, U, N, D + (long)level * N, half, KS + (long)level * N, ks, nullptr, 0, 1, 2 * n, 0, st, level);
     ntt_batch(E, U, 2 * n, level, 1, 1, false, st);
     rescale_corrections(E, KS + (long)m * N, ks, U, N, CL, N, Y, half, 2 * n, level, st);
-    ntt_batch(E, Y, 2 * n, 0, level, k, true, st);
-    ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, level, 2 * n, level, st);
+    if (fuse & kFuseCombine) {
+      combine_into(C, Y, 2 * n, level, D, half, 2 * n, KS, ks, level, nullptr, 0, &outp);
+    } else {
+      ntt_batch(E, Y, 2 * n, 0, level, k, true, st);
+      ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, level, 2 * n, level, st);
+    }
   } else {
     moddown_conv(E, KS + (long)m * N, ks, Y, half, 2 * n, m, st);
-    ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
-    ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, m, 2 * n, 0, st);
+    if (fuse & kFuseCombine) {
+      combine_into(C, Y, 2 * n, m, D, half, 2 * n, KS, ks, 0, nullptr, 0, &outp);
+    } else {
+      ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
+      ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, m, 2 * n, 0, st);
+    }
   }
   for (int z = 0; z < n; z++) {
     out[z]->level = do_rescale ? level - 1 : level;

@@ -241,6 +241,41 @@ __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
   }
 }
 
+// ---- fused epilogue of a forward transform ----------------------------------------
+__device__ __forceinline__ void epi_store(const NttEpi& e, long N, long p, int limb, int prime, long c, uint64_t v,
+                                          const PrimeConst& P) {
+  const long off = (long)limb * N + c;
+  if (e.mode == kEpiKeyProduct) {
+    const uint64_t kb = e.key[(long)prime * N + c], ka = e.key[e.key_half + (long)prime * N + c];
+    uint64_t* o = e.out + p * e.out_stride + off;
+    o[0] = mul_mod(v, kb, P);
+    o[e.out_poly1] = mul_mod(v, ka, P);
+  } else {
+    const uint64_t q = P.q;
+    const uint64_t kv = e.ks[p * e.ks_stride + off];
+    const uint64_t bv = p < e.base_polys ? e.base[p * e.base_stride + off] : 0;
+    uint64_t r;
+    if (e.resc) r = shoup(sub_mod(add_mod(bv, shoup(kv, e.binv[prime], q), q), v, q), e.resc[prime], q);
+    else r = add_mod(bv, shoup(sub_mod(kv, v, q), e.binv[prime], q), q);
+    uint64_t* o = e.use_ptrs ? e.outp.p[p] : e.out + p * e.out_stride;
+    o[off] = r;
+  }
+}
+
+// the same epilogue as a separate pass over transformed data (small rings)
+__global__ void ntt_epilogue_kernel(const uint64_t* data, long poly_stride, int npolys, int nlimbs, int first_prime,
+                                    int prime_shift, const PrimeConst* pc, int log_n, const __grid_constant__ NttEpi e) {
+  const long N = 1L << log_n;
+  const long total = (long)npolys * nlimbs * N;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long c = i % N;
+    const int limb = (int)((i / N) % nlimbs);
+    const long p = i / N / nlimbs;
+    const int prime = first_prime + (limb >> prime_shift);
+    epi_store(e, N, p, limb, prime, c, data[(p * poly_stride + limb) * N + c], pc[prime]);
+  }
+}
+
 // ---- kernels ---------------------------------------------------------------
 // Work items: limb l of poly p (item j = l * npolys + p) lives at
 // data + (p * poly_stride + l) * N under prime first_prime + l.  grid =
@@ -261,6 +296,9 @@ struct NttBatch {
   int prime_shift;         // limb l uses prime first_prime + (l >> prime_shift)
   long poly_stride;        // limbs between consecutive polys
   int npolys, nitems;      // nitems = nlimbs * npolys
+  const uint64_t* src;     // this pass loads from src (out of place) when set
+  long src_poly_stride;
+  int poly_base;           // poly index of the launch's first poly within the call
 };
 
 // Tile widths: a column-pass CTA takes W = PER_CTA >> DIV columns (at least 2,
@@ -309,6 +347,11 @@ ntt_cols(NttBatch b) {
   __syncthreads();
   auto src_of = [&](int j) -> const uint64_t* {
     const int limb = j / b.npolys, p = j % b.npolys;
+    if (b.src) return b.src + ((long)p * b.src_poly_stride + limb) * N + (long)blockIdx.x * W;
+    return b.data + ((long)p * b.poly_stride + limb) * N + (long)blockIdx.x * W;
+  };
+  auto dst_of = [&](int j) -> uint64_t* {
+    const int limb = j / b.npolys, p = j % b.npolys;
     return b.data + ((long)p * b.poly_stride + limb) * N + (long)blockIdx.x * W;
   };
   auto issue = [&](int j, int bi) {        // warp 0: S row segments of W words
@@ -341,7 +384,7 @@ ntt_cols(NttBatch b) {
     const PrimeConst& P = b.pc[prime];
     const uint64_t q = P.q;
     const uint32_t sm = sbuf + bi * TILE * 8 + w * 8;            // + row * W * 8
-    uint64_t* x = const_cast<uint64_t*>(src_of(j)) + w;
+    uint64_t* x = dst_of(j) + w;
     if (FWD) {
       uint64_t v[D::E];
 #pragma unroll
@@ -396,7 +439,7 @@ __device__ __forceinline__ int swz(int hi, int lo) {
 // Row pass.  Tile = ROWS contiguous rows of one limb: one bulk copy.
 template <int LOG_C, int DIV, bool LAZY, bool FWD>
 __global__ void __launch_bounds__(RowTile<LOG_C, DIV>::THREADS, RowTile<LOG_C, DIV>::MIN_BLOCKS)
-ntt_rows(NttBatch b) {
+ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
   using D = Sub<LOG_C>;
   constexpr int ROWS = RowTile<LOG_C, DIV>::ROWS;
   constexpr int TILE = ROWS * D::S;
@@ -417,7 +460,12 @@ ntt_rows(NttBatch b) {
     mbar_init_fence();
   }
   __syncthreads();
-  auto src_of = [&](int j) -> uint64_t* {
+  auto src_of = [&](int j) -> const uint64_t* {
+    const int limb = j / b.npolys, p = j % b.npolys;
+    if (b.src) return b.src + ((long)p * b.src_poly_stride + limb) * N + ((long)row0 << LOG_C);
+    return b.data + ((long)p * b.poly_stride + limb) * N + ((long)row0 << LOG_C);
+  };
+  auto dst_of = [&](int j) -> uint64_t* {
     const int limb = j / b.npolys, p = j % b.npolys;
     return b.data + ((long)p * b.poly_stride + limb) * N + ((long)row0 << LOG_C);
   };
@@ -453,7 +501,7 @@ ntt_rows(NttBatch b) {
       return;
     }
     const uint32_t s = sbuf + (bi * TILE + rho * D::S) * 8;
-    uint64_t* x = src_of(j) + rho * D::S;
+    uint64_t* x = dst_of(j) + rho * D::S;
     uint64_t v[D::E];
     if (FWD) {
 #pragma unroll
@@ -483,8 +531,20 @@ ntt_rows(NttBatch b) {
         for (int l = 0; l < D::L; l++) sts64(s + swz<LOG_C>(hi, l) * 8, u[l]);
       }
       __syncwarp();
+      if (epi.mode == kEpiStore) {
 #pragma unroll
-      for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = Bf<LAZY>::fwd_out(lds64(s + swz<LOG_C>(h, t) * 8), q);
+        for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = Bf<LAZY>::fwd_out(lds64(s + swz<LOG_C>(h, t) * 8), q);
+      } else {
+        const int limb = j / b.npolys;
+        const long p = b.poly_base + j % b.npolys;
+        const int prime = b.first_prime + (limb >> b.prime_shift);
+        const PrimeConst& P = b.pc[prime];
+        const long c0 = (long)(row0 + rho) << LOG_C;
+#pragma unroll
+        for (int h = 0; h < D::E; h++)
+          epi_store(epi, N, p, limb, prime, c0 + (h << D::LO) + t, Bf<LAZY>::fwd_out(lds64(s + swz<LOG_C>(h, t) * 8), q),
+                    P);
+      }
     } else {
 #pragma unroll
       for (int h = 0; h < D::E; h++) v[h] = lds64(s + ((h << D::LO) + t) * 8);
@@ -543,13 +603,13 @@ static void launch_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream
 }
 
 template <int LOG_C, int DIV, bool LAZY>
-static void launch_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+static void launch_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st, const NttEpi& epi) {
   using Tl = RowTile<LOG_C, DIV>;
   const int R = 1 << b.log_r;
   if (R % Tl::ROWS) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: row tile does not divide R");
   dim3 grid(R / Tl::ROWS, ctas_per_tile(E, R / Tl::ROWS, b.nitems, Tl::MIN_BLOCKS));
-  if (fwd) ntt_rows<LOG_C, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
-  else ntt_rows<LOG_C, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  if (fwd) ntt_rows<LOG_C, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, epi);
+  else ntt_rows<LOG_C, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, epi);
   note_launch();
 }
 
@@ -578,15 +638,15 @@ static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t 
 }
 
 template <bool LAZY>
-static void run_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+static void run_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st, const NttEpi& epi) {
   const int div = tile_div<LAZY>(E.tune.ntt_rows_div);
   switch (b.log_c) {
 #define AOA_CASE(s)                                                \
   case s:                                                          \
-    if constexpr (!LAZY) launch_rows<s, 0, false>(E, b, fwd, st);    \
-    else if (div == 0) launch_rows<s, 0, true>(E, b, fwd, st);      \
-    else if (div == 1) launch_rows<s, 1, true>(E, b, fwd, st);      \
-    else launch_rows<s, 2, true>(E, b, fwd, st);                    \
+    if constexpr (!LAZY) launch_rows<s, 0, false>(E, b, fwd, st, epi);    \
+    else if (div == 0) launch_rows<s, 0, true>(E, b, fwd, st, epi);      \
+    else if (div == 1) launch_rows<s, 1, true>(E, b, fwd, st, epi);      \
+    else launch_rows<s, 2, true>(E, b, fwd, st, epi);                    \
     break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
@@ -672,10 +732,13 @@ __global__ void ntt_small(NttBatch b, bool fwd) {
 // (l >> T.prime_shift).  Large transforms are split into chunks of whole polys
 // whose total size stays within the L2 budget, column and row pass per chunk.
 void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int npolys, int first_prime, int nlimbs,
-                      long poly_stride, bool forward, cudaStream_t st) {
+                      long poly_stride, bool forward, cudaStream_t st, const NttIo* io) {
   if (npolys <= 0 || nlimbs <= 0) return;
   if (first_prime < 0 || first_prime + ((nlimbs - 1) >> T.prime_shift) >= E.nprimes)
     throw AoaError(AOA_ERR_BAD_PARAM, "ntt: prime range out of bounds");
+  const NttEpi no_epi{};
+  const NttEpi& epi = io ? io->epi : no_epi;
+  if (epi.mode != kEpiStore && !forward) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: epilogues are for forward transforms");
   NttBatch b;
   b.tw = T.tw; b.itw = T.itw; b.pc = T.pc; b.err = E.d_err;
   b.log_n = T.log_n;
@@ -683,30 +746,47 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   b.log_c = std::max(std::max(5, T.log_n - 10), std::min(std::min(10, T.log_n - 5), b.log_c));
   b.log_r = T.log_n - b.log_c;
   b.first_prime = first_prime; b.prime_shift = T.prime_shift; b.poly_stride = poly_stride;
+  b.src = nullptr; b.src_poly_stride = 0; b.poly_base = 0;
+  const long n = 1L << T.log_n;
   if (T.log_n < 10) {
+    // small rings: the out-of-place source is copied first and the epilogue
+    // runs as its own pass
+    if (io && io->src)
+      AOA_CUDA(cudaMemcpy2DAsync(data, poly_stride * n * 8, io->src, io->src_poly_stride * n * 8,
+                                 (size_t)nlimbs * n * 8, npolys, cudaMemcpyDeviceToDevice, st));
     b.npolys = npolys;
     b.nitems = npolys * nlimbs;
     b.data = data;
-    const int n = 1 << T.log_n;
     const int grid = std::min(b.nitems, 8 * E.num_sms);
-    ntt_small<<<grid, std::max(32, std::min(n / 2, 256)), n * 8, st>>>(b, forward);
+    ntt_small<<<grid, std::max(32, std::min((int)n / 2, 256)), n * 8, st>>>(b, forward);
     note_launch();
+    if (epi.mode != kEpiStore) {
+      ntt_epilogue_kernel<<<2 * E.num_sms, 256, 0, st>>>(data, poly_stride, npolys, nlimbs, first_prime,
+                                                         T.prime_shift, T.pc, T.log_n, epi);
+      note_launch();
+    }
     AOA_CHECK_LAUNCH();
     return;
   }
-  const long limb_bytes = (8L << T.log_n);
+  const long limb_bytes = 8 * n;
   const long chunk = std::max(1L, E.tune.ntt_chunk_bytes / (limb_bytes * nlimbs));
   for (long c0 = 0; c0 < npolys; c0 += chunk) {
     const int np = (int)std::min<long>(chunk, npolys - c0);
     b.npolys = np;
     b.nitems = np * nlimbs;
-    b.data = data + c0 * poly_stride * (1L << T.log_n);
+    b.data = data + c0 * poly_stride * n;
+    b.poly_base = (int)c0;
+    NttBatch first = b;                    // the first pass may read out of place
+    if (io && io->src) {
+      first.src = io->src + c0 * io->src_poly_stride * n;
+      first.src_poly_stride = io->src_poly_stride;
+    }
     if (T.lazy) {
-      if (forward) { run_cols<true>(E, b, true, st); run_rows<true>(E, b, true, st); }
-      else { run_rows<true>(E, b, false, st); run_cols<true>(E, b, false, st); }
+      if (forward) { run_cols<true>(E, first, true, st); run_rows<true>(E, b, true, st, epi); }
+      else { run_rows<true>(E, first, false, st, no_epi); run_cols<true>(E, b, false, st); }
     } else {
-      if (forward) { run_cols<false>(E, b, true, st); run_rows<false>(E, b, true, st); }
-      else { run_rows<false>(E, b, false, st); run_cols<false>(E, b, false, st); }
+      if (forward) { run_cols<false>(E, first, true, st); run_rows<false>(E, b, true, st, epi); }
+      else { run_rows<false>(E, first, false, st, no_epi); run_cols<false>(E, b, false, st); }
     }
   }
   AOA_CHECK_LAUNCH();
@@ -718,7 +798,16 @@ void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
   T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
-  ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st);
+  ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, nullptr);
+}
+
+// Limb transforms with a fused source and / or epilogue (NttIo).
+void ntt_batch_io(const Engine& E, uint64_t* data, int npolys, int first_prime, int nlimbs, long poly_stride,
+                  bool forward, const NttIo& io, cudaStream_t st) {
+  NttTables T;
+  T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
+  T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
+  ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, &io);
 }
 
 }  // namespace aoa

@@ -204,18 +204,20 @@ void tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D,
 }
 
 void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
-                            const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st) {
+                            const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st, int nb) {
   const long half = (long)E.nprimes * E.N;
-  keyswitch_mul_batch<<<ew_grid(E, nq + E.kl, n), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
+  if (nb < 0) nb = E.kl;
+  keyswitch_mul_batch<<<ew_grid(E, nq + nb, n), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
                                                                n, nq, E.k, E.d_pc, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
 }
 
 void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
-                      uint64_t* k1, int nq, cudaStream_t st) {
+                      uint64_t* k1, int nq, cudaStream_t st, int nb) {
   const long half = (long)E.nprimes * E.N;
-  keyswitch_mul<<<ew_grid(E, nq + E.kl, 1), 256, 0, st>>>(xq, xb, key, half, k0, k1, nq, E.k, E.d_pc, E.log_n); note_launch();
+  if (nb < 0) nb = E.kl;
+  keyswitch_mul<<<ew_grid(E, nq + nb, 1), 256, 0, st>>>(xq, xb, key, half, k0, k1, nq, E.k, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 

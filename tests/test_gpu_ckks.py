@@ -315,3 +315,51 @@ def test_hmult_batch_full_size_equals_pipeline():
         g = outs[z].download(nlimbs=29, domain=aoa.AOA_NTT)
         w = o1.download(nlimbs=29, domain=aoa.AOA_NTT)
         assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
+
+
+@pytest.mark.parametrize("log_n", [10, 12])
+@pytest.mark.parametrize("fuse", [1, 2, 4, 7])
+def test_fused_transform_ends_equal_separate_kernels(ref_table, log_n, fuse):
+    """Key products, key-switch combine and out-of-place inverses fused into the
+    transforms give the same residues as the separate kernels and the oracle."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(log_n, Q, B)
+    keys = make_keys(o, seed=5, rotations=(3,))
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rtk = aoa.SwitchKey(ctx, *keys["rtk"][3])
+    rng = np.random.default_rng(2)
+    N, k = E.N, E.k
+    a, b = _rand_ct(rng, Q, N, k), _rand_ct(rng, Q, N, k)
+
+    def run():
+        ca = aoa.Ciphertext.from_residues(ctx, *a, slots=N // 2, scale=1 << 35)
+        cb = aoa.Ciphertext.from_residues(ctx, *b, slots=N // 2, scale=1 << 35)
+        res = []
+        for rescale in (True, False):
+            ca.set(k - 1, N // 2, 1 << 35, ca.domain)
+            cb.set(k - 1, N // 2, 1 << 35, cb.domain)
+            o1 = aoa.Ciphertext(ctx)
+            (aoa.ckks_mul if rescale else aoa.ckks_mul_without_rescale)(ctx, o1, ca, cb, evk)
+            res.append(o1.download(nlimbs=o1.level + 1, domain=aoa.AOA_COEF))
+        outs = [aoa.Ciphertext(ctx), aoa.Ciphertext(ctx)]
+        ca.set(k - 1, N // 2, 1 << 35, ca.domain)
+        cb.set(k - 1, N // 2, 1 << 35, cb.domain)
+        aoa.ckks_mul_batch(ctx, outs, [ca, cb], [cb, ca], evk)
+        res += [x.download(nlimbs=x.level + 1, domain=aoa.AOA_COEF) for x in outs]
+        ca.set(k - 1, N // 2, 1 << 35, ca.domain)
+        r = aoa.Ciphertext(ctx)
+        aoa.ckks_rotate_left(ctx, r, ca, 3, rtk)
+        res.append(r.download(nlimbs=k, domain=aoa.AOA_COEF))
+        return res
+
+    E.tune("fuse", fuse)
+    fused = run()
+    E.tune("fuse", 0)
+    separate = run()
+    for f, s in zip(fused, separate):
+        assert np.array_equal(f[0], s[0]) and np.array_equal(f[1], s[1])
+    w0, w1, _ = o.hmult(a, b, keys["evk"], k - 1, 1 << 35, 1 << 35, rescale=True, a_state=ST_COEF, b_state=ST_COEF)
+    assert np.array_equal(fused[0][0], w0[:k - 1]) and np.array_equal(fused[0][1], w1[:k - 1])
+    r0, r1 = o.rotate_left(a, 3, keys["rtk"][3], k - 1, state=ST_COEF)
+    assert np.array_equal(fused[4][0], r0) and np.array_equal(fused[4][1], r1)
