@@ -331,6 +331,13 @@ ntt_cols(NttBatch b) {
   using D = Sub<LOG_R>;
   constexpr int W = ColTile<LOG_R, DIV>::W;
   constexpr int TILE = D::S * W;
+  // Row r of the tile sits at shared row sigma(r) = r ^ ((r >> (LO + G - 1)) & M):
+  // the low-digit accesses (rows (t G + g) 2^LO + l, threads t of one warp)
+  // then spread over the 128-byte bank line instead of hitting one W-word
+  // slice of it, while the high-digit accesses stay contiguous.
+  constexpr int LINE_ROWS = W >= 16 ? 1 : 16 / W;
+  constexpr int M = (LINE_ROWS < D::T ? LINE_ROWS : D::T) - 1;
+  auto sig = [](int r) { return r ^ ((r >> (D::LO + D::G - 1)) & M); };
   extern __shared__ __align__(128) uint64_t dyn[];
   __shared__ __align__(8) uint64_t mbar[2];
   const uint32_t sbuf = smem_u32(dyn);                          // [2][S][W] words
@@ -360,7 +367,7 @@ ntt_cols(NttBatch b) {
       __syncwarp();
       const uint64_t* src = src_of(j);
       for (int r = threadIdx.x; r < D::S; r += 32)
-        bulk_g2s(sbuf + (bi * TILE + r * W) * 8, src + r * C, W * 8, &mbar[bi]);
+        bulk_g2s(sbuf + (bi * TILE + sig(r) * W) * 8, src + r * C, W * 8, &mbar[bi]);
     }
   };
   int cur_limb = -1;
@@ -388,17 +395,17 @@ ntt_cols(NttBatch b) {
     if (FWD) {
       uint64_t v[D::E];
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + ((h << D::LO) + t) * W * 8);
+      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + sig((h << D::LO) + t) * W * 8);
       fwd_high_s<LOG_R, LAZY>(v, stw, q);
 #pragma unroll
-      for (int h = 0; h < D::E; h++) sts64(sm + ((h << D::LO) + t) * W * 8, v[h]);
+      for (int h = 0; h < D::E; h++) sts64(sm + sig((h << D::LO) + t) * W * 8, v[h]);
       __syncthreads();
 #pragma unroll
       for (int g = 0; g < D::G; g++) {
         const int hi = t * D::G + g;
         uint64_t u[D::L];
 #pragma unroll
-        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + ((hi << D::LO) + l) * W * 8);
+        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + sig((hi << D::LO) + l) * W * 8);
         fwd_low_s<LOG_R, LAZY>(u, stw, hi, q);
 #pragma unroll
         for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
@@ -410,15 +417,15 @@ ntt_cols(NttBatch b) {
         const int hi = t * D::G + g;
         uint64_t u[D::L];
 #pragma unroll
-        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + ((hi << D::LO) + l) * W * 8);
+        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + sig((hi << D::LO) + l) * W * 8);
         inv_low_s<LOG_R, LAZY>(u, stw, hi, q);
 #pragma unroll
-        for (int l = 0; l < D::L; l++) sts64(sm + ((hi << D::LO) + l) * W * 8, u[l]);
+        for (int l = 0; l < D::L; l++) sts64(sm + sig((hi << D::LO) + l) * W * 8, u[l]);
       }
       __syncthreads();
       uint64_t v[D::E];
 #pragma unroll
-      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + ((h << D::LO) + t) * W * 8);
+      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + sig((h << D::LO) + t) * W * 8);
       inv_high_s<LOG_R, LAZY>(v, stw, q, ninv, ninv_w1);
 #pragma unroll
       for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];

@@ -137,7 +137,8 @@ def run_reference(args, world, rank):
 
 def profile_case(args, aoa, ctx, rr, ps):
     """Small fixed cases for ncu: `ntt` = forward + inverse over args.polys
-    polys of 30 limbs (args.polys * 15 MiB); `hmult` = 2 HMult+relin+rescale."""
+    polys of 30 limbs (args.polys * 15 MiB); `hmult` = 2 HMult+relin+rescale;
+    `batch` = 2 batched calls of args.batch HMult+relin+rescale."""
     N = 1 << LOG_N
     if args.profile_case == "ntt":
         buf = ctx.alloc((args.polys, K, N))
@@ -150,6 +151,18 @@ def profile_case(args, aoa, ctx, rr, ps):
             ctx.ntt_inv(buf, args.polys, 0, K)
         ctx.sync()
         assert np.array_equal(buf.numpy()[0], xs), "inverse(forward(x)) != x"
+    elif args.profile_case == "batch":
+        evk = aoa.SwitchKey(ctx, rr(ps), rr(ps))
+        A = [aoa.Ciphertext.from_residues(ctx, rr(ps[:K]), rr(ps[:K]), slots=N // 2, scale=1 << SCALE_BITS,
+                                          domain=aoa.AOA_NTT) for _ in range(args.batch)]
+        Bs = [aoa.Ciphertext.from_residues(ctx, rr(ps[:K]), rr(ps[:K]), slots=N // 2, scale=1 << SCALE_BITS,
+                                           domain=aoa.AOA_NTT) for _ in range(args.batch)]
+        outs = [aoa.Ciphertext(ctx) for _ in range(args.batch)]
+        for _ in range(2):
+            for x in A + Bs:
+                x.set(K - 1, N // 2, 1 << SCALE_BITS, aoa.AOA_NTT)
+            aoa.ckks_mul_batch(ctx, outs, A, Bs, evk)
+        ctx.sync()
     else:
         evk = aoa.SwitchKey(ctx, rr(ps), rr(ps))
         a = aoa.Ciphertext.from_residues(ctx, rr(ps[:K]), rr(ps[:K]), slots=N // 2, scale=1 << SCALE_BITS)
@@ -161,6 +174,45 @@ def profile_case(args, aoa, ctx, rr, ps):
             aoa.ckks_mul(ctx, o, a, b, evk)
         ctx.sync()
     print("profile case done")
+
+
+def accuracy(aoa, log_n, q_bits, k, kl, scale_bits, seed):
+    """encode -> encrypt -> HMult + relinearise + rescale -> decrypt -> decode,
+    every stage on the GPU through the package API, keys generated on the GPU
+    from sampled draws (ternary secret of Hamming weight 64, Gaussian errors of
+    sigma 3.2, ternary u); slots = N/2 uniform in the unit disk.  Returns the
+    max and mean absolute error of the decoded product against the FP64
+    cleartext product."""
+    from aoa_b200 import params
+    primes = params.ntt_primes(q_bits, 2 << log_n, k + kl)
+    E = aoa.Engine(log_n, primes[:k], primes[k:], scale_bits=scale_bits)
+    ctx = aoa.Context(E)
+    rng = np.random.default_rng(seed)
+    N = 1 << log_n
+    s_int = np.zeros(N, np.int64)
+    idx = rng.choice(N, 64, replace=False)
+    s_int[idx] = rng.choice([-1, 1], 64)
+    s = ctx.upload(np.array([(s_int % q).astype(np.uint64) for q in primes]))
+    gauss = lambda: np.rint(rng.normal(0.0, 3.2, N)).astype(np.int64)
+    unif = lambda: np.array([rng.integers(0, q, N, dtype=np.uint64) for q in primes])
+    draws = {"pk": (ctx.upload(unif()), ctx.upload(gauss())), "evk": (ctx.upload(unif()), ctx.upload(gauss()))}
+    keys = aoa.ckks_keygen(ctx, s, draws)
+    slots = N // 2
+    vals = []
+    for _ in range(2):
+        r, t = np.sqrt(rng.uniform(0, 1, slots)), rng.uniform(0, 2 * np.pi, slots)
+        vals.append(r * np.exp(1j * t))
+    scale = 1 << scale_bits
+    cts = [aoa.ckks_encrypt(ctx, v, keys["pk"], rng.integers(-1, 2, N).astype(np.int64), gauss(), gauss(),
+                            scale=scale) for v in vals]
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_mul(ctx, out, cts[0], cts[1], keys["evk"])
+    sk = ctx.upload(np.array([(s_int % q).astype(np.uint64) for q in primes[:k]]))
+    dec = aoa.ckks_decrypt(ctx, out, sk)
+    err = np.abs(dec - vals[0] * vals[1])
+    return {"log_n": log_n, "q_limbs": k, "q_bits": q_bits, "special_limbs": kl, "scale_bits": scale_bits,
+            "slots": slots, "max_abs_err": float(err.max()), "mean_abs_err": float(err.mean()),
+            "max_abs_err_log2": float(np.log2(err.max())), "within_2^-20": bool(err.max() <= 2.0 ** -20)}
 
 
 def systems_workloads(aoa, torch):
@@ -231,7 +283,7 @@ def main():
     ap.add_argument("--impl", default="aoa", choices=["aoa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-systems", action="store_true", help="skip the uneven-batch and serving measurements")
-    ap.add_argument("--profile-case", choices=["ntt", "hmult"],
+    ap.add_argument("--profile-case", choices=["ntt", "hmult", "batch"],
                     help="run a small fixed case for ncu captures (no timing, no JSON)")
     ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default transform launch shapes")
@@ -529,6 +581,11 @@ def main():
                "sample": "%d HMult+relin+rescale on the same N=2^16, k=30, kl=31 workload "
                          "(reference op sequence, oracle/ckks_oracle.cpp, OpenMP)" % n_cpu}
 
+    acc = None
+    if rank == 0:
+        acc = {"plain_ckks_n4096": accuracy(aoa, 12, 52, 3, 4, 40, seed=7),
+               "hmult_n65536": accuracy(aoa, LOG_N, 60, K, KL, SCALE_BITS, seed=8),
+               "reference": "decoded HMult+relin+rescale product vs the FP64 cleartext product (numpy)"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -540,6 +597,7 @@ def main():
                        "parallelism": "replicas",
                        "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % B,
                        "transform_tuning": tuning},
+            "accuracy": acc,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "single_op_ops_per_s": float(1000.0 / np.mean(lat))},
             "plain_per_call": {"ops_per_s": world * B / (plain_ms / 1000.0),
