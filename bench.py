@@ -95,10 +95,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from aoa_b200.replicas import ranks
+    return ranks()
 
 
 def run_reference(args, world, rank):
@@ -289,19 +287,15 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default transform launch shapes")
     ap.add_argument("--knobs", default="", help="engine knobs name=value,... applied instead of the autotuner")
     args = ap.parse_args()
-    world, rank, local = dist_setup()
+    world, rank, local = dist_setup()     # the launcher's WORLD_SIZE / RANK / LOCAL_RANK
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
 
     import torch
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-        pg = dist
+    from aoa_b200 import replicas
+    pg = replicas.init("nccl", timeout_s=120, device=torch.device("cuda", local))
     import aoa_b200 as aoa
 
     ps = primes()
@@ -318,7 +312,7 @@ def main():
     stream = torch.cuda.ExternalStream(ctx.stream)
     N = 1 << LOG_N
     B = args.batch
-    rng = np.random.default_rng(1000 + rank)
+    rng = np.random.default_rng(replicas.replica_seed(1000, rank))
     rr = lambda qs: np.array([rng.integers(0, q, N, dtype=np.uint64) for q in qs], dtype=np.uint64)
     if args.profile_case:
         profile_case(args, aoa, ctx, rr, ps)
@@ -345,15 +339,10 @@ def main():
     def barrier():
         torch.cuda.synchronize()
         ctx.sync()
-        if pg:
-            pg.barrier()
+        replicas.barrier(pg)
 
     def maxt(ms):
-        if not pg:
-            return ms
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(ms, pg, device="cuda")
 
     # ---- device-resident throughput -------------------------------------------
     for _ in range(max(3, args.warmup)):
@@ -374,7 +363,7 @@ def main():
     clk = clocks.stop()
     ms = maxt(e0.elapsed_time(e1))
     ms_step = ms / args.steps
-    value = world * B * args.steps / (ms / 1000.0)
+    value = replicas.job_rate(B * args.steps, world, ms)
 
     def timed(fn, steps):
         fn()
@@ -555,7 +544,7 @@ def main():
     q1.record(stream)
     barrier()
     e2e_ms = maxt(q0.elapsed_time(q1))
-    e2e_value = world * B * e2e_steps / (e2e_ms / 1000.0)
+    e2e_value = replicas.job_rate(B * e2e_steps, world, e2e_ms)
     h2d = B * 2 * 2 * K * N * 8
     d2h = B * 2 * (K - 1) * N * 8
 
@@ -630,9 +619,7 @@ def main():
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    replicas.finish(pg)
 
 
 if __name__ == "__main__":
