@@ -318,7 +318,9 @@ struct RowTile {
   static constexpr int R0 = Sub<LOG_S>::PER_CTA >> DIV;
   static constexpr int ROWS = R0 < 1 ? 1 : R0;
   static constexpr int THREADS = Sub<LOG_S>::T * ROWS;
-  static constexpr int MIN_BLOCKS = 512 / THREADS < 1 ? 1 : (512 / THREADS > 32 ? 32 : 512 / THREADS);
+  // 384 threads per SM: up to 170 registers, so the low-digit twiddles held in
+  // registers do not spill (measured 1% faster than 512 threads with spills)
+  static constexpr int MIN_BLOCKS = 384 / THREADS < 1 ? 1 : (384 / THREADS > 32 ? 32 : 384 / THREADS);
   static constexpr size_t SMEM =
       2 * (size_t)ROWS * Sub<LOG_S>::S * 8 + (size_t)ROWS * (Sub<LOG_S>::E - 1) * sizeof(ShoupW);
 };
