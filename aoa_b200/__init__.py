@@ -529,6 +529,64 @@ def ckks_batch_inner_prod(ctx, out, ct, other, rtks):
     ckks_sumslots(ctx, out, out, {k: v for k, v in rtks.items() if isinstance(k, int)})
 
 
+# ---- compositions (aoa-ntt src/ckks/ckks.cpp:423-455, 732-906) ---------------------
+
+# Maclaurin coefficients of the reference's function approximations
+# (CKKSContext, aoa-ntt include/newckks/ckks/ckkscontext.h:101-120), with the
+# number of terms each of its functions evaluates (ckks.cpp:813-906).  The
+# values are the reference's, quirks included (its cosine table), so that the
+# results match it.
+MACLAURIN = {
+    "exp": ([1.0, 1.0, 1.0 / 2, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720, 1.0 / 5040, 1.0 / 40320, 1.0 / 362880,
+             1.0 / 3628800], 11),
+    "sin": ([0.0, 1.0, 0.0, -1.0 / 6, 0.0, 1.0 / 120, 0.0, -1.0 / 5040, 0.0, 1.0 / 362880, 0.0, -1.0 / 39916800], 12),
+    "cos": ([1.0, 0.0, -0.5, 1.0 / 24, 0.0, -1.0 / 720, 0.0, 1.0 / 40320, 0.0, -1.0 / 362880, 0.0, 1.0 / 362880], 12),
+    "sigmoid": ([1.0 / 2, 1.0 / 4, 0.0, -1.0 / 48, 0.0, 1.0 / 480, 0.0, -17.0 / 80640, 0.0, 31.0 / 1451520], 8),
+}
+
+
+def ckks_power(ctx, out, ct, x, evk):
+    """ct^x by square-and-multiply (ckks_power)."""
+    capi.check(capi.load().aoa_power(ctx.handle, out.handle, ct.handle, int(x), evk.handle if evk else None))
+
+
+def ckks_eval_polynomial(ctx, out, ct, coeffs, evk):
+    """sum_i coeffs[i] ct^i by Horner's rule (ckks_eval_polynomial)."""
+    c = np.ascontiguousarray(coeffs, dtype=np.float64)
+    capi.check(capi.load().aoa_eval_polynomial(ctx.handle, out.handle, ct.handle,
+                                               c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), c.size,
+                                               evk.handle))
+
+
+def _maclaurin(name):
+    def f(ctx, out, ct, evk):
+        coeffs, n = MACLAURIN[name]
+        ckks_eval_polynomial(ctx, out, ct, coeffs[:n], evk)
+    f.__name__ = "ckks_" + name
+    f.__doc__ = "ckks_%s: the reference's %d-term Maclaurin polynomial." % (name, MACLAURIN[name][1])
+    return f
+
+
+ckks_exp = _maclaurin("exp")
+ckks_sin = _maclaurin("sin")
+ckks_cos = _maclaurin("cos")
+ckks_sigmoid = _maclaurin("sigmoid")
+
+
+def ckks_inner_prod(ctx, out, a, b, evk=None):
+    """sum_i a[i] * b[i] with one rescale (ckks_inner_prod); b is a list of
+    ciphertexts (needs evk) or of real weights."""
+    n = len(a)
+    pa = (ctypes.c_void_p * n)(*[x.handle.value for x in a])
+    if b and isinstance(b[0], Ciphertext):
+        pb = (ctypes.c_void_p * n)(*[x.handle.value for x in b])
+        capi.check(capi.load().aoa_inner_prod(ctx.handle, out.handle, pa, pb, n, evk.handle))
+    else:
+        w = np.ascontiguousarray(b, dtype=np.float64)
+        capi.check(capi.load().aoa_inner_prod_const(ctx.handle, out.handle, pa,
+                                                    w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+
+
 # ---- CUDA graphs ------------------------------------------------------------------
 
 class Graph:

@@ -103,6 +103,10 @@ SIGNATURES = {
     "aoa_mul_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int]),
     "aoa_add_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double]),
     "aoa_sumslots": (c_int, [c_void_p, c_void_p, c_void_p, vpp, c_int]),
+    "aoa_power": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, c_void_p]),
+    "aoa_eval_polynomial": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_double), c_int, c_void_p]),
+    "aoa_inner_prod": (c_int, [c_void_p, c_void_p, vpp, vpp, c_int, c_void_p]),
+    "aoa_inner_prod_const": (c_int, [c_void_p, c_void_p, vpp, ctypes.POINTER(c_double), c_int]),
     "aoa_ctx_capture_begin": (c_int, [c_void_p]),
     "aoa_ctx_capture_end": (c_int, [c_void_p, c_void_p]),
     "aoa_graph_launch": (c_int, [c_void_p, c_void_p]),

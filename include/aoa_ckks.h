@@ -285,6 +285,16 @@ int aoa_add_const(aoa_ctx* c, aoa_ct* out, aoa_ct* in, double val);
 /* ckks_sumslots (ckks.cpp:484-500): rotate-and-add over slots/2 .. 1;
  * rtks[j] is the left-rotation key for 2^j.                                */
 int aoa_sumslots(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* const* rtks, int nkeys);
+/* Compositions with the reference's operation sequences and metadata rules:
+ * ckks_power (ckks.cpp:732-761; x = 0 gives the noiseless encryption of 1),
+ * ckks_eval_polynomial (ckks.cpp:778-796, Horner from a cleared
+ * accumulator), ckks_inner_prod of ciphertext pairs (ckks.cpp:423-441) and
+ * with real weights (ckks.cpp:443-455).  out must differ from the input of
+ * aoa_power / aoa_eval_polynomial.                                          */
+int aoa_power(aoa_ctx* c, aoa_ct* out, aoa_ct* in, uint64_t x, const aoa_swk* evk);
+int aoa_eval_polynomial(aoa_ctx* c, aoa_ct* out, aoa_ct* x, const double* coeffs, int n, const aoa_swk* evk);
+int aoa_inner_prod(aoa_ctx* c, aoa_ct* out, aoa_ct* const* a, aoa_ct* const* b, int size, const aoa_swk* evk);
+int aoa_inner_prod_const(aoa_ctx* c, aoa_ct* out, aoa_ct* const* a, const double* w, int size);
 
 /* --- encoder and encryption (src/ckks/encoder.cu:12-298, ckks.cpp:87-192,
  *     CKKSContext::encode/decode ckkscontext.cpp:5-38).  Complex values are
