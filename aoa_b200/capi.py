@@ -104,6 +104,12 @@ SIGNATURES = {
     "aoa_add_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double]),
     "aoa_sumslots": (c_int, [c_void_p, c_void_p, c_void_p, vpp, c_int]),
     "aoa_power": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, c_void_p]),
+    "aoa_ct_wire_size": (c_size_t, [c_void_p, c_void_p]),
+    "aoa_ct_serialize": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, ctypes.POINTER(c_size_t)]),
+    "aoa_ct_deserialize": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
+    "aoa_swk_wire_size": (c_size_t, [c_void_p]),
+    "aoa_swk_serialize": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, ctypes.POINTER(c_size_t)]),
+    "aoa_swk_deserialize": (c_int, [c_void_p, c_void_p, c_size_t, vpp]),
     "aoa_eval_polynomial": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_double), c_int, c_void_p]),
     "aoa_inner_prod": (c_int, [c_void_p, c_void_p, vpp, vpp, c_int, c_void_p]),
     "aoa_inner_prod_const": (c_int, [c_void_p, c_void_p, vpp, ctypes.POINTER(c_double), c_int]),

@@ -186,12 +186,14 @@ __device__ __forceinline__ void tc_commit(uint64_t* mb) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -200,7 +202,7 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 // mod P.  Groups of four diagonals W_m = sum_t S_(4m+t) 2^(8t) < 2^51 are
 // formed with 32 x 32 -> 64-bit multiply-adds, then added at 32-bit offsets
 // 32m into the 128-bit total (below 2^126, so W_3 < 2^30 fits word 3).
-__device__ __forceinline__ uint64_t tc_combine(const uint32_t (&v)[16], const PrimeConst& P) {
+__device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const PrimeConst& P) {
   uint64_t W[4];
 #pragma unroll
   for (int m = 0; m < 4; m++) {
@@ -229,6 +231,7 @@ __device__ __forceinline__ uint64_t tc_combine(const uint32_t (&v)[16], const Pr
 // (tile rows) and every fourth output starting at w / 4.
 constexpr int kTcPairs = 32 / 2 / (kTcThreads / kTcRows);   // input pairs per thread (nin <= 32)
 
+template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
 basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   extern __shared__ __align__(1024) uint8_t tcs[];
@@ -280,7 +283,6 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   bool in_flight = false;                                  // an MMA group not yet waited for
   const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
   const int ksteps = (a.nin + 3) / 4;                      // 4 inputs (32 bytes) per MMA K step
-  const int nout = j_end - j_first;
   uint32_t phase = 0;
   for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
     const long poly = tile / tiles_per_poly;
@@ -318,29 +320,57 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     in_flight = false;
     phase ^= 1;
     tc_fence_after();
+    // warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (tile rows) and a
+    // contiguous run of outputs: quarter w / 4 of them, two per load
     const int g = warp % 4, par = warp / 4;
     const long c = c0 + g * 32 + lane;
     const uint32_t t_lane = tmem + ((uint32_t)(g * 32) << 16);
     uint64_t* out = a.out + poly * a.out_poly_stride + c;
     uint64_t dv = 0;
-    if (a.mode >= kRescaleTop) dv = a.d[poly * a.d_poly_stride + c];
-    uint32_t v[16];
-    if (a.mode == kRescaleFused) {
-      const int l = j_end - 1;
-      tc_ld16(t_lane + l * 16, v);
+    if (MODE >= kRescaleTop) dv = a.d[poly * a.d_poly_stride + c];
+    uint32_t v[32];
+    if (MODE == kRescaleFused) {
+      const int l = j_end - 1;                 // outputs 0..l-1 from c_l (j_first = 0)
+      tc_ld32(t_lane + (l & ~1) * 16, v);
       const PrimeConst& Pl = a.pc[a.out_prime0 + l];
-      const uint64_t cl = sub_mod(dv, shoup(tc_combine(v, Pl), a.binv[l], Pl.q), Pl.q);
-      for (int j = par; j < l; j += kTcThreads / 128) {
-        tc_ld16(t_lane + j * 16, v);
-        const PrimeConst& P = a.pc[a.out_prime0 + j];
-        out[(long)(j - a.out_shift) * N] =
-            add_mod(shoup(tc_combine(v, P), a.binv[j], P.q), shoup(cl, 1, P.one_sh, P.q), P.q);
+      const uint64_t sl = (l & 1) ? tc_combine(v + 16, Pl) : tc_combine(v, Pl);
+      const uint64_t cl = sub_mod(dv, shoup(sl, a.binv[l], Pl.q), Pl.q);
+      const int per = (((l + 3) / 4) + 1) & ~1;
+      const int jb = par * per, je = min(l, jb + per);
+      for (int j = jb; j < je; j += 2) {
+        tc_ld32(t_lane + j * 16, v);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          if (j + u < je) {
+            const PrimeConst& P = a.pc[a.out_prime0 + j + u];
+            out[(long)(j + u - a.out_shift) * N] =
+                add_mod(shoup(tc_combine(v + 16 * u, P), a.binv[j + u], P.q), shoup(cl, 1, P.one_sh, P.q), P.q);
+          }
+        }
       }
     } else {
-      for (int j = par; j < nout; j += kTcThreads / 128) {
-        const int jj = j_first + j;
-        tc_ld16(t_lane + jj * 16, v);
-        conv_store(a, jj, tc_combine(v, a.pc[a.out_prime0 + jj]), dv, out, c, N, poly);
+      const int nout = j_end - j_first;
+      const int per = (((nout + 3) / 4) + 1) & ~1;
+      const int jb = j_first + par * per, je = min(j_end, jb + per);
+      for (int jj = jb & ~1; jj < je; jj += 2) {
+        tc_ld32(t_lane + jj * 16, v);
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int o = jj + u;
+          if (o >= jb && o < je) {
+            const PrimeConst& P = a.pc[a.out_prime0 + o];
+            uint64_t r = tc_combine(v + 16 * u, P);
+            if (MODE == kModDown) {
+              const uint64_t x = a.x[poly * a.x_poly_stride + (long)(o - a.x_shift) * N + c];
+              r = shoup(sub_mod(x, r, P.q), a.binv[o], P.q);
+            } else if (MODE == kRescaleTop) {
+              r = sub_mod(dv, shoup(r, a.binv[o], P.q), P.q);
+            } else if (MODE == kRescaleY) {
+              r = add_mod(shoup(r, a.binv[o], P.q), shoup(dv, 1, P.one_sh, P.q), P.q);
+            }
+            out[(long)(o - a.out_shift) * N] = r;
+          }
+        }
       }
     }
     tc_fence_before();
@@ -368,7 +398,14 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
     t.err = E.d_err;
     t.npolys = npolys;
     const long tiles = (N / kTcRows) * npolys;
-    basis_convert_tc<<<(unsigned)std::min<long>(tiles, E.num_sms), kTcThreads, kTcSmem, st>>>(t, j_begin, j_end);
+    const unsigned grid_tc = (unsigned)std::min<long>(tiles, E.num_sms);
+    switch (a.mode) {
+      case kRaw: basis_convert_tc<kRaw><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
+      case kModDown: basis_convert_tc<kModDown><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
+      case kRescaleTop: basis_convert_tc<kRescaleTop><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
+      case kRescaleY: basis_convert_tc<kRescaleY><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
+      default: basis_convert_tc<kRescaleFused><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
+    }
     note_launch();
     AOA_CHECK_LAUNCH();
     return;
@@ -384,7 +421,14 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
 // conversion kernel needs, and check the 128-bit accumulation bound.
 void rns_init(Engine& E) {
   AOA_CUDA(cudaFuncSetAttribute(basis_convert, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRaw>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kModDown>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRescaleTop>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kTcSmem));
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRescaleY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kTcSmem));
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRescaleFused>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kTcSmem));
   auto bits = [](uint64_t x) { int b = 0; while (x) { b++; x >>= 1; } return b; };
   uint64_t mq = 0, mb = 0;
   for (int i = 0; i < E.k; i++) mq = std::max(mq, E.primes[i]);

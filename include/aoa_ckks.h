@@ -296,6 +296,20 @@ int aoa_eval_polynomial(aoa_ctx* c, aoa_ct* out, aoa_ct* x, const double* coeffs
 int aoa_inner_prod(aoa_ctx* c, aoa_ct* out, aoa_ct* const* a, aoa_ct* const* b, int size, const aoa_swk* evk);
 int aoa_inner_prod_const(aoa_ctx* c, aoa_ct* out, aoa_ct* const* a, const double* w, int size);
 
+/* --- binary wire format (serving payloads; the reference's JSON export,
+ *     cipher_export / cipher_import cipher_t.cpp:42-81 and export_keys /
+ *     load_keys ckkscontext.cpp:50-100, is in the Python package).  A 64-byte
+ *     header (magic "AOACKKS1", kind, ring, primes fingerprint, level, slots,
+ *     scale, domain) and the residues as u64: a ciphertext's live limbs in its
+ *     current domain, a key's two (k+kl)-limb polys.  Readers reject buffers
+ *     of another kind, ring, prime set or length (AOA_ERR_BAD_PARAM).        */
+size_t aoa_ct_wire_size(const aoa_ctx* c, const aoa_ct* ct);
+int aoa_ct_serialize(aoa_ctx* c, const aoa_ct* ct, uint8_t* buf, size_t cap, size_t* len);
+int aoa_ct_deserialize(aoa_ctx* c, aoa_ct* ct, const uint8_t* buf, size_t len);
+size_t aoa_swk_wire_size(const aoa_ctx* c);
+int aoa_swk_serialize(aoa_ctx* c, const aoa_swk* k, uint8_t* buf, size_t cap, size_t* len);
+int aoa_swk_deserialize(aoa_ctx* c, const uint8_t* buf, size_t len, aoa_swk** out);
+
 /* --- encoder and encryption (src/ckks/encoder.cu:12-298, ckks.cpp:87-192,
  *     CKKSContext::encode/decode ckkscontext.cpp:5-38).  Complex values are
  *     (re, im) double pairs (the layout of std::complex<double>).             */
