@@ -529,6 +529,69 @@ def ckks_batch_inner_prod(ctx, out, ct, other, rtks):
     ckks_sumslots(ctx, out, out, {k: v for k, v in rtks.items() if isinstance(k, int)})
 
 
+# ---- device samplers (Philox4x32-10; Sampler, aoa-ntt src/cuda/sampler.cu) ----------
+
+def sample_uniform(ctx, first_prime, nlimbs, seed, stream=0):
+    """[nlimbs][N] uniform residues under primes first_prime.. on the device."""
+    out = ctx.alloc((nlimbs, ctx.engine.N))
+    capi.check(capi.load().aoa_sample_uniform(ctx.handle, out.ptr, first_prime, nlimbs, seed, stream))
+    return out
+
+
+def sample_gaussian(ctx, n, seed, stream=0, sigma=3.2):
+    """n rounded Gaussian integers (int64) on the device (sample_DG)."""
+    out = ctx.alloc((n,), np.int64)
+    capi.check(capi.load().aoa_sample_gaussian(ctx.handle, out.ptr, n, float(sigma), seed, stream))
+    return out
+
+
+def sample_ternary(ctx, n, hw, seed, stream=0):
+    """n int64 in {-1, 0, 1} with exactly hw non-zeros (sample_hw / sample_Z0)."""
+    out = ctx.alloc((n,), np.int64)
+    capi.check(capi.load().aoa_sample_ternary(ctx.handle, out.ptr, n, hw, seed, stream))
+    return out
+
+
+def ckks_keygen_sampled(ctx, seed, rotations=(), conjugation=False, hw=64):
+    """Secret (ternary, Hamming weight hw) and all keys from the device
+    samplers (streams 0..: secret, pk a / e, evk a / e, then per rotation key
+    and the conjugation key).  Returns (secret as [k+kl][N] residues on the
+    device, keys)."""
+    E = ctx.engine
+    nqb = len(E.primes)
+    s_int = sample_ternary(ctx, E.N, hw, seed, 0)
+    s = ctx.alloc((nqb, E.N))
+    capi.check(capi.load().aoa_signed_to_residues(ctx.handle, s_int.ptr, s.ptr, 0, nqb))
+    stream = [1]
+
+    def draw():
+        a = sample_uniform(ctx, 0, nqb, seed, stream[0])
+        e = sample_gaussian(ctx, E.N, seed, stream[0] + 1)
+        stream[0] += 2
+        return a, e
+    draws = {"pk": draw(), "evk": draw()}
+    for r in rotations:
+        draws[("rtk", r)] = draw()
+    if conjugation:
+        draws["cjk"] = draw()
+    return s, ckks_keygen(ctx, s, draws, rotations, conjugation)
+
+
+def ckks_encrypt_sampled(ctx, values, pk, seed, stream=0, empty_slots=0, scale=None, out=None):
+    """ckks_encrypt with its draws from the device samplers: u ternary with N/2
+    non-zeros (sample_Z0), e1 and e2 rounded Gaussian (streams stream ..
+    stream + 2)."""
+    m, scale = ckks_encode(ctx, values, empty_slots, scale)
+    N = ctx.engine.N
+    u = sample_ternary(ctx, N, N // 2, seed, stream)
+    e1 = sample_gaussian(ctx, N, seed, stream + 1)
+    e2 = sample_gaussian(ctx, N, seed, stream + 2)
+    out = out if out is not None else Ciphertext(ctx)
+    capi.check(capi.load().aoa_encrypt(ctx.handle, out.handle, m.ptr, AOA_COEF, pk.handle, u.ptr, e1.ptr, e2.ptr,
+                                       len(values) + empty_slots, int(scale)))
+    return out
+
+
 # ---- compositions (aoa-ntt src/ckks/ckks.cpp:423-455, 732-906) ---------------------
 
 # Maclaurin coefficients of the reference's function approximations

@@ -104,6 +104,10 @@ SIGNATURES = {
     "aoa_add_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double]),
     "aoa_sumslots": (c_int, [c_void_p, c_void_p, c_void_p, vpp, c_int]),
     "aoa_power": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint64, c_void_p]),
+    "aoa_sample_uniform": (c_int, [c_void_p, c_void_p, c_int, c_int, ctypes.c_uint64, ctypes.c_uint64]),
+    "aoa_sample_gaussian": (c_int, [c_void_p, c_void_p, c_long, c_double, ctypes.c_uint64, ctypes.c_uint64]),
+    "aoa_sample_ternary": (c_int, [c_void_p, c_void_p, c_long, c_long, ctypes.c_uint64, ctypes.c_uint64]),
+    "aoa_signed_to_residues": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int]),
     "aoa_ct_wire_size": (c_size_t, [c_void_p, c_void_p]),
     "aoa_ct_serialize": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, ctypes.POINTER(c_size_t)]),
     "aoa_ct_deserialize": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),

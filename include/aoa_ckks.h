@@ -296,6 +296,18 @@ int aoa_eval_polynomial(aoa_ctx* c, aoa_ct* out, aoa_ct* x, const double* coeffs
 int aoa_inner_prod(aoa_ctx* c, aoa_ct* out, aoa_ct* const* a, aoa_ct* const* b, int size, const aoa_swk* evk);
 int aoa_inner_prod_const(aoa_ctx* c, aoa_ct* out, aoa_ct* const* a, const double* w, int size);
 
+/* --- device samplers (Sampler, src/cuda/sampler.cu:13-230) on Philox4x32-10
+ *     (Salmon et al., SC 2011): every draw is a function of (seed, stream,
+ *     index), reproducible on the host.  Uniform residues of limbs
+ *     first_prime .. +nlimbs ([nlimbs][N], 128-bit draw mod q); rounded
+ *     Gaussian (Box-Muller, sigma); ternary with exactly hw entries +-1
+ *     (sample_hw: hw = 64, sample_Z0: hw = N/2).  Asynchronous.             */
+int aoa_sample_uniform(aoa_ctx* c, uint64_t* d_out, int first_prime, int nlimbs, uint64_t seed, uint64_t stream);
+int aoa_sample_gaussian(aoa_ctx* c, int64_t* d_out, long n, double sigma, uint64_t seed, uint64_t stream);
+int aoa_sample_ternary(aoa_ctx* c, int64_t* d_out, long n, long hw, uint64_t seed, uint64_t stream);
+/* small signed integers (N of them) -> [nlimbs][N] canonical residues */
+int aoa_signed_to_residues(aoa_ctx* c, const int64_t* d_in, uint64_t* d_out, int first_prime, int nlimbs);
+
 /* --- binary wire format (serving payloads; the reference's JSON export,
  *     cipher_export / cipher_import cipher_t.cpp:42-81 and export_keys /
  *     load_keys ckkscontext.cpp:50-100, is in the Python package).  A 64-byte
