@@ -174,16 +174,16 @@ def profile_case(args, aoa, ctx, rr, ps):
     print("profile case done")
 
 
-def accuracy(aoa, log_n, q_bits, k, kl, scale_bits, seed):
+def accuracy(aoa, log_n, Q, B, scale_bits, seed):
     """encode -> encrypt -> HMult + relinearise + rescale -> decrypt -> decode,
     every stage on the GPU through the package API, keys generated on the GPU
     from sampled draws (ternary secret of Hamming weight 64, Gaussian errors of
     sigma 3.2, ternary u); slots = N/2 uniform in the unit disk.  Returns the
     max and mean absolute error of the decoded product against the FP64
     cleartext product."""
-    from aoa_b200 import params
-    primes = params.ntt_primes(q_bits, 2 << log_n, k + kl)
-    E = aoa.Engine(log_n, primes[:k], primes[k:], scale_bits=scale_bits)
+    primes = list(Q) + list(B)
+    k, kl = len(Q), len(B)
+    E = aoa.Engine(log_n, Q, B, scale_bits=scale_bits)
     ctx = aoa.Context(E)
     rng = np.random.default_rng(seed)
     N = 1 << log_n
@@ -208,9 +208,67 @@ def accuracy(aoa, log_n, q_bits, k, kl, scale_bits, seed):
     sk = ctx.upload(np.array([(s_int % q).astype(np.uint64) for q in primes[:k]]))
     dec = aoa.ckks_decrypt(ctx, out, sk)
     err = np.abs(dec - vals[0] * vals[1])
-    return {"log_n": log_n, "q_limbs": k, "q_bits": q_bits, "special_limbs": kl, "scale_bits": scale_bits,
+    return {"log_n": log_n, "q_limbs": k, "q_bits": [int(q).bit_length() for q in Q], "special_limbs": kl,
+            "b_bits": int(B[0]).bit_length(), "scale_bits": scale_bits,
             "slots": slots, "max_abs_err": float(err.max()), "mean_abs_err": float(err.mean()),
             "max_abs_err_log2": float(np.log2(err.max())), "within_2^-20": bool(err.max() <= 2.0 ** -20)}
+
+
+def reference_layout_n4096():
+    """The primes the reference's CUDAManager::init(k = 3, kl = 4, N = 2^12,
+    prec = 52) selects: its first 63-bit prime, two of its 52-bit bucket, and
+    four of its 55-bit bucket as the special primes (a copy of its tables is
+    the fixture tests/golden/reference_primes.json)."""
+    from aoa_b200 import params
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                           "reference_primes.json")) as f:
+        table = json.load(f)
+    return params.reference_prime_set(table, 3, 4, 52)
+
+
+def cpu_chain(Q, B, scale_bits):
+    """Config 1 on the host: the oracle (the reference's CPU path restated)
+    runs encode -> encrypt -> HMult + relinearise + rescale -> decrypt -> decode
+    at N = 2^12, single-threaded and on all host threads."""
+    import oracle
+    from oracle import Oracle
+    from tests.ckks_inputs import make_keys, encrypt_values, decrypt_values
+    o = Oracle(1 << 12, list(Q), list(B))
+    keys = make_keys(o, seed=2)
+    rng = np.random.default_rng(1)
+    slots = 2048
+    vals = []
+    for _ in range(2):
+        r, t = np.sqrt(rng.uniform(0, 1, slots)), rng.uniform(0, 2 * np.pi, slots)
+        vals.append(r * np.exp(1j * t))
+    scale = 1 << scale_bits
+    out = {"slots": slots, "scale_bits": scale_bits, "q_bits": [int(q).bit_length() for q in Q]}
+    for label, threads in (("single_thread", 1), ("all_threads", os.cpu_count() or 1)):
+        oracle.lib().oc_set_threads(threads)
+        t0 = time.perf_counter()
+        ca = encrypt_values(o, keys, vals[0], scale, seed=3)
+        cb = encrypt_values(o, keys, vals[1], scale, seed=4)
+        r0, r1, rsc = o.hmult(ca, cb, keys["evk"], len(Q) - 1, scale, scale, rescale=True, a_state=oracle.ST_NTT,
+                              b_state=oracle.ST_NTT)
+        pad = lambda x: np.concatenate([x[: len(Q) - 1], np.zeros((1, x.shape[1]), np.uint64)])
+        dec = decrypt_values(o, keys, (pad(r0), pad(r1)), slots, rsc, state=oracle.ST_COEF)
+        ms = (time.perf_counter() - t0) * 1000
+        err = np.abs(dec - vals[0] * vals[1])
+        out[label] = {"threads": threads, "ms": ms, "max_abs_err": float(err.max()),
+                      "mean_abs_err": float(err.mean())}
+    out["cpu_model"] = cpu_model()
+    return out
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def systems_workloads(aoa, torch):
@@ -572,9 +630,17 @@ def main():
 
     acc = None
     if rank == 0:
-        acc = {"plain_ckks_n4096": accuracy(aoa, 12, 52, 3, 4, 40, seed=7),
-               "hmult_n65536": accuracy(aoa, LOG_N, 60, K, KL, SCALE_BITS, seed=8),
+        from aoa_b200 import params
+        p52 = params.ntt_primes(52, 2 << 12, 7)
+        ref_q, ref_b = reference_layout_n4096()
+        acc = {"plain_ckks_n4096": accuracy(aoa, 12, p52[:3], p52[3:], 40, seed=7),
+               "plain_ckks_n4096_scale52": accuracy(aoa, 12, p52[:3], p52[3:], 52, seed=7),
+               "reference_layout_n4096_scale52": accuracy(aoa, 12, ref_q, ref_b, 52, seed=7),
+               "reference_layout_n4096_scale40": accuracy(aoa, 12, ref_q, ref_b, 40, seed=7),
+               "hmult_n65536": accuracy(aoa, LOG_N, ps[:K], ps[K:], SCALE_BITS, seed=8),
                "reference": "decoded HMult+relin+rescale product vs the FP64 cleartext product (numpy)"}
+        if cpu is not None:
+            acc["cpu_chain_n4096"] = cpu_chain(p52[:3], p52[3:], 40)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
