@@ -73,6 +73,7 @@ SIGNATURES = {
     "aoa_ct_data": (c_int, [c_void_p, vpp]),
     "aoa_ct_upload": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int]),
     "aoa_ct_download": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int]),
+    "aoa_ct_download_async": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int]),
     "aoa_swk_create": (c_int, [c_void_p, c_void_p, c_void_p, c_int, vpp]),
     "aoa_swk_destroy": (c_int, [c_void_p, c_void_p]),
     "aoa_hmult": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

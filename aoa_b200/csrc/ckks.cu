@@ -610,7 +610,19 @@ int aoa_ct_upload(aoa_ctx* c, aoa_ct* ct, const uint64_t* host, int nlimbs, int 
 }
 
 // download limbs 0..nlimbs-1 of both polys in `domain` (converts a copy)
+static int download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain, bool wait);
+
 int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain) {
+  return download(c, ct, host, nlimbs, domain, true);
+}
+
+// the same, queued on the context's stream without waiting: `host` (pinned for
+// an asynchronous copy) is valid after aoa_ctx_sync or a later synchronising call
+int aoa_ct_download_async(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain) {
+  return download(c, ct, host, nlimbs, domain, false);
+}
+
+static int download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain, bool wait) {
   if (!c || !ct || !host) return fail(AOA_ERR_BAD_PARAM, "null argument");
   return guarded([&] {
     Ctx& C = c->c;
@@ -637,7 +649,7 @@ int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, in
     for (int p = 0; p < 2; p++)
       AOA_CUDA(cudaMemcpyAsync(host + (size_t)p * nlimbs * E.N, src + (size_t)p * E.k * E.N, nlimbs * limb,
                                cudaMemcpyDeviceToHost, C.stream));
-    AOA_CUDA(cudaStreamSynchronize(C.stream));
+    if (wait) AOA_CUDA(cudaStreamSynchronize(C.stream));
   });
 }
 

@@ -191,6 +191,9 @@ int aoa_ct_data(aoa_ct* ct, uint64_t** device_ptr);          /* [2][k][N] */
  * poly_t.cpp:74-100) and synchronises the stream.                           */
 int aoa_ct_upload(aoa_ctx* c, aoa_ct* ct, const uint64_t* host, int nlimbs, int domain);
 int aoa_ct_download(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain);
+/* aoa_ct_download queued without waiting (host pinned; read it after
+ * aoa_ctx_sync): lets a caller overlap result copies with later work.     */
+int aoa_ct_download_async(aoa_ctx* c, const aoa_ct* ct, uint64_t* host, int nlimbs, int domain);
 
 /* --- switching keys: SwitchKey {a, b} over QB (include/newckks/defines.h:85-101,
  *     src/ckks/ckkskeys.cpp:101-191).  host_b / host_a: [k+kl][N] residues.   */
