@@ -40,6 +40,7 @@ struct Tune {
   bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
   int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split
   int ntt_cols_div = 0;               // column-pass tile width: widest >> div (0..2)
+  int ntt_cols_kind = 0;              // column pass: 0 CTA-wide exchange, 1 warp-owned columns
   int ntt_rows_div = 0;               // row-pass tile height: tallest >> div (0..2)
   // transform ends fused with their neighbours (bit mask): 1 out-of-place
   // inverse instead of a copy, 2 key products in the special-limb forward

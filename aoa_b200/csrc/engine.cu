@@ -288,6 +288,7 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   else if (k == "ntt_split" && value >= -2 && value <= 2 && value == (int)value) h->e.tune.ntt_split = (int)value;
   else if (k == "ntt_cols_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_cols_div = (int)value;
   else if (k == "ntt_rows_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_rows_div = (int)value;
+  else if (k == "ntt_cols_kind" && (value == 0 || value == 1)) h->e.tune.ntt_cols_kind = (int)value;
   else if (k == "fuse" && value >= 0 && value <= 7 && value == (int)value) h->e.tune.fuse = (int)value;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob or value out of range: " + k);
   return AOA_OK;

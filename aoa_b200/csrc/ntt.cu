@@ -439,6 +439,153 @@ ntt_cols(NttBatch b) {
   }
 }
 
+// ---- column pass with warp-owned columns ----------------------------------------
+// The same column transforms as ntt_cols, with every column's T threads in
+// one warp (a warp holds 32 / T whole columns), so the exchange between the
+// two digit rounds needs only the warp: no CTA barrier inside an item.  A
+// producer warp streams the tiles (and the prime's twiddles when they change)
+// into two buffers through full / empty mbarrier pairs; compute warps wait
+// only for their buffer.  Row r of a tile sits at word
+//   P(r) = (W + 2) r + CW (k mod M) + 16 (k div M),  k = r >> (LO + G - 1),
+// M = 16 / CW: rows start 16-byte aligned and, for both digit access patterns
+// (rows (h << LO) + t and ((t G + g) << LO) + l over a warp's T lanes and CW
+// columns), the warp's 32 words fall twice on each 8-byte bank slot, so every
+// shared-memory access is conflict-free.
+template <int LOG_R, int NW>
+struct WoTile {
+  using D = Sub<LOG_R>;
+  static constexpr int CW = 32 / D::T;           // whole columns per warp
+  static constexpr int W = NW * CW;              // columns per tile
+  static constexpr int RS = W + 2;
+  static constexpr int M = 16 / CW;
+  static constexpr int SH = D::LO + D::G - 1;
+  static constexpr __host__ __device__ int row(int r) {
+    return RS * r + CW * ((r >> SH) % M) + 16 * ((r >> SH) / M);
+  }
+  static constexpr int WORDS = ((row(D::S - 1) + W + 15) / 16) * 16;   // one buffer, 128-byte multiple
+  static constexpr int THREADS = (NW + 1) * 32;
+  static constexpr size_t SMEM = 2 * (size_t)WORDS * 8 + 2 * (size_t)D::S * sizeof(ShoupW);
+  static constexpr int BY_SMEM = (int)((232448 - 1024) / (SMEM + 1024));
+  static constexpr int MIN_BLOCKS = BY_SMEM < 1 ? 1 : (BY_SMEM > 16 ? 16 : BY_SMEM);
+};
+
+template <int LOG_R, int NW, bool FWD>
+__global__ void __launch_bounds__(WoTile<LOG_R, NW>::THREADS, WoTile<LOG_R, NW>::MIN_BLOCKS)
+ntt_cols_wo(NttBatch b) {
+  using D = Sub<LOG_R>;
+  using Tl = WoTile<LOG_R, NW>;
+  constexpr int W = Tl::W, CW = Tl::CW, WORDS = Tl::WORDS;
+  extern __shared__ __align__(128) uint64_t dyn[];
+  __shared__ __align__(8) uint64_t full[2], empty[2];
+  const uint32_t sbuf = smem_u32(dyn);                       // [2][WORDS] words
+  ShoupW* tws = (ShoupW*)(dyn + 2 * WORDS);                   // [2][S]
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const long N = 1L << b.log_n, C = 1L << b.log_c;
+  const int G = gridDim.y;
+  if (threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], NW);
+    mbar_init(&empty[1], NW);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const int j_lo = (int)((long)blockIdx.y * b.nitems / G), j_hi = (int)((long)(blockIdx.y + 1) * b.nitems / G);
+  auto prime_of = [&](int j) { return b.first_prime + ((j / b.npolys) >> b.prime_shift); };
+  if (warp == NW) {
+    // producer: tile rows of W words (one bulk copy each) and, when the prime
+    // of the buffer changes, its S twiddles
+    int prime_in0 = -1, prime_in1 = -1;      // prime whose twiddles each buffer holds
+    int issued = 0;
+    bool ok = true;
+    for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
+      const int bi = it & 1;
+      if (it >= 2 && !mbar_wait(&empty[bi], ((it - 2) >> 1) & 1)) {
+        ok = false;
+        break;
+      }
+      const int limb = j / b.npolys, p = j % b.npolys;
+      const int prime = prime_of(j);
+      const bool new_tw = (bi ? prime_in1 : prime_in0) != prime;
+      if (bi) prime_in1 = prime;
+      else prime_in0 = prime;
+      if (lane == 0) mbar_expect_tx(&full[bi], (unsigned)(D::S * W * 8 + (new_tw ? D::S * 16 : 0)));
+      __syncwarp();
+      const uint64_t* src = (b.src ? b.src + ((long)p * b.src_poly_stride + limb) * N
+                                   : b.data + ((long)p * b.poly_stride + limb) * N) + (long)blockIdx.x * W;
+      for (int r = lane; r < D::S; r += 32)
+        bulk_g2s(sbuf + (bi * WORDS + Tl::row(r)) * 8, src + r * C, W * 8, &full[bi]);
+      if (new_tw && lane == 0)
+        bulk_g2s(smem_u32(tws + bi * D::S), (FWD ? b.tw : b.itw) + (long)prime * N, D::S * 16, &full[bi]);
+      issued = it + 1;
+    }
+    if (!ok && lane == 0) atomicOr(b.err, kErrWaitTimeout);
+    // the last copies into each buffer land before the CTA may exit (bounded)
+    if (issued >= 1) mbar_wait(&full[(issued - 1) & 1], ((issued - 1) >> 1) & 1);
+    if (issued >= 2) mbar_wait(&full[(issued - 2) & 1], ((issued - 2) >> 1) & 1);
+    return;
+  }
+  // compute warps: lanes (column w of the tile, thread t of its column)
+  const int t = lane % D::T;
+  const int w = warp * CW + lane / D::T;
+  for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
+    const int bi = it & 1;
+    if (!mbar_wait(&full[bi], (it >> 1) & 1)) {
+      if (lane == 0) atomicOr(b.err, kErrWaitTimeout);
+      return;
+    }
+    const int limb = j / b.npolys, p = j % b.npolys;
+    const PrimeConst& P = b.pc[prime_of(j)];
+    const uint64_t q = P.q;
+    const uint32_t sm = sbuf + (bi * WORDS + w) * 8;          // + row(r) * 8
+    const uint32_t stw = smem_u32(tws + bi * D::S);
+    uint64_t* x = b.data + ((long)p * b.poly_stride + limb) * N + (long)blockIdx.x * W + w;
+    if (FWD) {
+      uint64_t v[D::E];
+#pragma unroll
+      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + Tl::row((h << D::LO) + t) * 8);
+      fwd_high_s<LOG_R, true>(v, stw, q);
+#pragma unroll
+      for (int h = 0; h < D::E; h++) sts64(sm + Tl::row((h << D::LO) + t) * 8, v[h]);
+      __syncwarp();
+#pragma unroll
+      for (int g = 0; g < D::G; g++) {
+        const int hi = t * D::G + g;
+        uint64_t u[D::L];
+#pragma unroll
+        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + Tl::row((hi << D::LO) + l) * 8);
+        fwd_low_s<LOG_R, true>(u, stw, hi, q);
+#pragma unroll
+        for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
+      }
+    } else {
+      const ShoupW ninv{P.ninv, P.ninv_sh}, ninv_w1{P.ninv_w1, P.ninv_w1_sh};
+#pragma unroll
+      for (int g = 0; g < D::G; g++) {
+        const int hi = t * D::G + g;
+        uint64_t u[D::L];
+#pragma unroll
+        for (int l = 0; l < D::L; l++) u[l] = lds64(sm + Tl::row((hi << D::LO) + l) * 8);
+        inv_low_s<LOG_R, true>(u, stw, hi, q);
+#pragma unroll
+        for (int l = 0; l < D::L; l++) sts64(sm + Tl::row((hi << D::LO) + l) * 8, u[l]);
+      }
+      __syncwarp();
+      uint64_t v[D::E];
+#pragma unroll
+      for (int h = 0; h < D::E; h++) v[h] = lds64(sm + Tl::row((h << D::LO) + t) * 8);
+      inv_high_s<LOG_R, true>(v, stw, q, ninv, ninv_w1);
+#pragma unroll
+      for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];
+    }
+    // the buffer (tile and twiddles) is free once every lane has read it;
+    // the async-proxy refill is ordered after these generic accesses
+    fence_proxy_async();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[bi]);
+  }
+}
+
 // swizzled word offset inside one row of shared memory
 template <int LOG_S>
 __device__ __forceinline__ int swz(int hi, int lo) {
@@ -611,6 +758,17 @@ static void launch_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream
   note_launch();
 }
 
+template <int LOG_R, int NW>
+static void launch_cols_wo(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+  using Tl = WoTile<LOG_R, NW>;
+  const int C = 1 << b.log_c;
+  if (C % Tl::W) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: column tile does not divide C");
+  dim3 grid(C / Tl::W, ctas_per_tile(E, C / Tl::W, b.nitems, Tl::MIN_BLOCKS));
+  if (fwd) ntt_cols_wo<LOG_R, NW, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  else ntt_cols_wo<LOG_R, NW, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  note_launch();
+}
+
 template <int LOG_C, int DIV, bool LAZY>
 static void launch_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st, const NttEpi& epi) {
   using Tl = RowTile<LOG_C, DIV>;
@@ -632,6 +790,18 @@ static int tile_div(int knob) { return LAZY ? std::max(0, std::min(2, knob)) : 0
 template <bool LAZY>
 static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
   const int div = tile_div<LAZY>(E.tune.ntt_cols_div);
+  if (LAZY && E.tune.ntt_cols_kind == 1 && b.log_r >= 6 && b.log_r <= 9) {
+    // warp-owned columns: 8, 4 or 2 compute warps per CTA
+    switch (b.log_r * 4 + div) {
+#define AOA_WO(s)                                                    \
+  case s * 4 + 0: launch_cols_wo<s, 8>(E, b, fwd, st); return;       \
+  case s * 4 + 1: launch_cols_wo<s, 4>(E, b, fwd, st); return;       \
+  case s * 4 + 2: launch_cols_wo<s, 2>(E, b, fwd, st); return;
+      AOA_WO(6) AOA_WO(7) AOA_WO(8) AOA_WO(9)
+#undef AOA_WO
+      default: break;
+    }
+  }
   switch (b.log_r) {
 #define AOA_CASE(s)                                                \
   case s:                                                          \
@@ -683,10 +853,19 @@ static void allow_size() {
 }
 
 // Once per engine: opt every transform kernel in to its dynamic shared memory.
+template <int S, int NW>
+static void allow_wo() {
+  allow_smem(ntt_cols_wo<S, NW, true>, WoTile<S, NW>::SMEM);
+  allow_smem(ntt_cols_wo<S, NW, false>, WoTile<S, NW>::SMEM);
+}
+
 void ntt_init(Engine& E) {
 #define AOA_ALLOW(s) allow_size<s, 0>(); allow_size<s, 1>(); allow_size<s, 2>();
   AOA_NTT_SIZES(AOA_ALLOW)
 #undef AOA_ALLOW
+#define AOA_ALLOW_WO(s) allow_wo<s, 8>(); allow_wo<s, 4>(); allow_wo<s, 2>();
+  AOA_ALLOW_WO(6) AOA_ALLOW_WO(7) AOA_ALLOW_WO(8) AOA_ALLOW_WO(9)
+#undef AOA_ALLOW_WO
   int sms = 0;
   AOA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E.device));
   E.num_sms = sms;

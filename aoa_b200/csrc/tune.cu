@@ -81,6 +81,8 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
          [](Tune& t, double v) { t.ntt_split = (int)v; }},
         {"ntt_cols_div", {0, 1, 2}, [](const Tune& t) { return (double)t.ntt_cols_div; },
          [](Tune& t, double v) { t.ntt_cols_div = (int)v; }},
+        {"ntt_cols_kind", {0, 1}, [](const Tune& t) { return (double)t.ntt_cols_kind; },
+         [](Tune& t, double v) { t.ntt_cols_kind = (int)v; }},
         {"ntt_rows_div", {0, 1, 2}, [](const Tune& t) { return (double)t.ntt_rows_div; },
          [](Tune& t, double v) { t.ntt_rows_div = (int)v; }},
         {"ntt_waves", {1, 2, 0.5, 4}, [](const Tune& t) { return t.ntt_waves; },
@@ -116,9 +118,9 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
     for (int round = 0; round < 2; round++)
       for (const Knob& kn : knobs) descend(kn);
     snprintf(line, sizeof line,
-             "], \"best_ms\": %.4f, \"choice\": {\"ntt_split\": %d, \"ntt_cols_div\": %d, \"ntt_rows_div\": %d, "
-             "\"ntt_waves\": %g, \"ntt_chunk_bytes\": %ld}}",
-             best, E.tune.ntt_split, E.tune.ntt_cols_div, E.tune.ntt_rows_div, E.tune.ntt_waves,
+             "], \"best_ms\": %.4f, \"choice\": {\"ntt_split\": %d, \"ntt_cols_div\": %d, \"ntt_cols_kind\": %d, "
+             "\"ntt_rows_div\": %d, \"ntt_waves\": %g, \"ntt_chunk_bytes\": %ld}}",
+             best, E.tune.ntt_split, E.tune.ntt_cols_div, E.tune.ntt_cols_kind, E.tune.ntt_rows_div, E.tune.ntt_waves,
              E.tune.ntt_chunk_bytes);
     rep += line;
   });

@@ -96,7 +96,10 @@ int aoa_engine_destroy(aoa_engine* e);
  * "ntt_waves" (transform CTAs per pass in resident waves, default 1),
  * "ntt_split" (log2 C - floor(log2 N / 2) of the R x C transform split,
  * -2..2), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width and
- * row-pass tile height = widest >> div, 0..2) and "conv_tensor_cores"
+ * row-pass tile height = widest >> div, 0..2), "ntt_cols_kind" (0 CTA-wide
+ * exchange, 1 warp-owned columns), "fuse" (bit mask of fused transform
+ * ends: 1 out-of-place inverse, 2 key products, 4 key-switch combine) and
+ * "conv_tensor_cores"
  * (0/1: basis conversion on the int8 tensor cores where it applies).      */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
 /* Autotuner: times forward + inverse limb transforms of this engine's ring

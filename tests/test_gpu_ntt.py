@@ -91,17 +91,20 @@ def test_ntt_edge_values(ref_table):
 
 
 @pytest.mark.parametrize("log_n", [12, 15, 16])
-@pytest.mark.parametrize("shape", [(s, c, r) for s in (-2, -1, 0, 1, 2) for c, r in ((0, 0), (1, 2), (2, 1))])
+@pytest.mark.parametrize("shape", [(s, c, r, k) for s in (-2, -1, 0, 1, 2) for c, r in ((0, 0), (1, 2), (2, 1))
+                                   for k in (0, 1)])
 def test_ntt_launch_shapes_bit_exact(log_n, shape):
-    """Every split and tile shape the autotuner may pick gives the oracle's transform."""
+    """Every split, tile shape and column-pass kind the autotuner may pick
+    gives the oracle's transform."""
     require_gpu()
-    split, cdiv, rdiv = shape
+    split, cdiv, rdiv, kind = shape
     ps = oracle.gen_ntt_primes(60, 2 << log_n, 3)
     E, ctx, o = _engine_and_oracle(log_n, ps[:2], ps[2:])
     E.tune("ntt_split", split)
     E.tune("ntt_cols_div", cdiv)
     E.tune("ntt_rows_div", rdiv)
-    rng = np.random.default_rng(log_n + 7 * (split + 2))
+    E.tune("ntt_cols_kind", kind)
+    rng = np.random.default_rng(log_n + 7 * (split + 2) + 100 * kind)
     x = _rand(rng, ps, 1 << log_n, npolys=3)
     d = ctx.upload(x)
     ctx.ntt_fwd(d, 3, 0, 3)
