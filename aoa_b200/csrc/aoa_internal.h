@@ -46,6 +46,7 @@ struct Tune {
   // inverse instead of a copy, 2 key products in the special-limb forward
   // transform, 4 key-switch combine in the corrections' forward transform
   int fuse = 1;
+  int batch_streams = 2;              // streams a large HMult batch is split over (1 or 2)
 };
 
 // Device copy of the basis-conversion / rescale constants.
@@ -126,6 +127,12 @@ struct Ctx {
   size_t conv_bytes = 0;
   void* enc = nullptr;          // encoder / key generation buffer
   size_t enc_bytes = 0;
+  // second stream of the context: a large HMult batch runs as two halves on
+  // `stream` and `aux`, forked and joined by events (each half its own workspace)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  void* batch2 = nullptr;
+  size_t batch2_bytes = 0;
   int transform = AOA_NTT;      // transform domain of this context's evaluations (AOA_NTT / AOA_DGT)
 };
 

@@ -97,7 +97,7 @@ static bool fused(const Ctx& C, int what) { return C.transform == AOA_NTT && (C.
 // limbs 0..nlimbs-1) with the key-switch combine as its epilogue.
 static void combine_into(Ctx& C, uint64_t* Y, int npolys, int nlimbs, const uint64_t* base, long base_stride,
                          int base_polys, const uint64_t* KS, long ks_stride, int rescale_level, uint64_t* out,
-                         long out_stride, const OutPtrs* outp) {
+                         long out_stride, const OutPtrs* outp, cudaStream_t st = nullptr) {
   const Engine& E = *C.E;
   NttIo io;
   io.epi.mode = kEpiCombine;
@@ -115,7 +115,7 @@ static void combine_into(Ctx& C, uint64_t* Y, int npolys, int nlimbs, const uint
     io.epi.out = out;
     io.epi.out_stride = out_stride;
   }
-  ntt_batch_io(E, Y, npolys, 0, nlimbs, E.k, true, io, C.stream);
+  ntt_batch_io(E, Y, npolys, 0, nlimbs, E.k, true, io, st ? st : C.stream);
 }
 
 static void keyswitch_core(Ctx& C, const Workspace& w, const uint64_t* x_coef, const uint64_t* x_ntt,
@@ -322,24 +322,24 @@ static size_t batch_words(const Engine& E, int n) {
   return (size_t)E.N * n * (8 * E.k + 3 * std::max(E.kl, 1) + 4);
 }
 
-static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b,
-                              const aoa_swk* evk, bool do_rescale, int level) {
+static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_bytes, int n, aoa_ct* const* out,
+                              aoa_ct* const* a, aoa_ct* const* b, const aoa_swk* evk, bool do_rescale, int level) {
   const Engine& E = *C.E;
   const long N = E.N;
   const int m = level + 1, k = E.k, kl = E.kl;
   const long half = (long)k * N, ks = (long)(k + kl) * N;
   const size_t need = batch_words(E, n) * 8;
-  if (C.batch_bytes < need) {
-    if (C.batch) AOA_CUDA(cudaFreeAsync(C.batch, C.stream));
-    C.batch = nullptr;
-    C.batch_bytes = 0;
-    if (cudaMallocAsync(&C.batch, need, C.stream) != cudaSuccess) {
+  if (ws_bytes < need) {
+    if (ws) AOA_CUDA(cudaFreeAsync(ws, st));
+    ws = nullptr;
+    ws_bytes = 0;
+    if (cudaMallocAsync(&ws, need, st) != cudaSuccess) {
       cudaGetLastError();
       throw AoaError(AOA_ERR_OOM, "batch workspace allocation failed");
     }
-    C.batch_bytes = need;
+    ws_bytes = need;
   }
-  uint64_t* p = (uint64_t*)C.batch;
+  uint64_t* p = (uint64_t*)ws;
   uint64_t* D = p;  p += 3L * n * half;
   uint64_t* T = p;  p += (long)n * half;
   uint64_t* UB = p; p += (long)n * kl * N;
@@ -347,13 +347,10 @@ static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* 
   uint64_t* U = p;  p += 2L * n * N;
   uint64_t* CL = p; p += 2L * n * N;
   uint64_t* Y = p;
-  cudaStream_t st = C.stream;
   CtPtrs ptr;
   uint64_t sa[kMaxBatch], sb[kMaxBatch];
   int slots[kMaxBatch];
-  for (int z = 0; z < n; z++) {
-    to_domain(C, a[z], AOA_NTT, a[z]->level + 1);
-    to_domain(C, b[z], AOA_NTT, b[z]->level + 1);
+  for (int z = 0; z < n; z++) {                 // operands are in the transform domain already
     ptr.a[z] = a[z]->d;
     ptr.b[z] = b[z]->d;
     sa[z] = a[z]->scale;
@@ -398,7 +395,7 @@ static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* 
     ntt_batch(E, U, 2 * n, level, 1, 1, false, st);
     rescale_corrections(E, KS + (long)m * N, ks, U, N, CL, N, Y, half, 2 * n, level, st);
     if (fuse & kFuseCombine) {
-      combine_into(C, Y, 2 * n, level, D, half, 2 * n, KS, ks, level, nullptr, 0, &outp);
+      combine_into(C, Y, 2 * n, level, D, half, 2 * n, KS, ks, level, nullptr, 0, &outp, st);
     } else {
       ntt_batch(E, Y, 2 * n, 0, level, k, true, st);
       ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, level, 2 * n, level, st);
@@ -406,7 +403,7 @@ static void hmult_batch_group(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* 
   } else {
     moddown_conv(E, KS + (long)m * N, ks, Y, half, 2 * n, m, st);
     if (fuse & kFuseCombine) {
-      combine_into(C, Y, 2 * n, m, D, half, 2 * n, KS, ks, 0, nullptr, 0, &outp);
+      combine_into(C, Y, 2 * n, m, D, half, 2 * n, KS, ks, 0, nullptr, 0, &outp, st);
     } else {
       ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
       ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, m, 2 * n, 0, st);
@@ -439,6 +436,10 @@ void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* co
       throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
     idx[z] = z;
   }
+  for (int z = 0; z < n; z++) {                  // operands to the transform domain (poly_mul's rule)
+    to_domain(C, a[z], AOA_NTT, a[z]->level + 1);
+    to_domain(C, b[z], AOA_NTT, b[z]->level + 1);
+  }
   // group by level (the operands' common limb count), chunks of kMaxBatch
   auto lvl = [&](int z) { return std::min(a[z]->level, b[z]->level); };
   std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lvl(x) > lvl(y); });
@@ -452,7 +453,34 @@ void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* co
       ga.push_back(a[idx[t]]);
       gb.push_back(b[idx[t]]);
     }
-    hmult_batch_group(C, e - s, go.data(), ga.data(), gb.data(), evk, do_rescale, lvl(idx[s]));
+    const int g = e - s;
+    // halves run concurrently, so an output of one half must not be an
+    // operand of the other (within a launch all operands are read first)
+    bool cross = false;
+    for (int u = 0; u < g && !cross; u++)
+      for (int v = 0; v < g && !cross; v++)
+        cross = (u < g / 2) != (v < g / 2) && (go[u] == ga[v] || go[u] == gb[v]);
+    if (E.tune.batch_streams == 2 && g >= 8 && !cross) {
+      // two halves on the context's two streams: one half's memory-bound
+      // stages overlap the other's integer-bound transforms
+      if (!C.aux) {
+        AOA_CUDA(cudaStreamCreateWithFlags(&C.aux, cudaStreamNonBlocking));
+        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_fork, cudaEventDisableTiming));
+        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_join, cudaEventDisableTiming));
+      }
+      const int h = g / 2;
+      AOA_CUDA(cudaEventRecord(C.ev_fork, C.stream));
+      AOA_CUDA(cudaStreamWaitEvent(C.aux, C.ev_fork, 0));
+      hmult_batch_group(C, C.stream, C.batch, C.batch_bytes, h, go.data(), ga.data(), gb.data(), evk, do_rescale,
+                        lvl(idx[s]));
+      hmult_batch_group(C, C.aux, C.batch2, C.batch2_bytes, g - h, go.data() + h, ga.data() + h, gb.data() + h, evk,
+                        do_rescale, lvl(idx[s]));
+      AOA_CUDA(cudaEventRecord(C.ev_join, C.aux));
+      AOA_CUDA(cudaStreamWaitEvent(C.stream, C.ev_join, 0));
+    } else {
+      hmult_batch_group(C, C.stream, C.batch, C.batch_bytes, g, go.data(), ga.data(), gb.data(), evk, do_rescale,
+                        lvl(idx[s]));
+    }
     s = e;
   }
 }

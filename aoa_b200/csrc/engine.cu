@@ -289,6 +289,7 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   else if (k == "ntt_cols_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_cols_div = (int)value;
   else if (k == "ntt_rows_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_rows_div = (int)value;
   else if (k == "ntt_cols_kind" && (value == 0 || value == 1)) h->e.tune.ntt_cols_kind = (int)value;
+  else if (k == "batch_streams" && (value == 1 || value == 2)) h->e.tune.batch_streams = (int)value;
   else if (k == "fuse" && value >= 0 && value <= 7 && value == (int)value) h->e.tune.fuse = (int)value;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob or value out of range: " + k);
   return AOA_OK;
@@ -328,6 +329,13 @@ int aoa_ctx_destroy(aoa_ctx* h) {
     if (h->c.batch) AOA_CUDA(cudaFreeAsync(h->c.batch, h->c.stream));
     if (h->c.conv) AOA_CUDA(cudaFreeAsync(h->c.conv, h->c.stream));
     if (h->c.enc) AOA_CUDA(cudaFreeAsync(h->c.enc, h->c.stream));
+    if (h->c.aux) {
+      if (h->c.batch2) AOA_CUDA(cudaFreeAsync(h->c.batch2, h->c.aux));
+      AOA_CUDA(cudaStreamSynchronize(h->c.aux));
+      AOA_CUDA(cudaStreamDestroy(h->c.aux));
+      AOA_CUDA(cudaEventDestroy(h->c.ev_fork));
+      AOA_CUDA(cudaEventDestroy(h->c.ev_join));
+    }
     AOA_CUDA(cudaStreamSynchronize(h->c.stream));
     if (h->c.own_stream) AOA_CUDA(cudaStreamDestroy(h->c.stream));
   });

@@ -363,3 +363,33 @@ def test_fused_transform_ends_equal_separate_kernels(ref_table, log_n, fuse):
     assert np.array_equal(fused[0][0], w0[:k - 1]) and np.array_equal(fused[0][1], w1[:k - 1])
     r0, r1 = o.rotate_left(a, 3, keys["rtk"][3], k - 1, state=ST_COEF)
     assert np.array_equal(fused[4][0], r0) and np.array_equal(fused[4][1], r1)
+
+
+def test_hmult_batch_two_streams_equal_one_stream(ref_table):
+    """A large batch split over the context's two streams (halves forked and
+    joined by events) gives the residues of the single-stream batch, with an
+    output aliasing an operand inside a half and across halves."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=19)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(12)
+    N, k = E.N, E.k
+    data = [(_rand_ct(rng, Q, N, k), _rand_ct(rng, Q, N, k)) for _ in range(12)]
+
+    def run(streams, cross):
+        E.tune("batch_streams", streams)
+        A = [aoa.Ciphertext.from_residues(ctx, *x[0], slots=8, scale=1 << 35, domain=aoa.AOA_NTT) for x in data]
+        Bc = [aoa.Ciphertext.from_residues(ctx, *x[1], slots=8, scale=1 << 36, domain=aoa.AOA_NTT) for x in data]
+        outs = [aoa.Ciphertext(ctx) for _ in data]
+        outs[2] = A[2]                                   # aliasing inside a half
+        if cross:
+            outs[1] = Bc[9]                              # an output is an operand of the other half
+        aoa.ckks_mul_batch(ctx, outs, A, Bc, evk)
+        return [x.download(nlimbs=k - 1, domain=aoa.AOA_COEF) for x in outs]
+
+    for cross in (False, True):
+        one, two = run(1, cross), run(2, cross)
+        for x, y in zip(one, two):
+            assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
