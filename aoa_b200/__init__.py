@@ -377,6 +377,26 @@ def ckks_mul_batch(ctx, outs, c1s, c2s, evk, rescale=True):
     capi.check(capi.load().aoa_hmult_batch(ctx.handle, n, o, a, b, _h(evk), 1 if rescale else 0))
 
 
+def ckks_rotate_batch(ctx, outs, cts, steps, rtk):
+    """outs[i] = cts[i] rotated left by `steps` slots, one key for the batch,
+    in grouped batched launches."""
+    n = len(outs)
+    if len(cts) != n:
+        raise ValueError("batch lists differ in length")
+    arr = ctypes.c_void_p * max(n, 1)
+    capi.check(capi.load().aoa_rotate_batch(ctx.handle, n, arr(*[x.handle.value for x in outs]),
+                                            arr(*[x.handle.value for x in cts]), steps, _h(rtk)))
+
+
+def ckks_conjugate_batch(ctx, outs, cts, cjk):
+    n = len(outs)
+    if len(cts) != n:
+        raise ValueError("batch lists differ in length")
+    arr = ctypes.c_void_p * max(n, 1)
+    capi.check(capi.load().aoa_conjugate_batch(ctx.handle, n, arr(*[x.handle.value for x in outs]),
+                                               arr(*[x.handle.value for x in cts]), _h(cjk)))
+
+
 # ---- encoder and encryption (aoa-ntt src/ckks/encoder.cu, ckks.cpp:87-192) --------
 
 def ckks_encode(ctx, values, empty_slots=0, scale=None, nlimbs=None, domain=AOA_COEF, out=None):

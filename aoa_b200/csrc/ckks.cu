@@ -8,6 +8,8 @@
 // it back and forth, and multiplies with the key in one kernel.
 #include <cstring>
 
+#include <functional>
+
 #include "aoa_internal.h"
 
 using namespace aoa;
@@ -417,6 +419,51 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
   }
 }
 
+// Runs `group(stream, workspace, bytes, count, outs, as, bs, level)` over groups of
+// equal level, a group of 8 or more as two halves on the context's two
+// streams unless an output of one half is an input of the other.
+template <class F>
+static void run_grouped(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b,
+                        const std::function<int(int)>& lvl, F&& group) {
+  const Engine& E = *C.E;
+  std::vector<int> idx(n);
+  for (int z = 0; z < n; z++) idx[z] = z;
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lvl(x) > lvl(y); });
+  std::vector<aoa_ct*> go, ga, gb;
+  for (int s = 0; s < n;) {
+    int e = s;
+    while (e < n && lvl(idx[e]) == lvl(idx[s]) && e - s < kMaxBatch) e++;
+    go.clear(); ga.clear(); gb.clear();
+    for (int t = s; t < e; t++) {
+      go.push_back(out[idx[t]]);
+      ga.push_back(a[idx[t]]);
+      gb.push_back(b ? b[idx[t]] : a[idx[t]]);
+    }
+    const int g = e - s;
+    bool cross = false;
+    for (int u = 0; u < g && !cross; u++)
+      for (int v = 0; v < g && !cross; v++)
+        cross = (u < g / 2) != (v < g / 2) && (go[u] == ga[v] || go[u] == gb[v]);
+    if (E.tune.batch_streams == 2 && g >= 8 && !cross) {
+      if (!C.aux) {
+        AOA_CUDA(cudaStreamCreateWithFlags(&C.aux, cudaStreamNonBlocking));
+        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_fork, cudaEventDisableTiming));
+        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_join, cudaEventDisableTiming));
+      }
+      const int h = g / 2;
+      AOA_CUDA(cudaEventRecord(C.ev_fork, C.stream));
+      AOA_CUDA(cudaStreamWaitEvent(C.aux, C.ev_fork, 0));
+      group(C.stream, C.batch, C.batch_bytes, h, go.data(), ga.data(), gb.data(), lvl(idx[s]));
+      group(C.aux, C.batch2, C.batch2_bytes, g - h, go.data() + h, ga.data() + h, gb.data() + h, lvl(idx[s]));
+      AOA_CUDA(cudaEventRecord(C.ev_join, C.aux));
+      AOA_CUDA(cudaStreamWaitEvent(C.stream, C.ev_join, 0));
+    } else {
+      group(C.stream, C.batch, C.batch_bytes, g, go.data(), ga.data(), gb.data(), lvl(idx[s]));
+    }
+    s = e;
+  }
+}
+
 void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b, const aoa_swk* evk,
                  bool do_rescale) {
   const Engine& E = *C.E;
@@ -427,62 +474,107 @@ void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* co
   if (!out || !a || !b) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
   if (!evk || !evk->d) throw AoaError(AOA_ERR_NO_KEY, "missing relinearisation key");
   if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
-  std::vector<int> idx(n);
   for (int z = 0; z < n; z++) {
     if (!out[z] || !a[z] || !b[z]) throw AoaError(AOA_ERR_BAD_PARAM, "null ciphertext in batch");
     if (a[z]->level == 0 || b[z]->level == 0)
       throw AoaError(AOA_ERR_LEVEL_EXHAUSTED, "The ciphertext level is 0. No more rescaling is possible.");
     if (a[z]->slots != b[z]->slots)
       throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
-    idx[z] = z;
   }
   for (int z = 0; z < n; z++) {                  // operands to the transform domain (poly_mul's rule)
     to_domain(C, a[z], AOA_NTT, a[z]->level + 1);
     to_domain(C, b[z], AOA_NTT, b[z]->level + 1);
   }
   // group by level (the operands' common limb count), chunks of kMaxBatch
-  auto lvl = [&](int z) { return std::min(a[z]->level, b[z]->level); };
-  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lvl(x) > lvl(y); });
-  std::vector<aoa_ct*> go, ga, gb;
-  for (int s = 0; s < n;) {
-    int e = s;
-    while (e < n && lvl(idx[e]) == lvl(idx[s]) && e - s < kMaxBatch) e++;
-    go.clear(); ga.clear(); gb.clear();
-    for (int t = s; t < e; t++) {
-      go.push_back(out[idx[t]]);
-      ga.push_back(a[idx[t]]);
-      gb.push_back(b[idx[t]]);
+  run_grouped(C, n, out, a, b, [&](int z) { return std::min(a[z]->level, b[z]->level); },
+              [&](cudaStream_t st, void*& ws, size_t& wb, int g, aoa_ct* const* go, aoa_ct* const* ga,
+                  aoa_ct* const* gb, int level) {
+                hmult_batch_group(C, st, ws, wb, g, go, ga, gb, evk, do_rescale, level);
+              });
+}
+
+// Batched Galois automorphism + key switch of n ciphertexts at one level with
+// one key (apply_galois per op: ckks_rotate_left / ckks_conjugate,
+// ckks.cpp:953-1040), every stage one launch over the batch.  Workspace
+// (N-word limbs): R [2][n][k] (permuted c0 | permuted c1)  T [n][k]
+// UB [n][kl]  KS [2][n][k+kl]  Y [2][n][k].
+static size_t galois_words(const Engine& E, int n) {
+  return (size_t)E.N * n * (3 * E.k + E.kl + 2 * (E.k + E.kl) + 2 * E.k);
+}
+
+static void galois_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_bytes, int n, aoa_ct* const* out,
+                               aoa_ct* const* in, long galois, const aoa_swk* key, int level) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  const int m = level + 1, k = E.k, kl = E.kl;
+  const long half = (long)k * N, ks = (long)(k + kl) * N;
+  const size_t need = galois_words(E, n) * 8;
+  if (ws_bytes < need) {
+    if (ws) AOA_CUDA(cudaFreeAsync(ws, st));
+    ws = nullptr;
+    ws_bytes = 0;
+    if (cudaMallocAsync(&ws, need, st) != cudaSuccess) {
+      cudaGetLastError();
+      throw AoaError(AOA_ERR_OOM, "batch workspace allocation failed");
     }
-    const int g = e - s;
-    // halves run concurrently, so an output of one half must not be an
-    // operand of the other (within a launch all operands are read first)
-    bool cross = false;
-    for (int u = 0; u < g && !cross; u++)
-      for (int v = 0; v < g && !cross; v++)
-        cross = (u < g / 2) != (v < g / 2) && (go[u] == ga[v] || go[u] == gb[v]);
-    if (E.tune.batch_streams == 2 && g >= 8 && !cross) {
-      // two halves on the context's two streams: one half's memory-bound
-      // stages overlap the other's integer-bound transforms
-      if (!C.aux) {
-        AOA_CUDA(cudaStreamCreateWithFlags(&C.aux, cudaStreamNonBlocking));
-        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_fork, cudaEventDisableTiming));
-        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_join, cudaEventDisableTiming));
-      }
-      const int h = g / 2;
-      AOA_CUDA(cudaEventRecord(C.ev_fork, C.stream));
-      AOA_CUDA(cudaStreamWaitEvent(C.aux, C.ev_fork, 0));
-      hmult_batch_group(C, C.stream, C.batch, C.batch_bytes, h, go.data(), ga.data(), gb.data(), evk, do_rescale,
-                        lvl(idx[s]));
-      hmult_batch_group(C, C.aux, C.batch2, C.batch2_bytes, g - h, go.data() + h, ga.data() + h, gb.data() + h, evk,
-                        do_rescale, lvl(idx[s]));
-      AOA_CUDA(cudaEventRecord(C.ev_join, C.aux));
-      AOA_CUDA(cudaStreamWaitEvent(C.stream, C.ev_join, 0));
-    } else {
-      hmult_batch_group(C, C.stream, C.batch, C.batch_bytes, g, go.data(), ga.data(), gb.data(), evk, do_rescale,
-                        lvl(idx[s]));
-    }
-    s = e;
+    ws_bytes = need;
   }
+  uint64_t* p = (uint64_t*)ws;
+  uint64_t* R = p;  p += 2L * n * half;
+  uint64_t* T = p;  p += (long)n * half;
+  uint64_t* UB = p; p += (long)n * kl * N;
+  uint64_t* KS = p; p += 2L * n * ks;
+  uint64_t* Y = p;
+  uint64_t* X = R + (long)n * half;
+  CtPtrs ptr;
+  int slots[kMaxBatch];
+  uint64_t scale[kMaxBatch];
+  for (int z = 0; z < n; z++) {
+    ptr.a[z] = in[z]->d;
+    slots[z] = in[z]->slots;
+    scale[z] = in[z]->scale;
+  }
+  automorph_ntt_batch_op(E, ptr, half, R, n, galois, m, st);
+  NttIo io;                                      // inverse of the permuted c1, out of place
+  io.src = X;
+  io.src_poly_stride = k;
+  ntt_batch_io(E, T, n, 0, m, k, false, io, st);
+  modup(E, T, half, UB, (long)kl * N, n, level, st);
+  ntt_batch(E, UB, n, k, kl, kl, true, st);
+  keyswitch_mul_batch_op(E, X, half, UB, (long)kl * N, key->d, KS, ks, n, m, st);
+  ntt_batch(E, KS + (long)m * N, 2 * n, k, kl, k + kl, false, st);
+  moddown_conv(E, KS + (long)m * N, ks, Y, half, 2 * n, m, st);
+  ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
+  OutPtrs outp;
+  for (int z = 0; z < n; z++) {
+    outp.p[z] = out[z]->d;
+    outp.p[n + z] = out[z]->d + half;
+  }
+  ks_combine_ptr(E, outp, R, half, KS, ks, Y, half, m, 2 * n, 0, st, n);   // c0 base for poly 0 only
+  for (int z = 0; z < n; z++) {
+    out[z]->level = level;
+    out[z]->slots = slots[z];
+    out[z]->scale = scale[z];
+    out[z]->domain = AOA_NTT;
+  }
+}
+
+void galois_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* in, long galois, const aoa_swk* key) {
+  const Engine& E = *C.E;
+  if (C.transform != AOA_NTT) throw AoaError(AOA_ERR_BAD_PARAM, "batched rotations run on the NTT transform only");
+  if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
+  if (n == 0) return;
+  if (!out || !in) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
+  if (!key || !key->d) throw AoaError(AOA_ERR_NO_KEY, "missing switching key for this automorphism");
+  if (key->domain != AOA_NTT) throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
+  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
+  for (int z = 0; z < n; z++) {
+    if (!out[z] || !in[z]) throw AoaError(AOA_ERR_BAD_PARAM, "null ciphertext in batch");
+    to_domain(C, in[z], AOA_NTT, in[z]->level + 1);
+  }
+  run_grouped(C, n, out, in, nullptr, [&](int z) { return in[z]->level; },
+              [&](cudaStream_t st, void*& ws, size_t& wb, int g, aoa_ct* const* go, aoa_ct* const* ga,
+                  aoa_ct* const*, int level) { galois_batch_group(C, st, ws, wb, g, go, ga, galois, key, level); });
 }
 
 // The reference's per-call HMult + relinearise + rescale, step for step
@@ -788,6 +880,22 @@ int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rt
     const long g = (long)h_powmod(5, (uint64_t)r, (uint64_t)M);
     apply_galois(c->c, out, in, g, rtk);
   });
+}
+
+// batched forms: every op of the batch rotates by the same step with the same key
+int aoa_rotate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, int steps, const aoa_swk* rtk) {
+  if (!c) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    long r = steps % (E.N / 2);
+    if (r < 0) r += E.N / 2;
+    galois_batch(c->c, n, out, in, (long)h_powmod(5, (uint64_t)r, (uint64_t)(2 * E.N)), rtk);
+  });
+}
+
+int aoa_conjugate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, const aoa_swk* cjk) {
+  if (!c) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { galois_batch(c->c, n, out, in, 2 * c->c.E->N - 1, cjk); });
 }
 
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk) {

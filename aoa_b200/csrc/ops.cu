@@ -125,6 +125,20 @@ __global__ void automorph_ntt(uint64_t* out, const uint64_t* in, long poly_strid
 
 // ---- batched variants (one launch for a batch of ciphertexts) ---------------------
 
+// NTT-domain automorphism of both polys of ciphertext z = blockIdx.z / 2
+// (poly blockIdx.z % 2, stride half) into out: poly 0 of every op first
+// (op stride half), then poly 1 (block offset n*half).
+__global__ void automorph_ntt_batch(CtPtrs ptr, long half, uint64_t* out, int n, long galois, int log_n) {
+  const long N = 1L << log_n;
+  const long p = coef_index();
+  const int z = blockIdx.z >> 1, poly = blockIdx.z & 1;
+  const uint32_t br = __brev((uint32_t)p) >> (32 - log_n);
+  const long e = ((2L * br + 1) * galois) & (2 * N - 1);
+  const long src = __brev((uint32_t)((e - 1) >> 1)) >> (32 - log_n);
+  const long limb = (long)blockIdx.y * N;
+  out[(long)poly * n * half + (long)z * half + limb + p] = ptr.a[z][(long)poly * half + limb + src];
+}
+
 // tensor for op z = blockIdx.z: a = ptr.a[z], b = ptr.b[z] ([c0 | c1], stride half);
 // outputs to the blocks D0 = D, D1 = D + n*half, D2 = D + 2n*half, op stride half.
 __global__ void hmult_tensor_batch(CtPtrs ptr, long half, uint64_t* D, int n, const PrimeConst* pc, int log_n) {
@@ -224,6 +238,13 @@ void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, c
 void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,
                        int nlimbs, int npolys, cudaStream_t st) {
   automorph_coef<<<ew_grid(E, nlimbs, npolys), 256, 0, st>>>(out, in, poly_stride, galois, E.d_pc, E.log_n); note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+void automorph_ntt_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* out, int n, long galois,
+                            int nlimbs, cudaStream_t st) {
+  automorph_ntt_batch<<<ew_grid(E, nlimbs, 2 * n), 256, 0, st>>>(ptr, half, out, n, galois, E.log_n);
+  note_launch();
   AOA_CHECK_LAUNCH();
 }
 

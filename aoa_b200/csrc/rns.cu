@@ -560,16 +560,16 @@ __global__ void ks_combine_kernel(uint64_t* out, long out_stride, const uint64_t
 }
 
 // Same epilogue writing poly p to outp.p[p] (a list of output polys).
-__global__ void ks_combine_ptr_kernel(OutPtrs outp, const uint64_t* base, long base_stride, const uint64_t* k,
-                                      long k_stride, const uint64_t* y, long y_stride, const ShoupW* binv,
-                                      const ShoupW* resc, const PrimeConst* pc, int log_n) {
+__global__ void ks_combine_ptr_kernel(OutPtrs outp, const uint64_t* base, long base_stride, int base_polys,
+                                      const uint64_t* k, long k_stride, const uint64_t* y, long y_stride,
+                                      const ShoupW* binv, const ShoupW* resc, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
   const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y, p = blockIdx.z;
   const long off = (long)i * N + c;
   const uint64_t q = pc[i].q;
   const uint64_t kv = k[p * k_stride + off], yv = y[p * y_stride + off];
-  const uint64_t bv = base ? base[p * base_stride + off] : 0;
+  const uint64_t bv = base && p < base_polys ? base[p * base_stride + off] : 0;
   uint64_t r;
   if (resc) {
     r = shoup(sub_mod(add_mod(bv, shoup(kv, binv[i], q), q), yv, q), resc[i], q);
@@ -581,12 +581,12 @@ __global__ void ks_combine_ptr_kernel(OutPtrs outp, const uint64_t* base, long b
 
 void ks_combine_ptr(const Engine& E, const OutPtrs& outp, const uint64_t* base, long base_stride, const uint64_t* k,
                     long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys, int rescale_level,
-                    cudaStream_t st) {
+                    cudaStream_t st, int base_polys) {
   if (nlimbs <= 0) return;
   dim3 grid(E.N / 256, nlimbs, npolys);
   const ShoupW* resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
-  ks_combine_ptr_kernel<<<grid, 256, 0, st>>>(outp, base, base_stride, k, k_stride, y, y_stride, E.rns.moddown_binv,
-                                              resc, E.d_pc, E.log_n);
+  ks_combine_ptr_kernel<<<grid, 256, 0, st>>>(outp, base, base_stride, base_polys < 0 ? npolys : base_polys, k,
+                                              k_stride, y, y_stride, E.rns.moddown_binv, resc, E.d_pc, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
 }

@@ -262,8 +262,12 @@ int aoa_sub(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b);
 /* ckks_rotate_left (steps > 0) / ckks_rotate_right (steps < 0, i.e. left by
  * N/2 - |steps|) with the matching key (ckks.cpp:953-1009).                  */
 int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk);
+/* n rotations by the same step with the same key (each op as aoa_rotate),
+ * every stage one launch over the batch grouped by level; NTT contexts.    */
+int aoa_rotate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, int steps, const aoa_swk* rtk);
 /* ckks_conjugate (ckks.cpp:1011-1040) */
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk);
+int aoa_conjugate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, const aoa_swk* cjk);
 
 /* --- CUDA-graph capture of a context's asynchronous work (no reference
  *     counterpart: the reference launches every kernel from the host).  Only

@@ -393,3 +393,53 @@ def test_hmult_batch_two_streams_equal_one_stream(ref_table):
         one, two = run(1, cross), run(2, cross)
         for x, y in zip(one, two):
             assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+
+
+@pytest.mark.parametrize("count", [5, 12])
+def test_rotate_batch_equals_single_rotations(ref_table, count):
+    """Batched rotations (one key, mixed levels, an output aliasing its input;
+    12 ops take the two-stream split) give the per-call residues, and the
+    oracle's for one op."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=14, rotations=(3,), conjugation=True)
+    rtk = aoa.SwitchKey(ctx, *keys["rtk"][3])
+    cjk = aoa.SwitchKey(ctx, *keys["cjk"])
+    rng = np.random.default_rng(15)
+    N, k = E.N, E.k
+    data = [_rand_ct(rng, Q, N, k) for _ in range(count)]
+    levels = [k - 1 - (z % 3) for z in range(count)]
+
+    def make():
+        cts = []
+        for x, lv in zip(data, levels):
+            c = aoa.Ciphertext.from_residues(ctx, *x, slots=N // 2, scale=1 << 40,
+                                             domain=aoa.AOA_NTT if lv % 2 else aoa.AOA_COEF)
+            c.set(lv, N // 2, 1 << 40, c.domain)
+            cts.append(c)
+        return cts
+
+    for batch_fn, single_fn, key in ((lambda o_, c_: aoa.ckks_rotate_batch(ctx, o_, c_, 3, rtk),
+                                      lambda o_, c_: aoa.ckks_rotate_left(ctx, o_, c_, 3, rtk), rtk),
+                                     (lambda o_, c_: aoa.ckks_conjugate_batch(ctx, o_, c_, cjk),
+                                      lambda o_, c_: aoa.ckks_conjugate(ctx, o_, c_, cjk), cjk)):
+        cts = make()
+        outs = [aoa.Ciphertext(ctx) for _ in cts]
+        outs[0] = cts[0]                                   # in place
+        batch_fn(outs, cts)
+        got = [x.download(nlimbs=x.level + 1, domain=aoa.AOA_COEF) for x in outs]
+        ref = make()
+        for z, (c, lv) in enumerate(zip(ref, levels)):
+            w = aoa.Ciphertext(ctx)
+            single_fn(w, c)
+            assert outs[z].level == lv == w.level
+            want = w.download(nlimbs=lv + 1, domain=aoa.AOA_COEF)
+            assert np.array_equal(got[z][0], want[0]) and np.array_equal(got[z][1], want[1]), z
+    # op 0 is at level k - 1 in coefficients: the oracle's rotation of the same residues
+    w0, w1 = o.rotate_left(data[0], 3, keys["rtk"][3], k - 1, state=ST_COEF)
+    cts = make()
+    outs = [aoa.Ciphertext(ctx) for _ in cts]
+    aoa.ckks_rotate_batch(ctx, outs, cts, 3, rtk)
+    g0, g1 = outs[0].download(nlimbs=k, domain=aoa.AOA_COEF)
+    assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
