@@ -20,7 +20,8 @@ import time
 import numpy as np
 
 from . import (AOA_COEF, AOA_NTT, Ciphertext, Context, Engine, Graph, SwitchKey, ckks_add, ckks_encode,
-               ckks_mul_batch, ckks_mul_plain, ckks_mul_pt, ckks_rescale, ckks_rotate_left, ckks_sumslots, params)
+               ckks_mul_batch, ckks_mul_plain, ckks_mul_pt, ckks_rescale, ckks_rotate_batch, ckks_rotate_left,
+               ckks_sumslots, params)
 
 
 def _rand_residues(rng, primes, n):
@@ -250,3 +251,117 @@ class Server:
         for c in (c for cs in self.pool.values() for c in cs):
             c.sync()
         return reqs
+
+
+# ---------------------------------------------------------------------------------
+
+class BatchServer(Server):
+    """The same requests served with iteration-level batching: every
+    iteration advances each active request of a ring degree by one stage of
+    its chain (plaintext multiply + rescale, one rotate-and-add step of the
+    slot sum, final rescale), the rotations of a stage batched over all the
+    requests at that stage (aoa_rotate_batch: one key, grouped by level);
+    requests that arrive join at the next iteration, finished ones leave.
+    One context per degree; completion is the end of the iteration that
+    finishes a request (an event on the context's stream)."""
+
+    def __init__(self, *args, max_inflight=2, **kw):
+        kw["slots_per_degree"] = 1
+        super().__init__(*args, **kw)
+        self.max_inflight = max_inflight
+
+    def _steps(self, ln):
+        slots = self.slots[ln]
+        out, i = [], slots >> 1
+        while i >= 1:
+            out.append(i)
+            i >>= 1
+        return out
+
+    def _iteration(self, ln, active):
+        """Enqueue one stage for every active request of degree 2^ln; returns
+        the requests this iteration finishes."""
+        ctx = self.pool[ln][0]
+        steps = self._steps(ln)
+        by_stage = {}
+        for r in active:
+            by_stage.setdefault(r["stage"], []).append(r)
+        done = []
+        for stage, reqs in by_stage.items():
+            if stage == 0:
+                for r in reqs:
+                    ct = r["ct"]
+                    ct.set(r["m"] - 1, self.slots[ln], self.scale, ct.domain)
+                    ckks_mul_pt(ctx, r["out"], ct, self.weights[ln], self.scale, rescale=True)
+            elif stage <= len(steps):
+                step = steps[stage - 1]
+                ckks_rotate_batch(ctx, [r["prod"] for r in reqs], [r["out"] for r in reqs], step,
+                                  self.keys[ln][step])
+                for r in reqs:
+                    ckks_add(ctx, r["out"], r["out"], r["prod"])
+            else:
+                for r in reqs:
+                    ckks_rescale(ctx, r["out"])
+                    done.append(r)
+            for r in reqs:
+                r["stage"] += 1
+        return done
+
+    def submit(self, ctx_index, req):
+        """Run one request alone through the same stages."""
+        ln = req["log_n"]
+        req["stage"] = 0
+        while req["stage"] <= len(self._steps(ln)) + 1:
+            self._iteration(ln, [req])
+
+    def run(self, requests, rate=None, poll=0.0):
+        import torch
+        rng = np.random.default_rng(17)
+        n = len(requests)
+        arrivals = np.zeros(n) if rate is None else np.cumsum(rng.exponential(1.0 / rate, n))
+        for r in requests:
+            r["stage"] = 0
+        active = {ln: [] for ln in self.log_ns}
+        inflight = {ln: [] for ln in self.log_ns}        # (event, finished request ids)
+        pending = list(range(n))
+        done_at = np.zeros(n)
+        ids = {id(r): i for i, r in enumerate(requests)}
+        t0 = time.perf_counter()
+        remaining = n
+        while remaining:
+            now = time.perf_counter() - t0
+            for ln in self.log_ns:                          # completions
+                keep = []
+                for ev, fin in inflight[ln]:
+                    if ev.query():
+                        t = time.perf_counter() - t0
+                        for i in fin:
+                            done_at[i] = t
+                            remaining -= 1
+                            self.hbm_used -= self.footprint(ln)
+                    else:
+                        keep.append((ev, fin))
+                inflight[ln] = keep
+            still = []
+            for i in pending:                               # admissions
+                r = requests[i]
+                ln = r["log_n"]
+                if arrivals[i] > now or self.hbm_used + self.footprint(ln) > self.hbm_budget:
+                    still.append(i)
+                    continue
+                active[ln].append(r)
+                self.hbm_used += self.footprint(ln)
+            pending = still
+            for ln in self.log_ns:                          # one iteration per degree
+                if not active[ln] or len(inflight[ln]) >= self.max_inflight:
+                    continue
+                fin = self._iteration(ln, active[ln])
+                ev = torch.cuda.Event()
+                ev.record(torch.cuda.ExternalStream(self.pool[ln][0].stream))
+                inflight[ln].append((ev, [ids[id(r)] for r in fin]))
+                finished = {id(r) for r in fin}
+                active[ln] = [r for r in active[ln] if id(r) not in finished]
+            if poll:
+                time.sleep(poll)
+        wall = time.perf_counter() - t0
+        return done_at - arrivals, wall

@@ -278,7 +278,7 @@ def systems_workloads(aoa, torch):
     (plaintext-weight multiply + rescale, rotate-and-sum, rescale; N in
     {2^15, 2^16}, live limbs 6..30) at 5 Poisson rates relative to its measured
     saturation throughput."""
-    from aoa_b200.workloads import UnevenBatch, Server
+    from aoa_b200.workloads import UnevenBatch, Server, BatchServer
     wb = UnevenBatch(n_ops=512, seed=4, autotune=True)
 
     def timed_multi(fn):
@@ -327,6 +327,23 @@ def systems_workloads(aoa, torch):
                "hbm_budget_bytes": 8 << 30, "rates": rates,
                "request": "ct*w (plaintext, rescale) + rotate-and-sum over N/2 slots + rescale; N in {2^15,2^16}, "
                           "live limbs 6..30; latency = arrival to completion (host clock)"}
+    del srv, reqs
+    # the same requests with iteration-level batching (one context per degree)
+    bsrv = BatchServer(log_ns=(15, 16), hbm_budget=8 << 30, autotune=True)
+    breqs = bsrv.make_requests(48, seed=6)
+    bsrv.run(breqs[:8], rate=None)
+    lat, wall = bsrv.run(breqs, rate=None)
+    bsat = len(breqs) / wall
+    brates = []
+    for f in (0.25, 0.5, 0.75, 0.9, 1.1):
+        lat, wall = bsrv.run(breqs, rate=f * bsat)
+        brates.append({"rate_factor": f, "offered_req_per_s": f * bsat, "served_req_per_s": len(breqs) / wall,
+                       "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000)})
+    serving["iteration_batched"] = {
+        "saturation_req_per_s": bsat, "rates": brates,
+        "schedule": "one context per degree; each iteration advances every active request one stage, the "
+                    "rotations of a stage in one batched launch sequence (aoa_rotate_batch); arrivals join at "
+                    "the next iteration"}
     return uneven, serving
 
 

@@ -82,3 +82,21 @@ def test_serving_results_alone_equal_in_mix():
         srv.pool[r["log_n"]][0].sync()
         w0, w1 = r["out"].download(nlimbs=r["out"].level + 1, domain=1)
         assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+
+
+def test_batched_serving_results_alone_equal_in_mix():
+    """Iteration-level batching (rotations of requests at the same stage in one
+    batched launch sequence): every result equals the request run alone."""
+    require_gpu()
+    from aoa_b200.workloads import BatchServer
+    srv = BatchServer(log_ns=(11, 12), k=6, kl=5, hbm_budget=1 << 30, n_slots_used=8)
+    mixed = srv.make_requests(10, seed=7)
+    lat, wall = srv.run(mixed, rate=2000.0)
+    assert np.all(lat >= 0) and wall > 0
+    got = [r["out"].download(nlimbs=r["out"].level + 1, domain=1) for r in mixed]
+    alone = srv.make_requests(10, seed=7)
+    for r, (g0, g1) in zip(alone, got):
+        srv.submit(0, r)
+        srv.pool[r["log_n"]][0].sync()
+        w0, w1 = r["out"].download(nlimbs=r["out"].level + 1, domain=1)
+        assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
