@@ -443,3 +443,29 @@ def test_rotate_batch_equals_single_rotations(ref_table, count):
     aoa.ckks_rotate_batch(ctx, outs, cts, 3, rtk)
     g0, g1 = outs[0].download(nlimbs=k, domain=aoa.AOA_COEF)
     assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+
+
+def test_tensor_core_and_cuda_core_conversions_agree(ref_table):
+    """The int8 tensor-core basis conversion and the CUDA-core kernel give the
+    same residues (ModUp, ModDown and the merged ModDown + rescale of HMult)."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=23)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(24)
+    N, k = E.N, E.k
+    a, b = _rand_ct(rng, Q, N, k), _rand_ct(rng, Q, N, k)
+    res = []
+    for tc in (1, 0):
+        E.tune("conv_tensor_cores", tc)
+        outs = []
+        for rescale in (True, False):
+            ca = aoa.Ciphertext.from_residues(ctx, *a, slots=8, scale=1 << 35)
+            cb = aoa.Ciphertext.from_residues(ctx, *b, slots=8, scale=1 << 35)
+            o1 = aoa.Ciphertext(ctx)
+            (aoa.ckks_mul if rescale else aoa.ckks_mul_without_rescale)(ctx, o1, ca, cb, evk)
+            outs.append(o1.download(nlimbs=o1.level + 1))
+        res.append(outs)
+    for x, y in zip(res[0], res[1]):
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
