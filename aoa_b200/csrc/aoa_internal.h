@@ -35,7 +35,8 @@ struct AoaError : public std::runtime_error {
 constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration limit
 
 struct Tune {
-  long ntt_chunk_bytes = 48L << 20;   // per NTT launch pair: stays inside L2
+  long ntt_chunk_bytes = 1L << 30;    // limbs per transform launch pair (bytes); larger chunks
+                                      // mean fewer launch tails (measured: 1 GiB beats an L2-sized chunk)
   double ntt_waves = 1.0;             // transform CTAs per pass, in resident waves
   bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
   int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split

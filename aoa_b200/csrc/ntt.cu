@@ -18,9 +18,10 @@
 // elements of an S = 2^s point sub-transform, does the high-digit stages in
 // registers, exchanges once through (swizzled) shared memory and does the
 // low-digit stages in registers.  Global loads and stores are coalesced in both
-// passes.  Passes run in place; the host launches them over chunks of limbs
-// sized so that the column-pass output is still in L2 when the row pass reads
-// it.
+// passes.  Passes run in place; the host launches them over chunks of whole
+// polys of at most the engine's chunk size (default 1 GiB: the passes are bound
+// by integer arithmetic, so fewer launch tails pay more than keeping the
+// column-pass output in L2 for the row pass).
 #include "aoa_internal.h"
 #include "async.cuh"
 
@@ -918,7 +919,7 @@ __global__ void ntt_small(NttBatch b, bool fwd) {
 // Transform limbs [0, nlimbs) of npolys polys (layout [npolys][poly_stride][N],
 // N = 2^T.log_n) with the tables T; limb l under prime first_prime +
 // (l >> T.prime_shift).  Large transforms are split into chunks of whole polys
-// whose total size stays within the L2 budget, column and row pass per chunk.
+// of at most tune.ntt_chunk_bytes, column and row pass per chunk.
 void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int npolys, int first_prime, int nlimbs,
                       long poly_stride, bool forward, cudaStream_t st, const NttIo* io) {
   if (npolys <= 0 || nlimbs <= 0) return;

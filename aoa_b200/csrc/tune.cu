@@ -52,8 +52,8 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
     if (E.log_n < 10) throw AoaError(AOA_ERR_BAD_PARAM, "autotune: ring too small for the two-pass transform");
     const long N = E.N;
     const int k = E.k;
-    // about 3x the L2 size by default, in whole polys of k limbs
-    const long want = limbs > 0 ? limbs : std::max<long>(k, (384L << 20) / (8 * N));
+    // about 12x the L2 size by default, in whole polys of k limbs
+    const long want = limbs > 0 ? limbs : std::max<long>(k, (1536L << 20) / (8 * N));
     const int npolys = (int)std::max<long>(1, (want + k - 1) / k);
     const long words = (long)npolys * k * N;
     AOA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -87,7 +87,7 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
          [](Tune& t, double v) { t.ntt_rows_div = (int)v; }},
         {"ntt_waves", {1, 2, 0.5, 4}, [](const Tune& t) { return t.ntt_waves; },
          [](Tune& t, double v) { t.ntt_waves = v; }},
-        {"ntt_chunk_bytes", {48.0 * (1 << 20), 24.0 * (1 << 20), 72.0 * (1 << 20), 96.0 * (1 << 20), 120.0 * (1 << 20)},
+        {"ntt_chunk_bytes", {1024.0 * (1 << 20), 120.0 * (1 << 20), 384.0 * (1 << 20), 4096.0 * (1 << 20)},
          [](const Tune& t) { return (double)t.ntt_chunk_bytes; },
          [](Tune& t, double v) { t.ntt_chunk_bytes = (long)v; }},
     };

@@ -92,7 +92,7 @@ int aoa_engine_create(const aoa_params* params, aoa_engine** out);
 int aoa_engine_destroy(aoa_engine* e);
 /* Launch-shape knobs, no reference counterpart (its kernel shapes are
  * compile-time constants): "ntt_chunk_bytes" (bytes of limbs per transform
- * launch pair, default 48 MiB so the column pass output stays in L2),
+ * launch pair, default 1 GiB),
  * "ntt_waves" (transform CTAs per pass in resident waves, default 1),
  * "ntt_split" (log2 C - floor(log2 N / 2) of the R x C transform split,
  * -2..2), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width and
@@ -103,7 +103,7 @@ int aoa_engine_destroy(aoa_engine* e);
  * (0/1: basis conversion on the int8 tensor cores where it applies).      */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
 /* Autotuner: times forward + inverse limb transforms of this engine's ring
- * over `limbs` limbs (0: a default above the L2 size) for candidate splits,
+ * over `limbs` limbs (0: about 1.5 GiB of limbs) for candidate splits,
  * tile shapes, waves and chunk sizes (coordinate descent from the current
  * setting), keeps the fastest and writes a JSON report of the choice and the
  * timings into report[0 .. report_len) (report may be NULL).  Run it before
