@@ -3,8 +3,9 @@
 // passes takes, on how many CTAs share a tile column (waves) and on how many
 // limbs one launch pair covers (the L2 budget of the column -> row handoff).
 // The tuner times forward + inverse transforms of the engine's ring on a
-// device buffer larger than L2 and walks the knobs one at a time (coordinate
-// descent), keeping a change only when it is faster.  No reference
+// device buffer far larger than L2 and on a batch-sized call, and walks the
+// knobs one at a time (coordinate descent), keeping a change only when it is
+// faster.  No reference
 // counterpart: the reference fixes its transform shapes at compile time
 // (aoa-ntt src/cuda/htrans/ntt.cu:35-65).
 #include <cstdio>
@@ -62,19 +63,27 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
     AOA_CUDA(cudaEventCreate(&e1));
     fill_residues<<<4 * E.num_sms, 256, 0, st>>>(buf, N, k, words, E.d_pc);
     AOA_CHECK_LAUNCH();
-    auto time_once = [&]() -> float {
-      ntt_batch(E, buf, npolys, 0, k, k, true, st);
-      ntt_batch(E, buf, npolys, 0, k, k, false, st);
+    // Objective: forward + inverse time per limb on the whole sample plus the
+    // same on a batch-sized call (the polys of 16 ciphertexts, as one stage
+    // of a batched HMult transforms), so that a shape that only pays off on
+    // very large calls does not win.
+    const int small = std::min(npolys, 16);
+    auto time_polys = [&](int np, int reps) -> float {
+      ntt_batch(E, buf, np, 0, k, k, true, st);
+      ntt_batch(E, buf, np, 0, k, k, false, st);
       AOA_CUDA(cudaEventRecord(e0, st));
-      for (int r = 0; r < 3; r++) {
-        ntt_batch(E, buf, npolys, 0, k, k, true, st);
-        ntt_batch(E, buf, npolys, 0, k, k, false, st);
+      for (int r = 0; r < reps; r++) {
+        ntt_batch(E, buf, np, 0, k, k, true, st);
+        ntt_batch(E, buf, np, 0, k, k, false, st);
       }
       AOA_CUDA(cudaEventRecord(e1, st));
       AOA_CUDA(cudaEventSynchronize(e1));
       float ms = 0;
       AOA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      return ms / 3;
+      return ms / reps;
+    };
+    auto time_once = [&]() -> float {
+      return time_polys(npolys, 3) + time_polys(small, 6) * (float)npolys / (float)small;
     };
     std::vector<Knob> knobs = {
         {"ntt_split", {0, -1, 1, -2, 2}, [](const Tune& t) { return (double)t.ntt_split; },
@@ -85,7 +94,7 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
          [](Tune& t, double v) { t.ntt_cols_kind = (int)v; }},
         {"ntt_rows_div", {0, 1, 2}, [](const Tune& t) { return (double)t.ntt_rows_div; },
          [](Tune& t, double v) { t.ntt_rows_div = (int)v; }},
-        {"ntt_waves", {1, 2, 0.5, 4}, [](const Tune& t) { return t.ntt_waves; },
+        {"ntt_waves", {1, 2, 0.5, 4, 8}, [](const Tune& t) { return t.ntt_waves; },
          [](Tune& t, double v) { t.ntt_waves = v; }},
         {"ntt_chunk_bytes", {1024.0 * (1 << 20), 120.0 * (1 << 20), 384.0 * (1 << 20), 4096.0 * (1 << 20)},
          [](const Tune& t) { return (double)t.ntt_chunk_bytes; },

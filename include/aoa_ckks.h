@@ -103,10 +103,12 @@ int aoa_engine_destroy(aoa_engine* e);
  * (0/1: basis conversion on the int8 tensor cores where it applies).      */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
 /* Autotuner: times forward + inverse limb transforms of this engine's ring
- * over `limbs` limbs (0: about 1.5 GiB of limbs) for candidate splits,
- * tile shapes, waves and chunk sizes (coordinate descent from the current
- * setting), keeps the fastest and writes a JSON report of the choice and the
- * timings into report[0 .. report_len) (report may be NULL).  Run it before
+ * over `limbs` limbs (0: about 1.5 GiB of limbs) and over a batch-sized call
+ * (16 polys, scaled to the same limb count; the sum is the objective) for
+ * candidate splits, tile shapes, column-pass kinds, waves and chunk sizes
+ * (coordinate descent from the current setting), keeps the best and writes
+ * a JSON report of the choice and the objective values (ms) into
+ * report[0 .. report_len) (report may be NULL).  Run it before
  * the engine is used from other streams; it synchronises the device.       */
 int aoa_engine_autotune(aoa_engine* e, int limbs, char* report, size_t report_len);
 /* ring degree, prime count, primes (out may be NULL) */
