@@ -74,6 +74,7 @@ struct RnsTables {
   // n = out*16 + d, byte k = in*8 + a holding byte (d - a) of the table entry.
   uint8_t* tc_modup = nullptr;     // [k][131072]
   uint8_t* tc_moddown = nullptr;   // [131072]
+  uint8_t* tc_moddown_binv = nullptr;   // [131072], entries (B/b_j) B^-1 mod q_i (rescale modes)
 };
 
 struct Engine {

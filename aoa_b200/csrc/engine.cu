@@ -169,11 +169,18 @@ static void build_rns_tables(Engine& E) {
             }
         }
     };
-    std::vector<uint8_t> up((size_t)k * kImg, 0), down(kImg, 0);
+    std::vector<uint8_t> up((size_t)k * kImg, 0), down(kImg, 0), down_binv(kImg, 0);
     for (int l = 0; l < k; l++) image(modup_hat.data() + (size_t)l * k * kl, kl, l + 1, kl, up.data() + l * kImg);
     image(moddown_hat.data(), k, kl, k, down.data());
+    // the rescale modes scale the conversion by B^-1 mod q_i: fold it into the table
+    std::vector<uint64_t> hat_binv(moddown_hat.size());
+    for (int j = 0; j < kl; j++)
+      for (int i = 0; i < k; i++)
+        hat_binv[(size_t)j * k + i] = h_mulmod(moddown_hat[(size_t)j * k + i], moddown_binv[i].w, P[i]);
+    image(hat_binv.data(), k, kl, k, down_binv.data());
     E.rns.tc_modup = dev_upload(E, up);
     E.rns.tc_moddown = dev_upload(E, down);
+    E.rns.tc_moddown_binv = dev_upload(E, down_binv);
   }
   E.rns.modup_inv = dev_upload(E, modup_inv);
   E.rns.modup_hat = dev_upload(E, modup_hat);

@@ -333,8 +333,9 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       const int l = j_end - 1;                 // outputs 0..l-1 from c_l (j_first = 0)
       tc_ld32(t_lane + (l & ~1) * 16, v);
       const PrimeConst& Pl = a.pc[a.out_prime0 + l];
+      // the rescale modes read the table with B^-1 folded in: sums are conv * B^-1
       const uint64_t sl = (l & 1) ? tc_combine(v + 16, Pl) : tc_combine(v, Pl);
-      const uint64_t cl = sub_mod(dv, shoup(sl, a.binv[l], Pl.q), Pl.q);
+      const uint64_t cl = sub_mod(dv, sl, Pl.q);
       const int per = (((l + 3) / 4) + 1) & ~1;
       const int jb = par * per, je = min(l, jb + per);
       for (int j = jb; j < je; j += 2) {
@@ -343,8 +344,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
         for (int u = 0; u < 2; u++) {
           if (j + u < je) {
             const PrimeConst& P = a.pc[a.out_prime0 + j + u];
-            out[(long)(j + u - a.out_shift) * N] =
-                add_mod(shoup(tc_combine(v + 16 * u, P), a.binv[j + u], P.q), shoup(cl, 1, P.one_sh, P.q), P.q);
+            out[(long)(j + u - a.out_shift) * N] = add_mod(tc_combine(v + 16 * u, P), shoup(cl, 1, P.one_sh, P.q), P.q);
           }
         }
       }
@@ -364,9 +364,9 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
               const uint64_t x = a.x[poly * a.x_poly_stride + (long)(o - a.x_shift) * N + c];
               r = shoup(sub_mod(x, r, P.q), a.binv[o], P.q);
             } else if (MODE == kRescaleTop) {
-              r = sub_mod(dv, shoup(r, a.binv[o], P.q), P.q);
+              r = sub_mod(dv, r, P.q);                             // folded table: r = conv * B^-1
             } else if (MODE == kRescaleY) {
-              r = add_mod(shoup(r, a.binv[o], P.q), shoup(dv, 1, P.one_sh, P.q), P.q);
+              r = add_mod(r, shoup(dv, 1, P.one_sh, P.q), P.q);    // folded table: r = conv * B^-1
             }
             out[(long)(o - a.out_shift) * N] = r;
           }
@@ -494,6 +494,7 @@ void rescale_corrections(const Engine& E, const uint64_t* in_b, long in_stride, 
                          long u_stride, uint64_t* cl_tmp, long cl_stride, uint64_t* y, long y_stride, int npolys,
                          int level, cudaStream_t st) {
   ConvArgs a = moddown_args(E, in_b, in_stride, y, y_stride);
+  a.tc_b = E.rns.tc_moddown_binv;                // the tensor-core kernel's rescale modes fold B^-1 in
   if (level < kConvOut) {
     a.mode = kRescaleFused;
     a.d = u_l; a.d_poly_stride = u_stride;
@@ -501,6 +502,7 @@ void rescale_corrections(const Engine& E, const uint64_t* in_b, long in_stride, 
     return;
   }
   ConvArgs t = moddown_args(E, in_b, in_stride, cl_tmp, cl_stride);
+  t.tc_b = E.rns.tc_moddown_binv;
   t.mode = kRescaleTop;
   t.d = u_l; t.d_poly_stride = u_stride;
   t.out_shift = level;
