@@ -30,8 +30,8 @@ namespace aoa {
 template <int LOG_S>
 struct Sub {
   static constexpr int S = 1 << LOG_S;
-  static constexpr int HI = (LOG_S + 1) / 2;   // high digit width (round 1)
-  static constexpr int LO = LOG_S / 2;         // low digit width (round 2)
+  static constexpr int HI = (LOG_S + 1) / 2;   // high digit width (first exchange half)
+  static constexpr int LO = LOG_S / 2;         // low digit width (second exchange half)
   static constexpr int T = 1 << LO;            // threads per sub-transform
   static constexpr int E = 1 << HI;            // elements per thread
   static constexpr int G = 1 << (HI - LO);     // low-digit groups per thread (1 or 2)
