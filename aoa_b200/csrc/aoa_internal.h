@@ -33,11 +33,13 @@ struct AoaError : public std::runtime_error {
   } while (0)
 
 constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration limit
+constexpr int kLargeItems = 1536;           // limb-transform launches this large use ntt_waves_large
 
 struct Tune {
   long ntt_chunk_bytes = 1L << 30;    // limbs per transform launch pair (bytes); larger chunks
                                       // mean fewer launch tails (measured: 1 GiB beats an L2-sized chunk)
   double ntt_waves = 1.0;             // transform CTAs per pass, in resident waves
+  double ntt_waves_large = 1.0;       // the same for launches of at least kLargeItems limbs
   bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
   int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split
   int ntt_cols_div = 0;               // column-pass tile width: widest >> div (0..2)

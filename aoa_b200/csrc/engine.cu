@@ -291,6 +291,7 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   const std::string k(knob);
   if (k == "ntt_chunk_bytes" && value >= (1 << 20) && value <= 6.4e10) h->e.tune.ntt_chunk_bytes = (long)value;
   else if (k == "ntt_waves" && value > 0 && value <= 64) h->e.tune.ntt_waves = value;
+  else if (k == "ntt_waves_large" && value > 0 && value <= 64) h->e.tune.ntt_waves_large = value;
   else if (k == "conv_tensor_cores" && (value == 0 || value == 1)) h->e.tune.conv_tensor_cores = value != 0;
   else if (k == "ntt_split" && value >= -2 && value <= 2 && value == (int)value) h->e.tune.ntt_split = (int)value;
   else if (k == "ntt_cols_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_cols_div = (int)value;

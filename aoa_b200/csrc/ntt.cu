@@ -744,7 +744,10 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
 
 // CTAs per tile column: about one resident wave of CTAs (blocks_per_sm per SM)
 static int ctas_per_tile(const Engine& E, int tiles, int items, int blocks_per_sm) {
-  const int target = std::max(1, (int)(E.tune.ntt_waves * E.num_sms * blocks_per_sm) / std::max(1, tiles));
+  // large launches balance better with more, shorter-lived CTAs (the hardware
+  // hands later waves to the SMs that finish first); small ones pay per CTA
+  const double waves = items >= kLargeItems ? E.tune.ntt_waves_large : E.tune.ntt_waves;
+  const int target = std::max(1, (int)(waves * E.num_sms * blocks_per_sm) / std::max(1, tiles));
   return std::max(1, std::min(items, target));
 }
 

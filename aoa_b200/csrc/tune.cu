@@ -96,6 +96,8 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
          [](Tune& t, double v) { t.ntt_rows_div = (int)v; }},
         {"ntt_waves", {1, 2, 0.5, 4, 8}, [](const Tune& t) { return t.ntt_waves; },
          [](Tune& t, double v) { t.ntt_waves = v; }},
+        {"ntt_waves_large", {1, 2, 4, 8, 16}, [](const Tune& t) { return t.ntt_waves_large; },
+         [](Tune& t, double v) { t.ntt_waves_large = v; }},
         {"ntt_chunk_bytes", {1024.0 * (1 << 20), 120.0 * (1 << 20), 384.0 * (1 << 20), 4096.0 * (1 << 20)},
          [](const Tune& t) { return (double)t.ntt_chunk_bytes; },
          [](Tune& t, double v) { t.ntt_chunk_bytes = (long)v; }},
@@ -128,9 +130,9 @@ extern "C" int aoa_engine_autotune(aoa_engine* h, int limbs, char* report, size_
       for (const Knob& kn : knobs) descend(kn);
     snprintf(line, sizeof line,
              "], \"best_ms\": %.4f, \"choice\": {\"ntt_split\": %d, \"ntt_cols_div\": %d, \"ntt_cols_kind\": %d, "
-             "\"ntt_rows_div\": %d, \"ntt_waves\": %g, \"ntt_chunk_bytes\": %ld}}",
+             "\"ntt_rows_div\": %d, \"ntt_waves\": %g, \"ntt_waves_large\": %g, \"ntt_chunk_bytes\": %ld}}",
              best, E.tune.ntt_split, E.tune.ntt_cols_div, E.tune.ntt_cols_kind, E.tune.ntt_rows_div, E.tune.ntt_waves,
-             E.tune.ntt_chunk_bytes);
+             E.tune.ntt_waves_large, E.tune.ntt_chunk_bytes);
     rep += line;
   });
   if (st_ != AOA_OK) E.tune = saved;

@@ -94,6 +94,7 @@ int aoa_engine_destroy(aoa_engine* e);
  * compile-time constants): "ntt_chunk_bytes" (bytes of limbs per transform
  * launch pair, default 1 GiB),
  * "ntt_waves" (transform CTAs per pass in resident waves, default 1),
+ * "ntt_waves_large" (the same for launches of at least 1536 limbs),
  * "ntt_split" (log2 C - floor(log2 N / 2) of the R x C transform split,
  * -2..2), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width and
  * row-pass tile height = widest >> div, 0..2), "ntt_cols_kind" (0 CTA-wide
