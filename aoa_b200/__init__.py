@@ -45,8 +45,9 @@ class Engine:
         self.handle = h
 
     def tune(self, knob, value):
-        """Set a launch-shape knob ("ntt_chunk_bytes", "ntt_waves", "ntt_split",
-        "ntt_cols_div", "ntt_rows_div", "conv_tensor_cores")."""
+        """Set a launch-shape knob ("ntt_split", "ntt_cols_div", "ntt_cols_kind",
+        "ntt_rows_div", "ntt_waves", "ntt_waves_large", "ntt_chunk_bytes",
+        "conv_tensor_cores", "fuse", "batch_streams")."""
         capi.check(capi.load().aoa_engine_tune(self.handle, knob.encode(), float(value)))
 
     def autotune(self, limbs=0):

@@ -75,6 +75,13 @@ static void build_prime_tables(Engine& E) {
     c.ninv_sh = h_shoup_companion(c.ninv, q);
     c.ninv_w1 = h_mulmod(c.ninv, itw[(size_t)p * N + 1].w, q);
     c.ninv_w1_sh = h_shoup_companion(c.ninv_w1, q);
+    c.bar_sh = 0;
+    c.bar_mu = 0;
+    if (q >= 4 && q < (1ull << 62)) {
+      const int n = 64 - __builtin_clzll(q);
+      c.bar_sh = (uint64_t)(n - 2);
+      c.bar_mu = (uint64_t)((one128 << (64 + n - 2)) / q);
+    }
     E.h_pc[p] = c;
   }
   if (bad) throw AoaError(AOA_ERR_BAD_PARAM, "every prime must be prime, < 2^63 and = 1 mod 2N");

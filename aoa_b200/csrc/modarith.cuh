@@ -6,7 +6,8 @@
 // cheapest exact form per use:
 //   * Shoup multiplication by a precomputed constant w with w' = floor(w 2^64/q)
 //     (twiddles, CRT constants): one mul.hi and two mul.lo;
-//   * Montgomery REDC for products of two variable residues;
+//   * Barrett multiplication with a 64-bit quotient estimate for products of
+//     two variable residues (q < 2^62), Montgomery REDC above that;
 //   * two Shoup steps to fold a 128-bit accumulator (basis conversion sums).
 // All routines require q < 2^63 and return canonical values in [0, q)
 // unless named *_lazy.
@@ -25,6 +26,8 @@ struct PrimeConst {
   uint64_t one_sh;     // floor(2^64 / q)       (Shoup companion of 1)
   uint64_t ninv, ninv_sh;          // N^-1 mod q
   uint64_t ninv_w1, ninv_w1_sh;    // N^-1 * psi^-bitrev(1) mod q (last inverse stage)
+  uint64_t bar_mu;     // floor(2^(64+s) / q), s = bar_sh       (Barrett, q < 2^62)
+  uint64_t bar_sh;     // bit length of q minus 2; 0 when q >= 2^62 (Montgomery instead)
 };
 
 struct ShoupW {      // twiddle or constant w with its Shoup companion
@@ -70,8 +73,23 @@ AOA_HD uint64_t redc(uint64_t lo, uint64_t hi, uint64_t q, uint64_t qinv_neg) {
   return t >= q ? t - q : t;
 }
 
-// a * b mod q for a, b < q (two REDC steps through R^2).
+// a * b mod q for a, b < 2^n, q < 2^62 of bit length n, by Barrett's method
+// with a 64-bit quotient estimate: with s = n - 2, x = a b < 2^2n,
+// x1 = floor(x / 2^s) < 2^64 and mu = floor(2^(64+s) / q) < 2^63, the
+// estimate qh = floor(x1 mu / 2^64) satisfies x/q - 2.5 < qh <= x/q (the
+// truncations of x1 and mu cost < 2^(n-62) + 2^s/q <= 1.5, the final floor
+// < 1), so r = x - qh q lies in [0, 3q) and is exact in 64 bits.
+AOA_HD uint64_t barrett_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t mu, uint32_t s) {
+  const uint64_t lo = a * b, hi = mulhi64(a, b);
+  const uint64_t x1 = (hi << (64 - s)) | (lo >> s);
+  uint64_t r = lo - mulhi64(x1, mu) * q;
+  r = r >= q ? r - q : r;
+  return r >= q ? r - q : r;
+}
+
+// a * b mod q for a, b < q: Barrett for q < 2^62, else two REDC steps through R^2.
 AOA_HD uint64_t mul_mod(uint64_t a, uint64_t b, const PrimeConst& P) {
+  if (P.bar_sh) return barrett_mul(a, b, P.q, P.bar_mu, (uint32_t)P.bar_sh);
   uint64_t lo = a * b, hi = mulhi64(a, b);
   uint64_t t = redc(lo, hi, P.q, P.qinv_neg);          // a b R^-1
   return redc(t * P.r2, mulhi64(t, P.r2), P.q, P.qinv_neg);   // a b

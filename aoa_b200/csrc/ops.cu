@@ -63,20 +63,37 @@ __global__ void ew_muladd(Limbs d, CLimbs a, CLimbs b, CLimbs c, int prime0, con
 // HMult tensor (ckks_mul_without_rescale, ckks.cpp:300-307), transform domain:
 //   d0 = a0 b0,  d1 = a0 b1 + a1 b0,  d2 = a1 b1
 // (the reference forms d1 as (a0+a1)(b0+b1) - d0 - d2: the same residues).
+__device__ __forceinline__ void tensor3(uint64_t x0, uint64_t x1, uint64_t y0, uint64_t y1, const PrimeConst& P,
+                                        uint64_t& d0, uint64_t& d1, uint64_t& d2) {
+  const uint64_t q = P.q;
+  if (P.bar_sh) {
+    const uint64_t mu = P.bar_mu;
+    const uint32_t s = (uint32_t)P.bar_sh;
+    d0 = barrett_mul(x0, y0, q, mu, s);
+    d1 = add_mod(barrett_mul(x0, y1, q, mu, s), barrett_mul(x1, y0, q, mu, s), q);
+    d2 = barrett_mul(x1, y1, q, mu, s);
+    return;
+  }
+  // q >= 2^62: Montgomery products carry a 2^-64 factor; one more REDC by R^2 clears it.
+  const uint64_t qi = P.qinv_neg;
+  const uint64_t m0 = mont_mul(x0, y0, q, qi);
+  const uint64_t m1 = add_mod(mont_mul(x0, y1, q, qi), mont_mul(x1, y0, q, qi), q);
+  const uint64_t m2 = mont_mul(x1, y1, q, qi);
+  d0 = mont_mul(m0, P.r2, q, qi);
+  d1 = mont_mul(m1, P.r2, q, qi);
+  d2 = mont_mul(m2, P.r2, q, qi);
+}
+
 __global__ void hmult_tensor(const uint64_t* a, const uint64_t* b, long a_half, long b_half, uint64_t* d0,
                              uint64_t* d1, uint64_t* d2, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
   const long off = (long)blockIdx.y * N + coef_index();
   const PrimeConst& P = pc[blockIdx.y];
-  const uint64_t x0 = a[off], x1 = a[a_half + off], y0 = b[off], y1 = b[b_half + off];
-  const uint64_t q = P.q, qi = P.qinv_neg;
-  // Montgomery products carry a 2^-64 factor; one more REDC by R^2 clears it.
-  uint64_t m0 = mont_mul(x0, y0, q, qi);
-  uint64_t m1 = add_mod(mont_mul(x0, y1, q, qi), mont_mul(x1, y0, q, qi), q);
-  uint64_t m2 = mont_mul(x1, y1, q, qi);
-  d0[off] = mont_mul(m0, P.r2, q, qi);
-  d1[off] = mont_mul(m1, P.r2, q, qi);
-  d2[off] = mont_mul(m2, P.r2, q, qi);
+  uint64_t r0, r1, r2;
+  tensor3(a[off], a[a_half + off], b[off], b[b_half + off], P, r0, r1, r2);
+  d0[off] = r0;
+  d1[off] = r1;
+  d2[off] = r2;
 }
 
 // Key-switch products over the QB limbs of the extended d2 (transform domain):
@@ -148,33 +165,38 @@ __global__ void hmult_tensor_batch(CtPtrs ptr, long half, uint64_t* D, int n, co
   const PrimeConst& P = pc[blockIdx.y];
   const uint64_t* a = ptr.a[z];
   const uint64_t* b = ptr.b[z];
-  const uint64_t x0 = a[off], x1 = a[half + off], y0 = b[off], y1 = b[half + off];
-  const uint64_t q = P.q, qi = P.qinv_neg;
-  uint64_t m0 = mont_mul(x0, y0, q, qi);
-  uint64_t m1 = add_mod(mont_mul(x0, y1, q, qi), mont_mul(x1, y0, q, qi), q);
-  uint64_t m2 = mont_mul(x1, y1, q, qi);
+  uint64_t r0, r1, r2;
+  tensor3(a[off], a[half + off], b[off], b[half + off], P, r0, r1, r2);
   const long nh = (long)n * half;
   uint64_t* d = D + (long)z * half + off;
-  d[0] = mont_mul(m0, P.r2, q, qi);
-  d[nh] = mont_mul(m1, P.r2, q, qi);
-  d[2 * nh] = mont_mul(m2, P.r2, q, qi);
+  d[0] = r0;
+  d[nh] = r1;
+  d[2 * nh] = r2;
 }
 
 // key products for op z: x limbs (Q part at xq + z*xq_stride, B part at
 // xb + z*xb_stride) times the key; k0 of op z at k + z*k_stride, k1 at
 // k + (n + z)*k_stride.
+// One thread per (limb, coefficient) loops over the n ops, so that each key
+// word is read from memory once per launch.
 __global__ void keyswitch_mul_batch(const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
                                     const uint64_t* key, long key_half, uint64_t* k, long k_stride, int n, int nq,
                                     int K, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
   const long c = coef_index();
-  const int l = blockIdx.y, z = blockIdx.z;
+  const int l = blockIdx.y;
   const int prime = l < nq ? l : K + (l - nq);
-  const uint64_t x = l < nq ? xq[z * xq_stride + (long)l * N + c] : xb[z * xb_stride + (long)(l - nq) * N + c];
-  const PrimeConst& P = pc[prime];
+  const uint64_t* x = l < nq ? xq + (long)l * N + c : xb + (long)(l - nq) * N + c;
+  const long xs = l < nq ? xq_stride : xb_stride;
+  const PrimeConst P = pc[prime];
   const uint64_t kb = key[(long)prime * N + c], ka = key[key_half + (long)prime * N + c];
-  k[z * k_stride + (long)l * N + c] = mul_mod(x, kb, P);
-  k[(n + z) * k_stride + (long)l * N + c] = mul_mod(x, ka, P);
+  uint64_t* o = k + (long)l * N + c;
+#pragma unroll 4
+  for (int z = 0; z < n; z++) {
+    const uint64_t v = x[z * xs];
+    o[z * k_stride] = mul_mod(v, kb, P);
+    o[(n + z) * k_stride] = mul_mod(v, ka, P);
+  }
 }
 
 // ---- host wrappers -----------------------------------------------------------
@@ -221,7 +243,7 @@ void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride,
                             const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st, int nb) {
   const long half = (long)E.nprimes * E.N;
   if (nb < 0) nb = E.kl;
-  keyswitch_mul_batch<<<ew_grid(E, nq + nb, n), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
+  keyswitch_mul_batch<<<ew_grid(E, nq + nb, 1), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
                                                                n, nq, E.k, E.d_pc, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
