@@ -164,27 +164,37 @@ static void build_rns_tables(Engine& E) {
   for (int l = 1; l < k; l++)
     for (int i = 0; i < l; i++) resc[(size_t)l * k + i] = sh(h_invmod(P[l] % P[i], P[i]), P[i]);
   if (k <= 32 && kl >= 1 && kl <= 32 && E.N % 128 == 0) {
-    constexpr size_t kImg = 131072;
-    auto image = [](const uint64_t* mat, int ld, int nin, int nout, uint8_t* img) {
-      for (int in = 0; in < nin; in++)
-        for (int out = 0; out < nout; out++) {
-          const uint64_t h = mat[(size_t)in * ld + out];
-          for (int a = 0; a < 8; a++)
+    // [16 k-chunks][256 columns][16 B]: byte k = 8 in + a of column n = 8 out + b
+    // holds byte b of h 2^(8a) mod p_out (the conversion kernel's B operand)
+    constexpr size_t kImg = 65536;
+    auto image = [](const uint64_t* mat, int ld, int nin, int nout, const uint64_t* outp, uint8_t* img) {
+      for (int out = 0; out < nout; out++) {
+        const uint64_t p = outp[out];
+        uint64_t sh[8];
+        sh[0] = 1 % p;
+        for (int a = 1; a < 8; a++) sh[a] = h_mulmod(sh[a - 1], 256 % p, p);
+        for (int in = 0; in < nin; in++) {
+          const uint64_t h = mat[(size_t)in * ld + out] % p;
+          for (int a = 0; a < 8; a++) {
+            const uint64_t g = h_mulmod(h, sh[a], p);
             for (int b = 0; b < 8; b++) {
-              const int kb = in * 8 + a, n = out * 16 + a + b;
-              img[((size_t)(kb / 16) * 512 + n) * 16 + kb % 16] = (uint8_t)(h >> (8 * b));
+              const int kb = in * 8 + a, n = out * 8 + b;
+              img[((size_t)(kb / 16) * 256 + n) * 16 + kb % 16] = (uint8_t)(g >> (8 * b));
             }
+          }
         }
+      }
     };
     std::vector<uint8_t> up((size_t)k * kImg, 0), down(kImg, 0), down_binv(kImg, 0);
-    for (int l = 0; l < k; l++) image(modup_hat.data() + (size_t)l * k * kl, kl, l + 1, kl, up.data() + l * kImg);
-    image(moddown_hat.data(), k, kl, k, down.data());
+    for (int l = 0; l < k; l++)
+      image(modup_hat.data() + (size_t)l * k * kl, kl, l + 1, kl, P.data() + k, up.data() + l * kImg);
+    image(moddown_hat.data(), k, kl, k, P.data(), down.data());
     // the rescale modes scale the conversion by B^-1 mod q_i: fold it into the table
     std::vector<uint64_t> hat_binv(moddown_hat.size());
     for (int j = 0; j < kl; j++)
       for (int i = 0; i < k; i++)
         hat_binv[(size_t)j * k + i] = h_mulmod(moddown_hat[(size_t)j * k + i], moddown_binv[i].w, P[i]);
-    image(hat_binv.data(), k, kl, k, down_binv.data());
+    image(hat_binv.data(), k, kl, k, P.data(), down_binv.data());
     E.rns.tc_modup = dev_upload(E, up);
     E.rns.tc_moddown = dev_upload(E, down);
     E.rns.tc_moddown_binv = dev_upload(E, down_binv);

@@ -73,18 +73,22 @@ AOA_HD uint64_t redc(uint64_t lo, uint64_t hi, uint64_t q, uint64_t qinv_neg) {
   return t >= q ? t - q : t;
 }
 
-// a * b mod q for a, b < 2^n, q < 2^62 of bit length n, by Barrett's method
-// with a 64-bit quotient estimate: with s = n - 2, x = a b < 2^2n,
-// x1 = floor(x / 2^s) < 2^64 and mu = floor(2^(64+s) / q) < 2^63, the
-// estimate qh = floor(x1 mu / 2^64) satisfies x/q - 2.5 < qh <= x/q (the
-// truncations of x1 and mu cost < 2^(n-62) + 2^s/q <= 1.5, the final floor
-// < 1), so r = x - qh q lies in [0, 3q) and is exact in 64 bits.
-AOA_HD uint64_t barrett_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t mu, uint32_t s) {
-  const uint64_t lo = a * b, hi = mulhi64(a, b);
+// x = hi 2^64 + lo mod q for x < 2^(64+s), q < 2^62 of bit length n, s = n - 2,
+// by Barrett's method with a 64-bit quotient estimate: x1 = floor(x / 2^s)
+// < 2^64 and mu = floor(2^(64+s) / q) < 2^63; the estimate
+// qh = floor(x1 mu / 2^64) satisfies x/q - 2.5 < qh <= x/q (the truncations
+// of x1 and mu cost < x / 2^(64+s) + 2^s/q <= 1.5, the final floor < 1), so
+// r = x - qh q lies in [0, 3q) and is exact in 64 bits.
+AOA_HD uint64_t barrett_wide(uint64_t lo, uint64_t hi, uint64_t q, uint64_t mu, uint32_t s) {
   const uint64_t x1 = (hi << (64 - s)) | (lo >> s);
   uint64_t r = lo - mulhi64(x1, mu) * q;
   r = r >= q ? r - q : r;
   return r >= q ? r - q : r;
+}
+
+// a * b mod q for a, b < 2^n (then a b < 2^2n <= 2^(64+s) for n <= 62).
+AOA_HD uint64_t barrett_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t mu, uint32_t s) {
+  return barrett_wide(a * b, mulhi64(a, b), q, mu, s);
 }
 
 // a * b mod q for a, b < q: Barrett for q < 2^62, else two REDC steps through R^2.

@@ -142,26 +142,30 @@ basis_convert(ConvArgs a, int j_first, int j_end) {
 
 // ---- tensor-core variant ------------------------------------------------------------
 // The conversion as one int8 GEMM per 128-coefficient tile on the 5th-generation
-// tensor cores.  With the scaled inputs z_i split into their 8 bytes z_i[a]
-// and the table entries h_ij into bytes h_ij[b], the sum over i of z_i h_ij
-// is sum_d 2^(8d) S_jd with the diagonal sums S_jd = sum_i sum_(a+b=d)
-// z_i[a] h_ij[b] < 2^24 (at most 32 inputs).  That is C = A B with
-//   A[row][8i + a] = z_i[a]           (the bytes of z_i: just z_i stored as u64)
-//   B[8i + a][16j + d] = h_ij[d - a]  (0 outside 0 <= d - a < 8; precomputed image)
+// tensor cores.  With the scaled inputs z_i split into their 8 bytes z_i[a],
+// sum_i z_i h_ij = sum_i sum_a z_i[a] (h_ij 2^(8a)), and modulo the output
+// prime p_j the factor h_ij 2^(8a) can be replaced by its residue
+// g_ija = h_ij 2^(8a) mod p_j.  Splitting g_ija into bytes g_ija[b]:
+//   sum_i z_i h_ij = sum_b 2^(8b) T_jb  (mod p_j),
+//   T_jb = sum_i sum_a z_i[a] g_ija[b] < 8 * 32 * 255^2 < 2^24  (at most 32 inputs).
+// That is C = A B with
+//   A[row][8i + a] = z_i[a]            (the bytes of z_i: just z_i stored as u64)
+//   B[8i + a][8j + b] = g_ija[b]       (a precomputed image per table)
 // so one tcgen05.mma kind::i8 (M = 128, N = 256, K = 32 per instruction,
-// u8 x u8 -> s32 in tensor memory) computes 16 diagonal sums per output, for
-// two N halves and 8 K steps.  The epilogue reads each thread's 16 columns of
-// an output from tensor memory (tcgen05.ld), combines them into the exact
-// 128-bit sum and reduces it once, as the CUDA-core kernel does.
+// u8 x u8 -> s32 in tensor memory) computes the 8 byte sums of all 32
+// outputs per K step (4 inputs).  The epilogue reads each thread's 8 columns
+// of an output from tensor memory (tcgen05.ld), forms sum_b 2^(8b) T_jb <
+// 2^81 and reduces it once.
 // Shared memory (no swizzle, K-major "core matrices" of 8 rows x 16 bytes):
 //   A: [16 k-chunks][128 rows][16 B]   = 32 KiB, descriptor LBO 2048, SBO 128
-//   B: [16 k-chunks][512 rows][16 B]   = 128 KiB, descriptor LBO 8192, SBO 128
+//   B: [16 k-chunks][256 rows][16 B]   = 64 KiB, descriptor LBO 4096, SBO 128
 constexpr int kTcRows = 128;
 constexpr int kTcThreads = 512;
+constexpr int kTcN = 256;
 constexpr size_t kTcA = 16 * kTcRows * 16;
-constexpr size_t kTcB = 131072;
+constexpr size_t kTcB = 16 * kTcN * 16;
 constexpr size_t kTcSmem = kTcA + kTcB + 1024;
-constexpr uint32_t kTcCols = 512;
+constexpr uint32_t kTcCols = 256;
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
@@ -186,42 +190,36 @@ __device__ __forceinline__ void tc_commit(uint64_t* mb) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// The exact sum of one output, sum_d S_d 2^(8d) (d < 15, S_d < 2^24), reduced
-// mod P.  Groups of four diagonals W_m = sum_t S_(4m+t) 2^(8t) < 2^51 are
-// formed with 32 x 32 -> 64-bit multiply-adds, then added at 32-bit offsets
-// 32m into the 128-bit total (below 2^126, so W_3 < 2^30 fits word 3).
+// sum_b T_b 2^(8b) (b < 8, T_b < 2^24) reduced mod P.  W_0 = sum_t T_t 2^(8t)
+// and W_1 = sum_t T_(4+t) 2^(8t) (< 2^49 each) come from 32 x 32 -> 64-bit
+// multiply-adds; x = W_0 + W_1 2^32 < 2^81 has a high word below 2^17, so
+// one Barrett step reduces it when s = bit length - 2 >= 17.
 __device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const PrimeConst& P) {
-  uint64_t W[4];
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    uint64_t w = v[4 * m];
-    asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(w) : "r"(v[4 * m + 1]));
-    asm("mad.wide.u32 %0, %1, 65536, %0;" : "+l"(w) : "r"(v[4 * m + 2]));
-    if (m < 3) asm("mad.wide.u32 %0, %1, 16777216, %0;" : "+l"(w) : "r"(v[4 * m + 3]));
-    W[m] = w;
-  }
-  uint32_t r1, r2, r3;
-  asm("add.cc.u32 %0, %3, %4;\n\t"
-      "addc.cc.u32 %1, %5, %6;\n\t"
-      "addc.u32 %2, %7, %8;"
-      : "=r"(r1), "=r"(r2), "=r"(r3)
-      : "r"((uint32_t)(W[0] >> 32)), "r"((uint32_t)W[1]), "r"((uint32_t)(W[1] >> 32)), "r"((uint32_t)W[2]),
-        "r"((uint32_t)(W[2] >> 32)), "r"((uint32_t)W[3]));
-  const uint64_t lo = ((uint64_t)r1 << 32) | (uint32_t)W[0];
-  const uint64_t hi = ((uint64_t)r3 << 32) | r2;
-  return reduce128(lo, hi, P);
+  uint64_t W0 = v[0], W1 = v[4];
+  asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(W0) : "r"(v[1]));
+  asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(W1) : "r"(v[5]));
+  asm("mad.wide.u32 %0, %1, 65536, %0;" : "+l"(W0) : "r"(v[2]));
+  asm("mad.wide.u32 %0, %1, 65536, %0;" : "+l"(W1) : "r"(v[6]));
+  asm("mad.wide.u32 %0, %1, 16777216, %0;" : "+l"(W0) : "r"(v[3]));
+  asm("mad.wide.u32 %0, %1, 16777216, %0;" : "+l"(W1) : "r"(v[7]));
+  uint32_t r1, r2;
+  asm("add.cc.u32 %0, %2, %3;\n\t"
+      "addc.u32 %1, %4, 0;"
+      : "=r"(r1), "=r"(r2)
+      : "r"((uint32_t)(W0 >> 32)), "r"((uint32_t)W1), "r"((uint32_t)(W1 >> 32)));
+  const uint64_t lo = ((uint64_t)r1 << 32) | (uint32_t)W0;
+  if (P.bar_sh >= 17) return barrett_wide(lo, r2, P.q, P.bar_mu, (uint32_t)P.bar_sh);
+  return reduce128(lo, r2, P);
 }
 
 // Persistent: CTA b handles tiles b, b + grid, ...  Per tile: the inputs (loaded
@@ -263,7 +261,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   const uint32_t tmem = tmem_slot;
   if (threadIdx.x == 0) {
     mbar_expect_tx(&mbar[0], (unsigned)kTcB);
-    for (int c = 0; c < 8; c++) bulk_g2s(smem_u32(Bs + c * 16384), a.tc_b + c * 16384, 16384, &mbar[0]);
+    for (int c = 0; c < (int)(kTcB / 16384); c++)
+      bulk_g2s(smem_u32(Bs + c * 16384), a.tc_b + c * 16384, 16384, &mbar[0]);
   }
   // this thread's A rows / input pairs, and its prefetched inputs
   const int ar = threadIdx.x % kTcRows, ap = threadIdx.x / kTcRows;
@@ -305,11 +304,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       tc_fence_after();
       for (int st = 0; st < ksteps; st++) {
         const uint64_t ad = umma_desc(a_base + st * 2 * (kTcRows * 16), kTcRows * 16, 128);
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const uint64_t bd = umma_desc(b_base + st * 2 * (512 * 16) + h * 256 * 16, 512 * 16, 128);
-          tc_mma(tmem + h * 256, ad, bd, st > 0);
-        }
+        const uint64_t bd = umma_desc(b_base + st * 2 * (kTcN * 16), kTcN * 16, 128);
+        tc_mma(tmem, ad, bd, st > 0);
       }
       tc_commit(&mbar[1]);
     }
@@ -328,23 +324,23 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     uint64_t* out = a.out + poly * a.out_poly_stride + c;
     uint64_t dv = 0;
     if (MODE >= kRescaleTop) dv = a.d[poly * a.d_poly_stride + c];
-    uint32_t v[32];
+    uint32_t v[16];
     if (MODE == kRescaleFused) {
       const int l = j_end - 1;                 // outputs 0..l-1 from c_l (j_first = 0)
-      tc_ld32(t_lane + (l & ~1) * 16, v);
+      tc_ld16(t_lane + (l & ~1) * 8, v);
       const PrimeConst& Pl = a.pc[a.out_prime0 + l];
       // the rescale modes read the table with B^-1 folded in: sums are conv * B^-1
-      const uint64_t sl = (l & 1) ? tc_combine(v + 16, Pl) : tc_combine(v, Pl);
+      const uint64_t sl = (l & 1) ? tc_combine(v + 8, Pl) : tc_combine(v, Pl);
       const uint64_t cl = sub_mod(dv, sl, Pl.q);
       const int per = (((l + 3) / 4) + 1) & ~1;
       const int jb = par * per, je = min(l, jb + per);
       for (int j = jb; j < je; j += 2) {
-        tc_ld32(t_lane + j * 16, v);
+        tc_ld16(t_lane + j * 8, v);
 #pragma unroll
         for (int u = 0; u < 2; u++) {
           if (j + u < je) {
             const PrimeConst& P = a.pc[a.out_prime0 + j + u];
-            out[(long)(j + u - a.out_shift) * N] = add_mod(tc_combine(v + 16 * u, P), shoup(cl, 1, P.one_sh, P.q), P.q);
+            out[(long)(j + u - a.out_shift) * N] = add_mod(tc_combine(v + 8 * u, P), shoup(cl, 1, P.one_sh, P.q), P.q);
           }
         }
       }
@@ -353,13 +349,13 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       const int per = (((nout + 3) / 4) + 1) & ~1;
       const int jb = j_first + par * per, je = min(j_end, jb + per);
       for (int jj = jb & ~1; jj < je; jj += 2) {
-        tc_ld32(t_lane + jj * 16, v);
+        tc_ld16(t_lane + jj * 8, v);
 #pragma unroll
         for (int u = 0; u < 2; u++) {
           const int o = jj + u;
           if (o >= jb && o < je) {
             const PrimeConst& P = a.pc[a.out_prime0 + o];
-            uint64_t r = tc_combine(v + 16 * u, P);
+            uint64_t r = tc_combine(v + 8 * u, P);
             if (MODE == kModDown) {
               const uint64_t x = a.x[poly * a.x_poly_stride + (long)(o - a.x_shift) * N + c];
               r = shoup(sub_mod(x, r, P.q), a.binv[o], P.q);
@@ -450,7 +446,7 @@ void modup(const Engine& E, const uint64_t* in, long in_stride, uint64_t* out_b,
   a.in_prime0 = 0; a.out_prime0 = E.k;
   a.zc = E.rns.modup_inv + (long)level * E.k;
   a.mat = E.rns.modup_hat + (long)level * E.k * E.kl;
-  a.tc_b = E.rns.tc_modup ? E.rns.tc_modup + (size_t)level * 131072 : nullptr;
+  a.tc_b = E.rns.tc_modup ? E.rns.tc_modup + (size_t)level * kTcB : nullptr;
   a.pc = E.d_pc; a.log_n = E.log_n; a.mode = kRaw;
   run_convert(E, a, npolys, 0, E.kl, st);
 }
