@@ -85,7 +85,7 @@ struct Engine {
   long N = 0;
   int k = 0, kl = 0, nprimes = 0;
   int scale_bits = 0;
-  bool lazy = false;          // every prime < 2^62: Harvey lazy butterflies
+  bool lazy = false;          // every prime < 2^61: Harvey lazy butterflies
   std::vector<uint64_t> primes, gens;
   std::vector<PrimeConst> h_pc;
   PrimeConst* d_pc = nullptr;

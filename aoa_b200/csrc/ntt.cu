@@ -43,15 +43,19 @@ struct Sub {
 
 // ---- butterflies ------------------------------------------------------------
 // Strict mode keeps every value canonical in [0, q) (any q < 2^63).  Lazy mode
-// (all primes < 2^62) follows Harvey's bounds: forward values live in [0, 4q),
-// inverse values in [0, 2q); the last stage of each transform reduces to [0, q).
+// (all primes < 2^61) follows Harvey's bounds with the forward reduction
+// taken every second stage: a reducing stage (even stage index within its
+// pass) maps inputs in [0, 8q) to [0, 6q) (U = x - 4q when x >= 4q), the
+// stage after it maps [0, 6q) to [0, 8q) without reducing, so 8q < 2^64 holds
+// throughout; inverse values live in [0, 2q).  The last stage of each
+// transform reduces to [0, q).
 
 template <bool LAZY>
 struct Bf;
 
 template <>
 struct Bf<false> {
-  static __device__ __forceinline__ void ct(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q) {
+  static __device__ __forceinline__ void ct(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q, bool) {
     uint64_t U = x, V = shoup(y, w, q);
     x = add_mod(U, V, q);
     y = sub_mod(U, V, q);
@@ -72,12 +76,14 @@ struct Bf<false> {
 
 template <>
 struct Bf<true> {
-  static __device__ __forceinline__ void ct(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q) {
-    const uint64_t q2 = q << 1;
-    uint64_t U = x >= q2 ? x - q2 : x;          // [0, 2q)
+  // red (a compile-time constant after unrolling): reducing stage
+  static __device__ __forceinline__ void ct(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q, bool red) {
+    const uint64_t q2 = q << 1, q4 = q << 2;
+    uint64_t U = x;                             // [0, 8q) if red, else [0, 6q)
+    if (red) U = U >= q4 ? U - q4 : U;          // [0, 4q)
     uint64_t V = shoup_lazy(y, w.w, w.wp, q);   // [0, 2q)
-    x = U + V;                                  // [0, 4q)
-    y = U - V + q2;                             // (0, 4q)
+    x = U + V;                                  // [0, 6q) if red, else [0, 8q)
+    y = U - V + q2;                             // likewise
   }
   static __device__ __forceinline__ void gs(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q) {
     const uint64_t q2 = q << 1;
@@ -94,8 +100,9 @@ struct Bf<true> {
     x = a >= q ? a - q : a;
     y = b >= q ? b - q : b;
   }
-  static __device__ __forceinline__ uint64_t fwd_out(uint64_t x, uint64_t q) {
-    const uint64_t q2 = q << 1;
+  static __device__ __forceinline__ uint64_t fwd_out(uint64_t x, uint64_t q) {   // [0, 8q) -> [0, q)
+    const uint64_t q2 = q << 1, q4 = q << 2;
+    x = x >= q4 ? x - q4 : x;
     x = x >= q2 ? x - q2 : x;
     return x >= q ? x - q : x;
   }
@@ -133,7 +140,7 @@ __device__ __forceinline__ void fwd_high_s(uint64_t (&v)[Sub<LOG_S>::E], uint32_
     for (int h = 0; h < D::E; h++) {
       if (h & span) continue;
       const ShoupW w = ldsw(tw + 16 * ((1 << (D::HI - 1 - i)) + (h >> (i + 1))));
-      Bf<LAZY>::ct(v[h], v[h + span], w, q);
+      Bf<LAZY>::ct(v[h], v[h + span], w, q, ((D::HI - 1 - i) & 1) == 0);
     }
   }
 }
@@ -148,7 +155,7 @@ __device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
       const ShoupW w = ldsw(tw + 16 * ((1 << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + (l >> (i + 1))));
-      Bf<LAZY>::ct(u[l], u[l + span], w, q);
+      Bf<LAZY>::ct(u[l], u[l + span], w, q, ((D::HI + D::LO - 1 - i) & 1) == 0);
     }
   }
 }
@@ -222,7 +229,8 @@ __device__ __forceinline__ void fwd_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      Bf<LAZY>::ct(u[l], u[l + span], w[(1 << (D::LO - 1 - i)) - 1 + (l >> (i + 1))], q);
+      Bf<LAZY>::ct(u[l], u[l + span], w[(1 << (D::LO - 1 - i)) - 1 + (l >> (i + 1))], q,
+                   ((D::HI + D::LO - 1 - i) & 1) == 0);
     }
   }
 }
@@ -670,7 +678,7 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
         for (int h = 0; h < D::E; h++) {
           if (h & span) continue;
           const ShoupW wv = ldsw(st1 + 16 * ((1 << (D::HI - 1 - i)) - 1 + (h >> (i + 1))));
-          Bf<LAZY>::ct(v[h], v[h + span], wv, q);
+          Bf<LAZY>::ct(v[h], v[h + span], wv, q, ((D::HI - 1 - i) & 1) == 0);
         }
       }
       __syncwarp();

@@ -114,6 +114,31 @@ def test_ntt_launch_shapes_bit_exact(log_n, shape):
     assert np.array_equal(d.numpy(), x), "inverse(forward(x)) != x"
 
 
+@pytest.mark.parametrize("bits", [61, 62])
+@pytest.mark.parametrize("shape", [(0, 0), (-1, 0), (1, 0), (0, 1), (1, 1)])
+def test_ntt_prime_size_edges(bits, shape):
+    """The largest primes below 2^61 (lazy butterflies: forward values up to
+    8q just below 2^64) and below 2^62 (strict butterflies), with all-(q-1)
+    and random inputs, for even and odd column-pass stage counts."""
+    require_gpu()
+    split, kind = shape
+    log_n = 15
+    ps = oracle.gen_ntt_primes(bits, 1 << 17, 4)
+    E, ctx, o = _engine_and_oracle(log_n, ps[:2], ps[2:])
+    E.tune("ntt_split", split)
+    E.tune("ntt_cols_kind", kind)
+    rng = np.random.default_rng(bits + 10 * (split + 2) + 100 * kind)
+    x = _rand(rng, ps, 1 << log_n, npolys=2)
+    x[0] = np.array([[p - 1] * (1 << log_n) for p in ps], dtype=np.uint64)
+    d = ctx.upload(x)
+    ctx.ntt_fwd(d, 2, 0, 4)
+    X = d.numpy()
+    for p in range(2):
+        assert np.array_equal(X[p], o.ntt_fwd(x[p])), "forward mismatch"
+    ctx.ntt_inv(d, 2, 0, 4)
+    assert np.array_equal(d.numpy(), x), "inverse(forward(x)) != x"
+
+
 def test_autotune_keeps_results_bit_exact():
     require_gpu()
     ps = oracle.gen_ntt_primes(60, 1 << 15, 6)
