@@ -319,7 +319,7 @@ struct ColTile {
   static constexpr int W = W0 < 2 ? 2 : W0;
   static constexpr int THREADS = Sub<LOG_S>::T * W;
   static constexpr int MIN_BLOCKS = 768 / THREADS < 1 ? 1 : (768 / THREADS > 32 ? 32 : 768 / THREADS);
-  static constexpr size_t SMEM = 2 * (size_t)Sub<LOG_S>::S * W * 8 + (size_t)Sub<LOG_S>::S * sizeof(ShoupW);
+  static constexpr size_t SMEM = 2 * (size_t)Sub<LOG_S>::S * W * 8 + 2 * (size_t)Sub<LOG_S>::S * sizeof(ShoupW);
 };
 
 template <int LOG_S, int DIV>
@@ -335,7 +335,14 @@ struct RowTile {
 };
 
 // Column pass.  Tile = S rows x W columns of one limb; its load is S bulk copies
-// of W*8 bytes (one per row) issued by warp 0.  Shared layout [S][W].
+// of W*8 bytes (one per row) issued by warp 0.  Shared layout [S][W].  Two
+// CTA barriers per item: the first (after the tile's mbarrier) also marks
+// that every thread has finished the previous item, so the next tile's copy
+// into that item's buffer is issued right after it; the second is the
+// exchange between the two digit rounds.  The prime's twiddles alternate
+// between two buffers, so a new limb's twiddles can be written before the
+// first barrier: the buffer's previous users finished at least one item
+// earlier.
 template <int LOG_R, int DIV, bool LAZY, bool FWD>
 __global__ void __launch_bounds__(ColTile<LOG_R, DIV>::THREADS, ColTile<LOG_R, DIV>::MIN_BLOCKS)
 ntt_cols(NttBatch b) {
@@ -352,8 +359,7 @@ ntt_cols(NttBatch b) {
   extern __shared__ __align__(128) uint64_t dyn[];
   __shared__ __align__(8) uint64_t mbar[2];
   const uint32_t sbuf = smem_u32(dyn);                          // [2][S][W] words
-  const uint32_t stw = smem_u32(dyn + 2 * TILE);                // [S] ShoupW
-  ShoupW* tws = (ShoupW*)(dyn + 2 * TILE);
+  ShoupW* tws = (ShoupW*)(dyn + 2 * TILE);                      // [2][S] ShoupW
   const int w = threadIdx.x % W, t = threadIdx.x / W;
   const long N = 1L << b.log_n, C = 1L << b.log_c;
   const int G = gridDim.y;
@@ -381,24 +387,29 @@ ntt_cols(NttBatch b) {
         bulk_g2s(sbuf + (bi * TILE + sig(r) * W) * 8, src + r * C, W * 8, &mbar[bi]);
     }
   };
-  int cur_limb = -1;
+  int cur_limb = -1, tb = 1;
   const int j_lo = (int)((long)blockIdx.y * b.nitems / G), j_hi = (int)((long)(blockIdx.y + 1) * b.nitems / G);
   if (j_lo < j_hi) issue(j_lo, 0);
   for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
     const int bi = it & 1;
     const int limb = j / b.npolys, prime = b.first_prime + (limb >> b.prime_shift);
-    if (j + 1 < j_hi) issue(j + 1, bi ^ 1);
-    if (limb != cur_limb) {                // previous users of tws passed the barrier below
+    if (limb != cur_limb) {                // the other buffer's users are at least one item behind
+      tb ^= 1;
       const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
-      for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[e] = tw[e];
+      for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[tb * D::S + e] = tw[e];
       cur_limb = limb;
     }
     const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
-      if (j + 1 < j_hi) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);   // drain the copy in flight
+      if (threadIdx.x == 0) {
+        atomicOr(b.err, kErrWaitTimeout);
+        mbar_wait(&mbar[bi], (it >> 1) & 1);   // the copy in flight: give it one more bounded wait
+      }
       return;
     }
+    // every thread is past item j - 1: its buffer takes the next tile
+    if (j + 1 < j_hi) issue(j + 1, bi ^ 1);
+    const uint32_t stw = smem_u32(tws + tb * D::S);
     const PrimeConst& P = b.pc[prime];
     const uint64_t q = P.q;
     const uint32_t sm = sbuf + bi * TILE * 8 + w * 8;            // + row * W * 8
@@ -442,9 +453,8 @@ ntt_cols(NttBatch b) {
       for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];
     }
     // generic-proxy accesses of buffer bi end here; the next bulk copy into it
-    // (issued in the next iteration) is an async-proxy write
+    // (issued after the next item's first barrier) is an async-proxy write
     fence_proxy_async();
-    __syncthreads();
   }
 }
 
