@@ -331,7 +331,7 @@ struct RowTile {
   // registers do not spill (measured 1% faster than 512 threads with spills)
   static constexpr int MIN_BLOCKS = 384 / THREADS < 1 ? 1 : (384 / THREADS > 32 ? 32 : 384 / THREADS);
   static constexpr size_t SMEM =
-      2 * (size_t)ROWS * Sub<LOG_S>::S * 8 + (size_t)ROWS * (Sub<LOG_S>::E - 1) * sizeof(ShoupW);
+      2 * (size_t)ROWS * Sub<LOG_S>::S * 8 + 2 * (size_t)ROWS * (Sub<LOG_S>::E - 1) * sizeof(ShoupW);
 };
 
 // Column pass.  Tile = S rows x W columns of one limb; its load is S bulk copies
@@ -611,7 +611,11 @@ __device__ __forceinline__ int swz(int hi, int lo) {
   return (hi << Sub<LOG_S>::LO) + (lo ^ (hi & (Sub<LOG_S>::L - 1)));
 }
 
-// Row pass.  Tile = ROWS contiguous rows of one limb: one bulk copy.
+// Row pass.  Tile = ROWS contiguous rows of one limb: one bulk copy.  A row's
+// threads share a warp, so the exchange needs only the warp; the one CTA
+// barrier per item (after the tile's mbarrier) also frees the previous
+// item's buffer for the next copy, and the high-digit twiddles alternate
+// between two buffers per limb, as in the column pass.
 template <int LOG_C, int DIV, bool LAZY, bool FWD>
 __global__ void __launch_bounds__(RowTile<LOG_C, DIV>::THREADS, RowTile<LOG_C, DIV>::MIN_BLOCKS)
 ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
@@ -622,13 +626,13 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
   extern __shared__ __align__(128) uint64_t dyn[];
   __shared__ __align__(8) uint64_t mbar[2];
   const uint32_t sbuf = smem_u32(dyn);                    // [2][ROWS][S] words
-  ShoupW* tw1 = (ShoupW*)(dyn + 2 * TILE);                 // [ROWS][NT1]
+  ShoupW* tw1 = (ShoupW*)(dyn + 2 * TILE);                 // [2][ROWS][NT1], alternating per limb
   const int t = threadIdx.x % D::T, rho = threadIdx.x / D::T;
   const long N = 1L << b.log_n;
   const int G = gridDim.y;
   const uint32_t row0 = blockIdx.x * ROWS;
   const uint32_t Kbase = (1u << b.log_r) + row0;
-  const uint32_t st1 = smem_u32(tw1 + rho * NT1);
+
   if (threadIdx.x == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
@@ -649,21 +653,21 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
     bulk_g2s(sbuf + bi * TILE * 8, src_of(j), TILE * 8, &mbar[bi]);
   };
   ShoupW w2[D::G][D::L - 1];
-  int cur_limb = -1;
+  int cur_limb = -1, tb = 1;
   uint64_t q = 0;
   const int j_lo = (int)((long)blockIdx.y * b.nitems / G), j_hi = (int)((long)(blockIdx.y + 1) * b.nitems / G);
   if (threadIdx.x == 0 && j_lo < j_hi) issue(j_lo, 0);
   for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
     const int bi = it & 1;
     const int limb = j / b.npolys;
-    if (threadIdx.x == 0 && j + 1 < j_hi) issue(j + 1, bi ^ 1);
-    if (limb != cur_limb) {
+    if (limb != cur_limb) {                // the other buffer's users are at least one item behind
+      tb ^= 1;
       const int prime = b.first_prime + (limb >> b.prime_shift);
       const ShoupW* tw = (FWD ? b.tw : b.itw) + (long)prime * N;
       for (int e = threadIdx.x; e < ROWS * NT1; e += blockDim.x) {
         const int r = e / NT1, jj = e % NT1;
         const int lvl = 31 - __clz(jj + 1);
-        tw1[e] = tw[((Kbase + r) << lvl) + jj + 1 - (1 << lvl)];
+        tw1[tb * ROWS * NT1 + e] = tw[((Kbase + r) << lvl) + jj + 1 - (1 << lvl)];
       }
       load_low_tw<LOG_C>(w2, tw, Kbase + rho, t);
       q = b.pc[prime].q;
@@ -671,10 +675,15 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
     }
     const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
     if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(b.err, kErrWaitTimeout);
-      if (j + 1 < j_hi) mbar_wait(&mbar[bi ^ 1], ((it + 1) >> 1) & 1);
+      if (threadIdx.x == 0) {
+        atomicOr(b.err, kErrWaitTimeout);
+        mbar_wait(&mbar[bi], (it >> 1) & 1);   // the copy in flight: give it one more bounded wait
+      }
       return;
     }
+    // every thread is past item j - 1: its buffer takes the next tile
+    if (threadIdx.x == 0 && j + 1 < j_hi) issue(j + 1, bi ^ 1);
+    const uint32_t st1 = smem_u32(tw1 + tb * ROWS * NT1 + rho * NT1);
     const uint32_t s = sbuf + (bi * TILE + rho * D::S) * 8;
     uint64_t* x = dst_of(j) + rho * D::S;
     uint64_t v[D::E];
@@ -753,8 +762,8 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
 #pragma unroll
       for (int h = 0; h < D::E; h++) x[(h << D::LO) + t] = v[h];
     }
+    // generic-proxy accesses of buffer bi end here (see the column pass)
     fence_proxy_async();
-    __syncthreads();
   }
 }
 

@@ -104,10 +104,12 @@ int aoa_engine_destroy(aoa_engine* e);
  * (0/1: basis conversion on the int8 tensor cores where it applies).      */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
 /* Autotuner: times forward + inverse limb transforms of this engine's ring
- * over `limbs` limbs (0: about 1.5 GiB of limbs) and over a batch-sized call
- * (16 polys, scaled to the same limb count; the sum is the objective) for
+ * over `limbs` limbs (0: about 1.5 GiB of limbs) and over batch-sized calls
+ * (8 polys on each of two streams at once, scaled to the same limb count;
+ * the sum is the objective, each figure the best of two timings) for
  * candidate splits, tile shapes, column-pass kinds, waves and chunk sizes
- * (coordinate descent from the current setting), keeps the best and writes
+ * (coordinate descent from the current setting; a change is kept when it
+ * is at least 2% faster), keeps the best and writes
  * a JSON report of the choice and the objective values (ms) into
  * report[0 .. report_len) (report may be NULL).  Run it before
  * the engine is used from other streams; it synchronises the device.       */
