@@ -104,6 +104,13 @@ AOA_HD uint64_t mont_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t qinv_neg) 
   return redc(a * b, mulhi64(a, b), q, qinv_neg);
 }
 
+// x mod q for x < p, another prime: one conditional subtraction when p < 2q
+// (primes of one bit length), else a Shoup reduction.
+AOA_HD uint64_t cross_mod(uint64_t x, uint64_t p, const PrimeConst& P) {
+  if (p < 2 * P.q) return x >= P.q ? x - P.q : x;
+  return shoup(x, 1, P.one_sh, P.q);
+}
+
 // Exact reduction of an arbitrary 128-bit value hi*2^64 + lo modulo q.
 AOA_HD uint64_t reduce128(uint64_t lo, uint64_t hi, const PrimeConst& P) {
   uint64_t h = shoup(hi, P.r1, P.r1_sh, P.q);     // hi * 2^64 mod q

@@ -340,7 +340,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
         for (int u = 0; u < 2; u++) {
           if (j + u < je) {
             const PrimeConst& P = a.pc[a.out_prime0 + j + u];
-            out[(long)(j + u - a.out_shift) * N] = add_mod(tc_combine(v + 8 * u, P), shoup(cl, 1, P.one_sh, P.q), P.q);
+            out[(long)(j + u - a.out_shift) * N] = add_mod(tc_combine(v + 8 * u, P), cross_mod(cl, Pl.q, P), P.q);
           }
         }
       }
