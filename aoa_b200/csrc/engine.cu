@@ -77,7 +77,7 @@ static void build_prime_tables(Engine& E) {
     c.ninv_w1_sh = h_shoup_companion(c.ninv_w1, q);
     c.bar_sh = 0;
     c.bar_mu = 0;
-    if (q >= 4 && q < (1ull << 62)) {
+    if (q >= (1ull << 33) && q < (1ull << 62)) {
       const int n = 64 - __builtin_clzll(q);
       c.bar_sh = (uint64_t)(n - 2);
       c.bar_mu = (uint64_t)((one128 << (64 + n - 2)) / q);

@@ -7,7 +7,7 @@
 //   * Shoup multiplication by a precomputed constant w with w' = floor(w 2^64/q)
 //     (twiddles, CRT constants): one mul.hi and two mul.lo;
 //   * Barrett multiplication with a 64-bit quotient estimate for products of
-//     two variable residues (q < 2^62), Montgomery REDC above that;
+//     two variable residues (2^33 <= q < 2^62), Montgomery REDC otherwise;
 //   * two Shoup steps to fold a 128-bit accumulator (basis conversion sums).
 // All routines require q < 2^63 and return canonical values in [0, q)
 // unless named *_lazy.
@@ -26,8 +26,8 @@ struct PrimeConst {
   uint64_t one_sh;     // floor(2^64 / q)       (Shoup companion of 1)
   uint64_t ninv, ninv_sh;          // N^-1 mod q
   uint64_t ninv_w1, ninv_w1_sh;    // N^-1 * psi^-bitrev(1) mod q (last inverse stage)
-  uint64_t bar_mu;     // floor(2^(64+s) / q), s = bar_sh       (Barrett, q < 2^62)
-  uint64_t bar_sh;     // bit length of q minus 2; 0 when q >= 2^62 (Montgomery instead)
+  uint64_t bar_mu;     // floor(2^(64+s) / q), s = bar_sh       (Barrett, 2^33 <= q < 2^62)
+  uint64_t bar_sh;     // bit length of q minus 2; 0 outside that range (Montgomery instead)
 };
 
 struct ShoupW {      // twiddle or constant w with its Shoup companion
@@ -73,14 +73,26 @@ AOA_HD uint64_t redc(uint64_t lo, uint64_t hi, uint64_t q, uint64_t qinv_neg) {
   return t >= q ? t - q : t;
 }
 
-// x = hi 2^64 + lo mod q for x < 2^(64+s), q < 2^62 of bit length n, s = n - 2,
-// by Barrett's method with a 64-bit quotient estimate: x1 = floor(x / 2^s)
-// < 2^64 and mu = floor(2^(64+s) / q) < 2^63; the estimate
-// qh = floor(x1 mu / 2^64) satisfies x/q - 2.5 < qh <= x/q (the truncations
-// of x1 and mu cost < x / 2^(64+s) + 2^s/q <= 1.5, the final floor < 1), so
-// r = x - qh q lies in [0, 3q) and is exact in 64 bits.
+// x = hi 2^64 + lo mod q for x < 2^(64+s), q of bit length n in [34, 62],
+// s = n - 2, by Barrett's method with a 64-bit quotient estimate:
+// x1 = floor(x / 2^s) < 2^64 and mu = floor(2^(64+s) / q) < 2^63; the
+// estimate qh = floor(x1 mu / 2^64) satisfies x/q - 2.5 < qh <= x/q (the
+// truncations of x1 and mu cost < x / 2^(64+s) + 2^s/q <= 1.5, the final floor
+// < 1), so r = x - qh q lies in [0, 3q) and is exact in 64 bits.  With
+// s >= 32, x1 is two 32-bit funnel shifts of the words 1..3 of x.
+AOA_HD uint32_t funnel_r32(uint32_t lo, uint32_t hi, uint32_t sh) {   // low word of (hi:lo) >> (sh % 32)
+#ifdef __CUDA_ARCH__
+  return __funnelshift_r(lo, hi, sh);
+#else
+  return (uint32_t)((((uint64_t)hi << 32) | lo) >> (sh & 31));
+#endif
+}
+
 AOA_HD uint64_t barrett_wide(uint64_t lo, uint64_t hi, uint64_t q, uint64_t mu, uint32_t s) {
-  const uint64_t x1 = (hi << (64 - s)) | (lo >> s);
+  const uint32_t t = s - 32;
+  const uint32_t x1lo = funnel_r32((uint32_t)(lo >> 32), (uint32_t)hi, t);
+  const uint32_t x1hi = funnel_r32((uint32_t)hi, (uint32_t)(hi >> 32), t);
+  const uint64_t x1 = ((uint64_t)x1hi << 32) | x1lo;
   uint64_t r = lo - mulhi64(x1, mu) * q;
   r = r >= q ? r - q : r;
   return r >= q ? r - q : r;
@@ -91,7 +103,19 @@ AOA_HD uint64_t barrett_mul(uint64_t a, uint64_t b, uint64_t q, uint64_t mu, uin
   return barrett_wide(a * b, mulhi64(a, b), q, mu, s);
 }
 
-// a * b mod q for a, b < q: Barrett for q < 2^62, else two REDC steps through R^2.
+// (a b + c d) mod q for a, b, c, d < 2^n with n <= 61: the 128-bit sum is
+// below 2^(2n+1) <= 2^(64+s), so one reduction serves both products.
+AOA_HD uint64_t barrett_mul_add2(uint64_t a, uint64_t b, uint64_t c, uint64_t d, uint64_t q, uint64_t mu,
+                                 uint32_t s) {
+  uint64_t lo = a * b, hi = mulhi64(a, b);
+  const uint64_t l2 = c * d;
+  hi += mulhi64(c, d);
+  lo += l2;
+  hi += lo < l2;
+  return barrett_wide(lo, hi, q, mu, s);
+}
+
+// a * b mod q for a, b < q: Barrett for 2^33 <= q < 2^62, else two REDC steps through R^2.
 AOA_HD uint64_t mul_mod(uint64_t a, uint64_t b, const PrimeConst& P) {
   if (P.bar_sh) return barrett_mul(a, b, P.q, P.bar_mu, (uint32_t)P.bar_sh);
   uint64_t lo = a * b, hi = mulhi64(a, b);

@@ -21,6 +21,12 @@ struct CLimbs {
 
 __device__ __forceinline__ long coef_index() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
 
+// The HMult element-wise kernels take kEwPer coefficients per thread (u-th at
+// coef_u(u), each access still coalesced across the block), so a thread's
+// per-limb constants and addresses serve several coefficients (N >= 1024).
+constexpr int kEwPer = 4;
+__device__ __forceinline__ long coef_u(int u) { return ((long)blockIdx.x * kEwPer + u) * blockDim.x + threadIdx.x; }
+
 // c = a (op) b over limbs; op: 0 add, 1 sub, 2 mul (Montgomery pair), 3 neg(a)
 __global__ void ew_binary(Limbs c, CLimbs a, CLimbs b, int op, int prime0, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
@@ -70,11 +76,12 @@ __device__ __forceinline__ void tensor3(uint64_t x0, uint64_t x1, uint64_t y0, u
     const uint64_t mu = P.bar_mu;
     const uint32_t s = (uint32_t)P.bar_sh;
     d0 = barrett_mul(x0, y0, q, mu, s);
-    d1 = add_mod(barrett_mul(x0, y1, q, mu, s), barrett_mul(x1, y0, q, mu, s), q);
+    d1 = s <= 59 ? barrett_mul_add2(x0, y1, x1, y0, q, mu, s)        // q < 2^61: one reduction
+                 : add_mod(barrett_mul(x0, y1, q, mu, s), barrett_mul(x1, y0, q, mu, s), q);
     d2 = barrett_mul(x1, y1, q, mu, s);
     return;
   }
-  // q >= 2^62: Montgomery products carry a 2^-64 factor; one more REDC by R^2 clears it.
+  // Montgomery products carry a 2^-64 factor; one more REDC by R^2 clears it.
   const uint64_t qi = P.qinv_neg;
   const uint64_t m0 = mont_mul(x0, y0, q, qi);
   const uint64_t m1 = add_mod(mont_mul(x0, y1, q, qi), mont_mul(x1, y0, q, qi), q);
@@ -84,16 +91,34 @@ __device__ __forceinline__ void tensor3(uint64_t x0, uint64_t x1, uint64_t y0, u
   d2 = mont_mul(m2, P.r2, q, qi);
 }
 
+// operands of kEwPer coefficients, loaded before any store
+__device__ __forceinline__ void tensor_ew(const uint64_t* a, long a_half, const uint64_t* b, long b_half,
+                                          uint64_t* d0, uint64_t* d1, uint64_t* d2, const PrimeConst& P) {
+  uint64_t x0[kEwPer], x1[kEwPer], y0[kEwPer], y1[kEwPer];
+#pragma unroll
+  for (int u = 0; u < kEwPer; u++) {
+    const long c = coef_u(u);
+    x0[u] = a[c];
+    x1[u] = a[a_half + c];
+    y0[u] = b[c];
+    y1[u] = b[b_half + c];
+  }
+#pragma unroll
+  for (int u = 0; u < kEwPer; u++) {
+    const long c = coef_u(u);
+    uint64_t r0, r1, r2;
+    tensor3(x0[u], x1[u], y0[u], y1[u], P, r0, r1, r2);
+    d0[c] = r0;
+    d1[c] = r1;
+    d2[c] = r2;
+  }
+}
+
 __global__ void hmult_tensor(const uint64_t* a, const uint64_t* b, long a_half, long b_half, uint64_t* d0,
                              uint64_t* d1, uint64_t* d2, const PrimeConst* pc, int log_n) {
-  const long N = 1L << log_n;
-  const long off = (long)blockIdx.y * N + coef_index();
-  const PrimeConst& P = pc[blockIdx.y];
-  uint64_t r0, r1, r2;
-  tensor3(a[off], a[a_half + off], b[off], b[b_half + off], P, r0, r1, r2);
-  d0[off] = r0;
-  d1[off] = r1;
-  d2[off] = r2;
+  const long limb = (long)blockIdx.y << log_n;
+  const PrimeConst P = pc[blockIdx.y];
+  tensor_ew(a + limb, a_half, b + limb, b_half, d0 + limb, d1 + limb, d2 + limb, P);
 }
 
 // Key-switch products over the QB limbs of the extended d2 (transform domain):
@@ -103,14 +128,25 @@ __global__ void hmult_tensor(const uint64_t* a, const uint64_t* b, long a_half, 
 __global__ void keyswitch_mul(const uint64_t* xq, const uint64_t* xb, const uint64_t* key, long key_half,
                               uint64_t* k0, uint64_t* k1, int nq, int K, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
-  const long c = coef_index();
   const int l = blockIdx.y;
   const int prime = l < nq ? l : K + (l - nq);
-  const uint64_t x = l < nq ? xq[(long)l * N + c] : xb[(long)(l - nq) * N + c];
-  const PrimeConst& P = pc[prime];
-  const uint64_t kb = key[(long)prime * N + c], ka = key[key_half + (long)prime * N + c];
-  k0[(long)l * N + c] = mul_mod(x, kb, P);
-  k1[(long)l * N + c] = mul_mod(x, ka, P);
+  const uint64_t* x = l < nq ? xq + (long)l * N : xb + (long)(l - nq) * N;
+  const uint64_t* kbp = key + (long)prime * N;
+  const PrimeConst P = pc[prime];
+  uint64_t xv[kEwPer], kb[kEwPer], ka[kEwPer];
+#pragma unroll
+  for (int u = 0; u < kEwPer; u++) {
+    const long c = coef_u(u);
+    xv[u] = x[c];
+    kb[u] = kbp[c];
+    ka[u] = kbp[key_half + c];
+  }
+#pragma unroll
+  for (int u = 0; u < kEwPer; u++) {
+    const long c = coef_u(u);
+    k0[(long)l * N + c] = mul_mod(xv[u], kb[u], P);
+    k1[(long)l * N + c] = mul_mod(xv[u], ka[u], P);
+  }
 }
 
 // Coefficient-domain automorphism X -> X^g (g odd, mod 2N) with the
@@ -159,49 +195,54 @@ __global__ void automorph_ntt_batch(CtPtrs ptr, long half, uint64_t* out, int n,
 // tensor for op z = blockIdx.z: a = ptr.a[z], b = ptr.b[z] ([c0 | c1], stride half);
 // outputs to the blocks D0 = D, D1 = D + n*half, D2 = D + 2n*half, op stride half.
 __global__ void hmult_tensor_batch(CtPtrs ptr, long half, uint64_t* D, int n, const PrimeConst* pc, int log_n) {
-  const long N = 1L << log_n;
   const int z = blockIdx.z;
-  const long off = (long)blockIdx.y * N + coef_index();
-  const PrimeConst& P = pc[blockIdx.y];
-  const uint64_t* a = ptr.a[z];
-  const uint64_t* b = ptr.b[z];
-  uint64_t r0, r1, r2;
-  tensor3(a[off], a[half + off], b[off], b[half + off], P, r0, r1, r2);
+  const long limb = (long)blockIdx.y << log_n;
+  const PrimeConst P = pc[blockIdx.y];
   const long nh = (long)n * half;
-  uint64_t* d = D + (long)z * half + off;
-  d[0] = r0;
-  d[nh] = r1;
-  d[2 * nh] = r2;
+  uint64_t* d = D + (long)z * half + limb;
+  tensor_ew(ptr.a[z] + limb, half, ptr.b[z] + limb, half, d, d + nh, d + 2 * nh, P);
 }
 
 // key products for op z: x limbs (Q part at xq + z*xq_stride, B part at
 // xb + z*xb_stride) times the key; k0 of op z at k + z*k_stride, k1 at
 // k + (n + z)*k_stride.
-// One thread per (limb, coefficient) loops over the n ops, so that each key
-// word is read from memory once per launch.
+// One thread per (limb, kEwPer coefficients) loops over the n ops, so that
+// each key word is read from memory once per launch.
 __global__ void keyswitch_mul_batch(const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
                                     const uint64_t* key, long key_half, uint64_t* k, long k_stride, int n, int nq,
                                     int K, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
-  const long c = coef_index();
   const int l = blockIdx.y;
   const int prime = l < nq ? l : K + (l - nq);
-  const uint64_t* x = l < nq ? xq + (long)l * N + c : xb + (long)(l - nq) * N + c;
+  const uint64_t* x = l < nq ? xq + (long)l * N : xb + (long)(l - nq) * N;
   const long xs = l < nq ? xq_stride : xb_stride;
   const PrimeConst P = pc[prime];
-  const uint64_t kb = key[(long)prime * N + c], ka = key[key_half + (long)prime * N + c];
-  uint64_t* o = k + (long)l * N + c;
-#pragma unroll 4
+  const uint64_t* kbp = key + (long)prime * N;
+  uint64_t kb[kEwPer], ka[kEwPer];
+#pragma unroll
+  for (int u = 0; u < kEwPer; u++) {
+    const long c = coef_u(u);
+    kb[u] = kbp[c];
+    ka[u] = kbp[key_half + c];
+  }
+  uint64_t* o = k + (long)l * N;
   for (int z = 0; z < n; z++) {
-    const uint64_t v = x[z * xs];
-    o[z * k_stride] = mul_mod(v, kb, P);
-    o[(n + z) * k_stride] = mul_mod(v, ka, P);
+    uint64_t v[kEwPer];
+#pragma unroll
+    for (int u = 0; u < kEwPer; u++) v[u] = x[z * xs + coef_u(u)];
+#pragma unroll
+    for (int u = 0; u < kEwPer; u++) {
+      const long c = coef_u(u);
+      o[z * k_stride + c] = mul_mod(v[u], kb[u], P);
+      o[(n + z) * k_stride + c] = mul_mod(v[u], ka[u], P);
+    }
   }
 }
 
 // ---- host wrappers -----------------------------------------------------------
 
 static dim3 ew_grid(const Engine& E, int nlimbs, int npolys) { return dim3(E.N / 256, nlimbs, npolys); }
+static dim3 ew4_grid(const Engine& E, int nlimbs, int npolys) { return dim3(E.N / (256 * kEwPer), nlimbs, npolys); }
 
 void ew_binary_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as, const uint64_t* b, long bs,
                   int op, int prime0, int nlimbs, int npolys, cudaStream_t st) {
@@ -229,12 +270,12 @@ void ew_muladd_op(const Engine& E, uint64_t* d, long ds, const uint64_t* a, long
 
 void tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
                uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st) {
-  hmult_tensor<<<ew_grid(E, nlimbs, 1), 256, 0, st>>>(a, b, a_half, b_half, d0, d1, d2, E.d_pc, E.log_n); note_launch();
+  hmult_tensor<<<ew4_grid(E, nlimbs, 1), 256, 0, st>>>(a, b, a_half, b_half, d0, d1, d2, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 
 void tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D, int n, int nlimbs, cudaStream_t st) {
-  hmult_tensor_batch<<<ew_grid(E, nlimbs, n), 256, 0, st>>>(ptr, half, D, n, E.d_pc, E.log_n);
+  hmult_tensor_batch<<<ew4_grid(E, nlimbs, n), 256, 0, st>>>(ptr, half, D, n, E.d_pc, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
 }
@@ -243,7 +284,7 @@ void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride,
                             const uint64_t* key, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st, int nb) {
   const long half = (long)E.nprimes * E.N;
   if (nb < 0) nb = E.kl;
-  keyswitch_mul_batch<<<ew_grid(E, nq + nb, 1), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
+  keyswitch_mul_batch<<<ew4_grid(E, nq + nb, 1), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key, half, k, k_stride,
                                                                n, nq, E.k, E.d_pc, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
@@ -253,7 +294,7 @@ void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, c
                       uint64_t* k1, int nq, cudaStream_t st, int nb) {
   const long half = (long)E.nprimes * E.N;
   if (nb < 0) nb = E.kl;
-  keyswitch_mul<<<ew_grid(E, nq + nb, 1), 256, 0, st>>>(xq, xb, key, half, k0, k1, nq, E.k, E.d_pc, E.log_n); note_launch();
+  keyswitch_mul<<<ew4_grid(E, nq + nb, 1), 256, 0, st>>>(xq, xb, key, half, k0, k1, nq, E.k, E.d_pc, E.log_n); note_launch();
   AOA_CHECK_LAUNCH();
 }
 

@@ -203,7 +203,7 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 // sum_b T_b 2^(8b) (b < 8, T_b < 2^24) reduced mod P.  W_0 = sum_t T_t 2^(8t)
 // and W_1 = sum_t T_(4+t) 2^(8t) (< 2^49 each) come from 32 x 32 -> 64-bit
 // multiply-adds; x = W_0 + W_1 2^32 < 2^81 has a high word below 2^17, so
-// one Barrett step reduces it when s = bit length - 2 >= 17.
+// one Barrett step (s >= 32) reduces it.
 __device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const PrimeConst& P) {
   uint64_t W0 = v[0], W1 = v[4];
   asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(W0) : "r"(v[1]));
@@ -218,7 +218,7 @@ __device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const PrimeCon
       : "=r"(r1), "=r"(r2)
       : "r"((uint32_t)(W0 >> 32)), "r"((uint32_t)W1), "r"((uint32_t)(W1 >> 32)));
   const uint64_t lo = ((uint64_t)r1 << 32) | (uint32_t)W0;
-  if (P.bar_sh >= 17) return barrett_wide(lo, r2, P.q, P.bar_mu, (uint32_t)P.bar_sh);
+  if (P.bar_sh) return barrett_wide(lo, r2, P.q, P.bar_mu, (uint32_t)P.bar_sh);
   return reduce128(lo, r2, P);
 }
 
@@ -536,25 +536,43 @@ void rescale(const Engine& E, uint64_t* d, long poly_stride, int npolys, int lev
 //   else:              out_i = base_i + (k_i - y_i) * B^-1           (ModDown)
 // base and y may be null (treated as 0); limb b of the launch is limb prime0 + b
 // (prime prime0 + b).  Strides are per poly, in words.
+// kCombPer coefficients per thread (the u-th at ((blockIdx.x kCombPer + u)
+// blockDim + threadIdx), coalesced), so the per-limb constants and addresses
+// serve several outputs.
+constexpr int kCombPer = 4;
+
+__device__ __forceinline__ uint64_t ks_combine_one(uint64_t bv, uint64_t kv, uint64_t yv, ShoupW binv,
+                                                   const ShoupW* resc, ShoupW rs, uint64_t q) {
+  if (resc) return shoup(sub_mod(add_mod(bv, shoup(kv, binv, q), q), yv, q), rs, q);
+  return add_mod(bv, shoup(sub_mod(kv, yv, q), binv, q), q);
+}
+
 __global__ void ks_combine_kernel(uint64_t* out, long out_stride, const uint64_t* base, long base_stride,
                                   const uint64_t* k, long k_stride, const uint64_t* y, long y_stride,
                                   const ShoupW* binv, const ShoupW* resc, const PrimeConst* pc, int prime0,
                                   int log_n) {
   const long N = 1L << log_n;
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = prime0 + blockIdx.y, p = blockIdx.z;
-  const long off = (long)blockIdx.y * N + c;
+  const long limb = (long)blockIdx.y * N;
   const uint64_t q = pc[i].q;
-  const uint64_t kv = k[p * k_stride + off], yv = y ? y[p * y_stride + off] : 0;
-  const uint64_t bv = base ? base[p * base_stride + off] : 0;
-  uint64_t r;
-  if (resc) {
-    r = sub_mod(add_mod(bv, shoup(kv, binv[i], q), q), yv, q);
-    r = shoup(r, resc[i], q);
-  } else {
-    r = add_mod(bv, shoup(sub_mod(kv, yv, q), binv[i], q), q);
+  const ShoupW bi = binv[i], rs = resc ? resc[i] : ShoupW{0, 0};
+  const uint64_t* kp = k + p * k_stride + limb;
+  const uint64_t* yp = y ? y + p * y_stride + limb : nullptr;
+  const uint64_t* bp = base ? base + p * base_stride + limb : nullptr;
+  uint64_t* op = out + p * out_stride + limb;
+  uint64_t kv[kCombPer], yv[kCombPer], bv[kCombPer];
+#pragma unroll
+  for (int u = 0; u < kCombPer; u++) {
+    const long c = ((long)blockIdx.x * kCombPer + u) * blockDim.x + threadIdx.x;
+    kv[u] = kp[c];
+    yv[u] = yp ? yp[c] : 0;
+    bv[u] = bp ? bp[c] : 0;
   }
-  out[p * out_stride + off] = r;
+#pragma unroll
+  for (int u = 0; u < kCombPer; u++) {
+    const long c = ((long)blockIdx.x * kCombPer + u) * blockDim.x + threadIdx.x;
+    op[c] = ks_combine_one(bv[u], kv[u], yv[u], bi, resc, rs, q);
+  }
 }
 
 // Same epilogue writing poly p to outp.p[p] (a list of output polys).
@@ -562,26 +580,34 @@ __global__ void ks_combine_ptr_kernel(OutPtrs outp, const uint64_t* base, long b
                                       const uint64_t* k, long k_stride, const uint64_t* y, long y_stride,
                                       const ShoupW* binv, const ShoupW* resc, const PrimeConst* pc, int log_n) {
   const long N = 1L << log_n;
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y, p = blockIdx.z;
-  const long off = (long)i * N + c;
+  const long limb = (long)i * N;
   const uint64_t q = pc[i].q;
-  const uint64_t kv = k[p * k_stride + off], yv = y[p * y_stride + off];
-  const uint64_t bv = base && p < base_polys ? base[p * base_stride + off] : 0;
-  uint64_t r;
-  if (resc) {
-    r = shoup(sub_mod(add_mod(bv, shoup(kv, binv[i], q), q), yv, q), resc[i], q);
-  } else {
-    r = add_mod(bv, shoup(sub_mod(kv, yv, q), binv[i], q), q);
+  const ShoupW bi = binv[i], rs = resc ? resc[i] : ShoupW{0, 0};
+  const uint64_t* kp = k + p * k_stride + limb;
+  const uint64_t* yp = y + p * y_stride + limb;
+  const uint64_t* bp = base && p < base_polys ? base + p * base_stride + limb : nullptr;
+  uint64_t* op = outp.p[p] + limb;
+  uint64_t kv[kCombPer], yv[kCombPer], bv[kCombPer];
+#pragma unroll
+  for (int u = 0; u < kCombPer; u++) {
+    const long c = ((long)blockIdx.x * kCombPer + u) * blockDim.x + threadIdx.x;
+    kv[u] = kp[c];
+    yv[u] = yp[c];
+    bv[u] = bp ? bp[c] : 0;
   }
-  outp.p[p][off] = r;
+#pragma unroll
+  for (int u = 0; u < kCombPer; u++) {
+    const long c = ((long)blockIdx.x * kCombPer + u) * blockDim.x + threadIdx.x;
+    op[c] = ks_combine_one(bv[u], kv[u], yv[u], bi, resc, rs, q);
+  }
 }
 
 void ks_combine_ptr(const Engine& E, const OutPtrs& outp, const uint64_t* base, long base_stride, const uint64_t* k,
                     long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys, int rescale_level,
                     cudaStream_t st, int base_polys) {
   if (nlimbs <= 0) return;
-  dim3 grid(E.N / 256, nlimbs, npolys);
+  dim3 grid(E.N / (256 * kCombPer), nlimbs, npolys);
   const ShoupW* resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
   ks_combine_ptr_kernel<<<grid, 256, 0, st>>>(outp, base, base_stride, base_polys < 0 ? npolys : base_polys, k,
                                               k_stride, y, y_stride, E.rns.moddown_binv, resc, E.d_pc, E.log_n);
@@ -593,7 +619,7 @@ void ks_combine(const Engine& E, uint64_t* out, long out_stride, const uint64_t*
                 const uint64_t* k, long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys,
                 int rescale_level, cudaStream_t st, int prime0) {
   if (nlimbs <= 0) return;
-  dim3 grid(E.N / 256, nlimbs, npolys);
+  dim3 grid(E.N / (256 * kCombPer), nlimbs, npolys);
   const ShoupW* resc = rescale_level > 0 ? E.rns.resc_inv + (long)rescale_level * E.k : nullptr;
   ks_combine_kernel<<<grid, 256, 0, st>>>(out, out_stride, base, base_stride, k, k_stride, y, y_stride,
                                           E.rns.moddown_binv, resc, E.d_pc, prime0, E.log_n);
