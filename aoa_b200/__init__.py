@@ -50,6 +50,23 @@ class Engine:
         "conv_tensor_cores", "fuse", "batch_streams")."""
         capi.check(capi.load().aoa_engine_tune(self.handle, knob.encode(), float(value)))
 
+    TRANSFORM_KNOBS = ("ntt_split", "ntt_cols_div", "ntt_cols_kind", "ntt_rows_div", "ntt_waves",
+                       "ntt_waves_large", "ntt_chunk_bytes")
+
+    def tune_get(self, knob):
+        """Current value of a launch-shape knob."""
+        v = ctypes.c_double()
+        capi.check(capi.load().aoa_engine_tune_get(self.handle, knob.encode(), ctypes.byref(v)))
+        return v.value
+
+    def transform_shapes(self):
+        """The transform knobs as a dict (ints where the knob is integral)."""
+        out = {}
+        for k in self.TRANSFORM_KNOBS:
+            v = self.tune_get(k)
+            out[k] = int(v) if v == int(v) else v
+        return out
+
     def autotune(self, limbs=0):
         """Time candidate transform shapes on this engine's ring and keep the
         fastest; returns the tuner's report (choice, timings in ms)."""

@@ -101,6 +101,7 @@ SIGNATURES = {
     "aoa_engine_dgt_roots": (c_int, [c_void_p, c_void_p]),
     "aoa_ctx_set_transform": (c_int, [c_void_p, c_int]),
     "aoa_engine_tune": (c_int, [c_void_p, c_char_p, c_double]),
+    "aoa_engine_tune_get": (c_int, [c_void_p, c_char_p, ctypes.POINTER(c_double)]),
     "aoa_engine_autotune": (c_int, [c_void_p, c_int, c_char_p, c_size_t]),
     "aoa_mul_plaintext": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_u64, c_int]),
     "aoa_mul_const": (c_int, [c_void_p, c_void_p, c_void_p, c_double, c_int]),

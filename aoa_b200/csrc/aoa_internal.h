@@ -36,15 +36,18 @@ constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration
 constexpr int kLargeItems = 1536;           // limb-transform launches this large use ntt_waves_large
 
 struct Tune {
-  long ntt_chunk_bytes = 1L << 30;    // limbs per transform launch pair (bytes); larger chunks
+  // Defaults: the shapes measured best on B200 at 2^16 for the batched HMult
+  // pipeline (8-row tiles in the row pass) and for large transform calls
+  // (4 GiB chunks, 8 waves); the autotuner can refine them per ring.
+  long ntt_chunk_bytes = 1L << 32;    // limbs per transform launch pair (bytes); larger chunks
                                       // mean fewer launch tails (measured: 1 GiB beats an L2-sized chunk)
   double ntt_waves = 1.0;             // transform CTAs per pass, in resident waves
-  double ntt_waves_large = 1.0;       // the same for launches of at least kLargeItems limbs
+  double ntt_waves_large = 8.0;       // the same for launches of at least kLargeItems limbs
   bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
   int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split
   int ntt_cols_div = 0;               // column-pass tile width: widest >> div (0..2)
   int ntt_cols_kind = 0;              // column pass: 0 CTA-wide exchange, 1 warp-owned columns
-  int ntt_rows_div = 0;               // row-pass tile height: tallest >> div (0..2)
+  int ntt_rows_div = 1;               // row-pass tile height: tallest >> div (0..2)
   // transform ends fused with their neighbours (bit mask): 1 out-of-place
   // inverse instead of a copy, 2 key products in the special-limb forward
   // transform, 4 key-switch combine in the corrections' forward transform

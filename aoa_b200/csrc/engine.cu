@@ -320,6 +320,24 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   return AOA_OK;
 }
 
+int aoa_engine_tune_get(const aoa_engine* h, const char* knob, double* value) {
+  if (!h || !knob || !value) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  const std::string k(knob);
+  const Tune& t = h->e.tune;
+  if (k == "ntt_chunk_bytes") *value = (double)t.ntt_chunk_bytes;
+  else if (k == "ntt_waves") *value = t.ntt_waves;
+  else if (k == "ntt_waves_large") *value = t.ntt_waves_large;
+  else if (k == "conv_tensor_cores") *value = t.conv_tensor_cores ? 1 : 0;
+  else if (k == "ntt_split") *value = t.ntt_split;
+  else if (k == "ntt_cols_div") *value = t.ntt_cols_div;
+  else if (k == "ntt_rows_div") *value = t.ntt_rows_div;
+  else if (k == "ntt_cols_kind") *value = t.ntt_cols_kind;
+  else if (k == "batch_streams") *value = t.batch_streams;
+  else if (k == "fuse") *value = t.fuse;
+  else return fail(AOA_ERR_BAD_PARAM, "unknown knob: " + k);
+  return AOA_OK;
+}
+
 int aoa_engine_info(const aoa_engine* h, int* log_n, int* k, int* kl, uint64_t* primes_out) {
   if (!h) return fail(AOA_ERR_BAD_PARAM, "null engine");
   if (log_n) *log_n = h->e.log_n;

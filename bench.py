@@ -359,8 +359,10 @@ def main():
     ap.add_argument("--profile-case", choices=["ntt", "hmult", "batch"],
                     help="run a small fixed case for ncu captures (no timing, no JSON)")
     ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt")
-    ap.add_argument("--no-autotune", action="store_true", help="keep the default transform launch shapes")
-    ap.add_argument("--knobs", default="", help="engine knobs name=value,... applied instead of the autotuner")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the transform autotuner first (default: the engine's measured-best shapes)")
+    ap.add_argument("--no-autotune", action="store_true", help="(default) keep the engine's transform shapes")
+    ap.add_argument("--knobs", default="", help="engine knobs name=value,... applied before the run")
     args = ap.parse_args()
     world, rank, local = dist_setup()     # the launcher's WORLD_SIZE / RANK / LOCAL_RANK
     if args.impl == "reference":
@@ -375,14 +377,16 @@ def main():
 
     ps = primes()
     E = aoa.Engine(LOG_N, ps[:K], ps[K:], scale_bits=SCALE_BITS)
-    tuning = None
+    source = "engine defaults (measured best on B200 at 2^16)"
     if args.knobs:
         for kv in args.knobs.split(","):
             k, v = kv.split("=")
             E.tune(k, float(v))
-        tuning = {"knobs": args.knobs}
-    elif not args.no_autotune and not args.profile_case:
-        tuning = E.autotune()["choice"]
+        source = "knobs " + args.knobs
+    elif args.autotune and not args.profile_case:
+        E.autotune()
+        source = "autotuner"
+    tuning = dict(E.transform_shapes(), source=source)
     ctx = aoa.Context(E)
     stream = torch.cuda.ExternalStream(ctx.stream)
     N = 1 << LOG_N

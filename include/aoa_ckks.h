@@ -103,6 +103,8 @@ int aoa_engine_destroy(aoa_engine* e);
  * "conv_tensor_cores"
  * (0/1: basis conversion on the int8 tensor cores where it applies).      */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
+/* current value of a knob (names as for aoa_engine_tune) */
+int aoa_engine_tune_get(const aoa_engine* e, const char* knob, double* value);
 /* Autotuner: times forward + inverse limb transforms of this engine's ring
  * over `limbs` limbs (0: about 1.5 GiB of limbs) and over batch-sized calls
  * (8 polys on each of two streams at once, scaled to the same limb count;
