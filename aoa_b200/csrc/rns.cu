@@ -159,7 +159,8 @@ basis_convert(ConvArgs a, int j_first, int j_end) {
 // Shared memory (no swizzle, K-major "core matrices" of 8 rows x 16 bytes):
 //   A: [16 k-chunks][128 rows][16 B]   = 32 KiB, descriptor LBO 2048, SBO 128
 //   B: [16 k-chunks][256 rows][16 B]   = 64 KiB, descriptor LBO 4096, SBO 128
-constexpr int kTcRows = 128;
+constexpr int kTcRowsLog = 7;
+constexpr int kTcRows = 1 << kTcRowsLog;
 constexpr int kTcThreads = 512;
 constexpr int kTcN = 256;
 constexpr size_t kTcA = 16 * kTcRows * 16;
@@ -239,8 +240,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   uint8_t* Bs = tcs + kTcA;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const long N = 1L << a.log_n;
-  const long tiles_per_poly = N / kTcRows;
-  const long ntiles = tiles_per_poly * a.npolys;
+  const int tile_shift = a.log_n - kTcRowsLog;             // tiles per poly = N / kTcRows = 2^tile_shift
+  const long ntiles = (long)a.npolys << tile_shift;
   const int npairs = (a.nin + 1) / 2;
   // zero A (inputs beyond nin stay zero), barriers, tensor memory, the table image
   for (int e = threadIdx.x; e < (int)(kTcA / 16); e += blockDim.x) ((uint4*)As)[e] = make_uint4(0, 0, 0, 0);
@@ -268,7 +269,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   const int ar = threadIdx.x % kTcRows, ap = threadIdx.x / kTcRows;
   uint64_t xa[kTcPairs], xb[kTcPairs];
   auto load_inputs = [&](long tile) {
-    const long poly = tile / tiles_per_poly, c0 = (tile % tiles_per_poly) * kTcRows;
+    const long poly = tile >> tile_shift, c0 = (tile & ((1L << tile_shift) - 1)) * kTcRows;
     const uint64_t* in = a.in + poly * a.in_poly_stride + c0 + ar;
 #pragma unroll
     for (int m = 0; m < kTcPairs; m++) {
@@ -284,8 +285,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   const int ksteps = (a.nin + 3) / 4;                      // 4 inputs (32 bytes) per MMA K step
   uint32_t phase = 0;
   for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const long poly = tile / tiles_per_poly;
-    const long c0 = (tile % tiles_per_poly) * kTcRows;
+    const long poly = tile >> tile_shift;
+    const long c0 = (tile & ((1L << tile_shift) - 1)) * kTcRows;
     // A: row ar, inputs 2p and 2p + 1 as one 16-byte store at chunk p
 #pragma unroll
     for (int m = 0; m < kTcPairs; m++) {
