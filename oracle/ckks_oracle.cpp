@@ -1,6 +1,6 @@
 // CKKS CPU ORACLE — test infrastructure only.
 //
-// This file is the checker, never the product: only tests/, the smoke check of
+// This file checks results and is never the product: only tests/, the smoke check of
 // __graft_entry__.py and the cpu_baseline / reference leg of bench.py load it.
 // It restates, on the CPU and in plain C++17 (`unsigned __int128`), the
 // algorithms of the reference evaluator pdroalves/aoa (aoa-ntt = library

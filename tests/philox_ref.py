@@ -1,6 +1,6 @@
 """Host restatement of Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011) and
-of the device samplers' output rules, used as the checker for
-aoa_sample_uniform / aoa_sample_gaussian / aoa_sample_ternary."""
+of the device samplers' output rules: the tests compare
+aoa_sample_uniform / aoa_sample_gaussian / aoa_sample_ternary against it."""
 import numpy as np
 
 M0, M1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
