@@ -469,3 +469,37 @@ def test_tensor_core_and_cuda_core_conversions_agree(ref_table):
         res.append(outs)
     for x, y in zip(res[0], res[1]):
         assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+
+
+@pytest.mark.parametrize("bits", [33, 34, 40, 61, 62])
+def test_hmult_prime_sizes_bit_exact(bits):
+    """Per-call and batched HMult + relinearise + rescale at prime sizes on
+    both sides of every arithmetic switch: Montgomery products below 2^33,
+    Barrett from 2^33 (funnel-shift quotient), the one-reduction cross term up
+    to 61 bits, two reductions at 62 bits, lazy transforms below 2^61."""
+    require_gpu()
+    ps = oracle.gen_ntt_primes(bits, 1 << 13, 11)
+    Q, B = ps[:5], ps[5:]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    keys = make_keys(o, seed=bits)
+    evk = aoa.SwitchKey(ctx, *keys["evk"])
+    rng = np.random.default_rng(bits)
+    N, k = E.N, E.k
+    pairs = [(_rand_ct(rng, Q, N, k), _rand_ct(rng, Q, N, k)) for _ in range(3)]
+    # all-(q - 1) residues for the first pair: the largest products
+    full = tuple(np.array([[q - 1] * N for q in Q], dtype=np.uint64) for _ in range(2))
+    pairs[0] = (full, full)
+    sa, sb = 1 << 30, 1 << 31
+    cts = [(aoa.Ciphertext.from_residues(ctx, *a, slots=8, scale=sa, domain=aoa.AOA_NTT),
+            aoa.Ciphertext.from_residues(ctx, *b, slots=8, scale=sb, domain=aoa.AOA_NTT)) for a, b in pairs]
+    outs = [aoa.Ciphertext(ctx) for _ in pairs]
+    aoa.ckks_mul_batch(ctx, outs, [c[0] for c in cts], [c[1] for c in cts], evk)
+    single = aoa.Ciphertext(ctx)
+    aoa.ckks_mul(ctx, single, cts[1][0], cts[1][1], evk)
+    for z, (a, b) in enumerate(pairs):
+        w0, w1, _ = o.hmult(a, b, keys["evk"], k - 1, sa, sb, rescale=True, a_state=ST_NTT, b_state=ST_NTT)
+        g0, g1 = outs[z].download(nlimbs=k - 1)
+        assert np.array_equal(g0, w0[:k - 1]) and np.array_equal(g1, w1[:k - 1]), z
+        if z == 1:
+            s0, s1 = single.download(nlimbs=k - 1)
+            assert np.array_equal(s0, w0[:k - 1]) and np.array_equal(s1, w1[:k - 1])
