@@ -300,9 +300,8 @@ int aoa_engine_destroy(aoa_engine* h) {
 }
 
 // Launch-shape knobs of the engine's kernels (the reference fixes its kernel
-// shapes at compile time): "ntt_chunk_bytes" (limbs per transform launch
-// pair, kept within L2) and "ntt_waves" (transform CTAs per pass, in resident
-// waves).  Set before the engine is used from several streams at once.
+// shapes at compile time); names, ranges and defaults in include/aoa_ckks.h.
+// Set before the engine is used from several streams at once.
 int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   if (!h || !knob) return fail(AOA_ERR_BAD_PARAM, "null argument");
   const std::string k(knob);

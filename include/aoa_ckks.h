@@ -92,14 +92,16 @@ int aoa_engine_create(const aoa_params* params, aoa_engine** out);
 int aoa_engine_destroy(aoa_engine* e);
 /* Launch-shape knobs, no reference counterpart (its kernel shapes are
  * compile-time constants): "ntt_chunk_bytes" (bytes of limbs per transform
- * launch pair, default 1 GiB),
+ * launch pair, default 4 GiB),
  * "ntt_waves" (transform CTAs per pass in resident waves, default 1),
- * "ntt_waves_large" (the same for launches of at least 1536 limbs),
+ * "ntt_waves_large" (the same for launches of at least 1536 limbs, default 8),
  * "ntt_split" (log2 C - floor(log2 N / 2) of the R x C transform split,
- * -2..2), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width and
- * row-pass tile height = widest >> div, 0..2), "ntt_cols_kind" (0 CTA-wide
- * exchange, 1 warp-owned columns), "fuse" (bit mask of fused transform
- * ends: 1 out-of-place inverse, 2 key products, 4 key-switch combine) and
+ * -2..2, default 0), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width
+ * and row-pass tile height = widest >> div, 0..2, defaults 0 / 1),
+ * "ntt_cols_kind" (0 CTA-wide exchange, 1 warp-owned columns; default 0),
+ * "fuse" (bit mask of fused transform ends: 1 out-of-place inverse, 2 key
+ * products, 4 key-switch combine; default 1), "batch_streams" (1 or 2
+ * streams for a batched HMult group of 8 or more; default 2) and
  * "conv_tensor_cores"
  * (0/1: basis conversion on the int8 tensor cores where it applies).      */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
