@@ -145,7 +145,27 @@ __device__ __forceinline__ void fwd_high_s(uint64_t (&v)[Sub<LOG_S>::E], uint32_
   }
 }
 
-template <int LOG_S, bool LAZY>
+// Low-digit twiddle of level lvl = LOG_S - 1 - i for digit hi and group s:
+// natural table order 2^lvl + hi 2^(lvl - HI) + s, or, with PERM, the order
+// 2^lvl + s 2^HI + hi, in which the lanes of one s read consecutive entries
+// (conflict-free when a warp's lanes hold different hi).
+template <int LOG_S, bool PERM>
+__device__ __forceinline__ int low_tw_index(int i, uint32_t hi, int s) {
+  using D = Sub<LOG_S>;
+  return PERM ? (1 << (LOG_S - 1 - i)) + (s << D::HI) + (int)hi
+              : (1 << (LOG_S - 1 - i)) + ((int)hi << (D::LO - 1 - i)) + s;
+}
+
+// position of natural twiddle entry e in the PERM order
+template <int LOG_S>
+__device__ __forceinline__ int low_tw_perm(int e) {
+  using D = Sub<LOG_S>;
+  if (e < (1 << D::HI)) return e;
+  const int lvl = 31 - __clz(e), sh = lvl - D::HI, off = e - (1 << lvl);
+  return (1 << lvl) + ((off & ((1 << sh) - 1)) << D::HI) + (off >> sh);
+}
+
+template <int LOG_S, bool LAZY, bool PERM = false>
 __device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t tw, uint32_t hi, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
@@ -154,7 +174,7 @@ __device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      const ShoupW w = ldsw(tw + 16 * ((1 << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + (l >> (i + 1))));
+      const ShoupW w = ldsw(tw + 16 * low_tw_index<LOG_S, PERM>(i, hi, l >> (i + 1)));
       Bf<LAZY>::ct(u[l], u[l + span], w, q, ((D::HI + D::LO - 1 - i) & 1) == 0);
     }
   }
@@ -162,7 +182,7 @@ __device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t
 
 // ---- inverse (Gentleman-Sande) -------------------------------------------
 
-template <int LOG_S, bool LAZY>
+template <int LOG_S, bool LAZY, bool PERM = false>
 __device__ __forceinline__ void inv_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t itw, uint32_t hi, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
@@ -171,7 +191,7 @@ __device__ __forceinline__ void inv_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t
 #pragma unroll
     for (int l = 0; l < D::L; l++) {
       if (l & span) continue;
-      const ShoupW w = ldsw(itw + 16 * ((1 << (LOG_S - 1 - i)) + (hi << (D::LO - 1 - i)) + (l >> (i + 1))));
+      const ShoupW w = ldsw(itw + 16 * low_tw_index<LOG_S, PERM>(i, hi, l >> (i + 1)));
       Bf<LAZY>::gs(u[l], u[l + span], w, q);
     }
   }
@@ -462,9 +482,11 @@ ntt_cols(NttBatch b) {
 // The same column transforms as ntt_cols, with every column's T threads in
 // one warp (a warp holds 32 / T whole columns), so the exchange between the
 // two digit rounds needs only the warp: no CTA barrier inside an item.  A
-// producer warp streams the tiles (and the prime's twiddles when they change)
-// into two buffers through full / empty mbarrier pairs; compute warps wait
-// only for their buffer.  Row r of a tile sits at word
+// producer warp streams the tiles (and the prime's twiddles when they change,
+// entry by entry into the order low_tw_perm gives, so that the lanes of a
+// warp, which hold different low digits, read consecutive twiddles) into two
+// buffers through full / empty mbarrier pairs; compute warps wait only for
+// their buffer.  Row r of a tile sits at word
 //   P(r) = (W + 2) r + CW (k mod M) + 16 (k div M),  k = r >> (LO + G - 1),
 // M = 16 / CW: rows start 16-byte aligned and, for both digit access patterns
 // (rows (h << LO) + t and ((t G + g) << LO) + l over a warp's T lanes and CW
@@ -534,8 +556,11 @@ ntt_cols_wo(NttBatch b) {
                                    : b.data + ((long)p * b.poly_stride + limb) * N) + (long)blockIdx.x * W;
       for (int r = lane; r < D::S; r += 32)
         bulk_g2s(sbuf + (bi * WORDS + Tl::row(r)) * 8, src + r * C, W * 8, &full[bi]);
-      if (new_tw && lane == 0)
-        bulk_g2s(smem_u32(tws + bi * D::S), (FWD ? b.tw : b.itw) + (long)prime * N, D::S * 16, &full[bi]);
+      if (new_tw) {                       // one 16-byte copy per entry, into the PERM order
+        const ShoupW* tsrc = (FWD ? b.tw : b.itw) + (long)prime * N;
+        for (int e = lane; e < D::S; e += 32)
+          bulk_g2s(smem_u32(tws + bi * D::S + low_tw_perm<LOG_R>(e)), tsrc + e, 16, &full[bi]);
+      }
       issued = it + 1;
     }
     if (!ok && lane == 0) atomicOr(b.err, kErrWaitTimeout);
@@ -573,7 +598,7 @@ ntt_cols_wo(NttBatch b) {
         uint64_t u[D::L];
 #pragma unroll
         for (int l = 0; l < D::L; l++) u[l] = lds64(sm + Tl::row((hi << D::LO) + l) * 8);
-        fwd_low_s<LOG_R, true>(u, stw, hi, q);
+        fwd_low_s<LOG_R, true, true>(u, stw, hi, q);
 #pragma unroll
         for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
       }
@@ -585,7 +610,7 @@ ntt_cols_wo(NttBatch b) {
         uint64_t u[D::L];
 #pragma unroll
         for (int l = 0; l < D::L; l++) u[l] = lds64(sm + Tl::row((hi << D::LO) + l) * 8);
-        inv_low_s<LOG_R, true>(u, stw, hi, q);
+        inv_low_s<LOG_R, true, true>(u, stw, hi, q);
 #pragma unroll
         for (int l = 0; l < D::L; l++) sts64(sm + Tl::row((hi << D::LO) + l) * 8, u[l]);
       }
