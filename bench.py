@@ -94,6 +94,16 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def issue_roofline(issue, clk, sms):
+    """The transform against the instruction issue peak: sms x 4 warp
+    instructions per SM clock, at the median SM clock of the timed region."""
+    if not issue:
+        return None
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    peak = sms * 4 * mhz * 1e6
+    return dict(issue, peak_per_s=peak, sm_mhz=mhz, frac=issue["achieved_per_s"] / peak)
+
+
 def dist_setup():
     from aoa_b200.replicas import ranks
     return ranks()
@@ -540,12 +550,20 @@ def main():
     achieved = algo_bytes / (fwd_ms / 1000.0) / 1e9
     peak, peak_src = measured_peaks()
     traffic = None
+    issue = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
             tj = json.load(f)
         if "ntt_fwd_bytes_per_coef" in tj:
             traffic = tj["ntt_fwd_bytes_per_coef"] * npolys * K * N
+        if "ntt_fwd_warp_instructions_per_limb" in tj:
+            # the transform is bound by integer issue: the same launch against
+            # the SMs' instruction issue peak (4 schedulers x 1 warp instruction
+            # per clock per SM), at the SM clock sampled during the timed region
+            wi = tj["ntt_fwd_warp_instructions_per_limb"] * npolys * K
+            issue = {"warp_instructions": wi, "achieved_per_s": wi / (fwd_ms / 1000.0),
+                     "source": "instructions per limb from the ncu capture in profiles/ntt_n65536.md"}
     del buf
 
     # ---- DGT variant: transform rate and per-call HMult on a DGT context -----------
@@ -744,6 +762,7 @@ def main():
             "roofline": {"kernel": "ntt forward (column + row kernel pair), N=2^16", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_src, "algorithmic_bytes": algo_bytes, "traffic": traffic},
+            "issue_roofline": issue_roofline(issue, clk, torch.cuda.get_device_properties(local).multi_processor_count),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "h2d_copy_gbs": h2d_gbs, "h2d_bound_ops_per_s": B * h2d_gbs * 1e9 / h2d,
                     "path": "aoa_ct_upload (pinned) + aoa_hmult_batch + aoa_ct_download_async (coefficients) "
