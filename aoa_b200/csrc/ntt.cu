@@ -398,14 +398,15 @@ ntt_cols(NttBatch b) {
     const int limb = j / b.npolys, p = j % b.npolys;
     return b.data + ((long)p * b.poly_stride + limb) * N + (long)blockIdx.x * W;
   };
-  auto issue = [&](int j, int bi) {        // warp 0: S row segments of W words
-    if (threadIdx.x < 32) {
-      if (threadIdx.x == 0) mbar_expect_tx(&mbar[bi], TILE * 8);
-      __syncwarp();
-      const uint64_t* src = src_of(j);
-      for (int r = threadIdx.x; r < D::S; r += 32)
-        bulk_g2s(sbuf + (bi * TILE + sig(r) * W) * 8, src + r * C, W * 8, &mbar[bi]);
-    }
+  // S row segments of W words, spread over all threads (one each when
+  // S = blockDim), so no warp lags behind the others into the next barrier;
+  // a copy may complete before thread 0's expect_tx (the transaction count
+  // may go below zero until then)
+  auto issue = [&](int j, int bi) {
+    if (threadIdx.x == 0) mbar_expect_tx(&mbar[bi], TILE * 8);
+    const uint64_t* src = src_of(j);
+    for (int r = threadIdx.x; r < D::S; r += blockDim.x)
+      bulk_g2s(sbuf + (bi * TILE + sig(r) * W) * 8, src + r * C, W * 8, &mbar[bi]);
   };
   int cur_limb = -1, tb = 1;
   const int j_lo = (int)((long)blockIdx.y * b.nitems / G), j_hi = (int)((long)(blockIdx.y + 1) * b.nitems / G);
