@@ -268,6 +268,10 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   // this thread's A rows / input pairs, and its prefetched inputs
   const int ar = threadIdx.x % kTcRows, ap = threadIdx.x / kTcRows;
   uint64_t xa[kTcPairs], xb[kTcPairs];
+  // the rescale modes' own-limb word of this thread's epilogue row, fetched
+  // with the inputs so that its latency is hidden too
+  uint64_t dv_next = 0;
+  const int erow = (warp % 4) * 32 + lane;
   auto load_inputs = [&](long tile) {
     const long poly = tile >> tile_shift, c0 = (tile & ((1L << tile_shift) - 1)) * kTcRows;
     const uint64_t* in = a.in + poly * a.in_poly_stride + c0 + ar;
@@ -277,6 +281,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       xa[m] = p < npairs ? in[(long)(2 * p) * N] : 0;
       xb[m] = 2 * p + 1 < a.nin ? in[(long)(2 * p + 1) * N] : 0;
     }
+    if (MODE >= kRescaleTop) dv_next = a.d[poly * a.d_poly_stride + c0 + erow];
   };
   if (blockIdx.x < ntiles) load_inputs(blockIdx.x);
   bool ok = __syncthreads_and(mbar_wait(&mbar[0], 0));
@@ -311,6 +316,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       tc_commit(&mbar[1]);
     }
     in_flight = true;
+    const uint64_t dv_cur = dv_next;                       // this tile's word, loaded with its inputs
     if (tile + gridDim.x < ntiles) load_inputs(tile + gridDim.x);   // overlaps the MMAs and the epilogue
     ok = !__syncthreads_or(!mbar_wait(&mbar[1], phase));
     if (!ok) break;
@@ -323,8 +329,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     const long c = c0 + g * 32 + lane;
     const uint32_t t_lane = tmem + ((uint32_t)(g * 32) << 16);
     uint64_t* out = a.out + poly * a.out_poly_stride + c;
-    uint64_t dv = 0;
-    if (MODE >= kRescaleTop) dv = a.d[poly * a.d_poly_stride + c];
+    const uint64_t dv = dv_cur;
     uint32_t v[16];
     if (MODE == kRescaleFused) {
       const int l = j_end - 1;                 // outputs 0..l-1 from c_l (j_first = 0)
