@@ -205,7 +205,12 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 // and W_1 = sum_t T_(4+t) 2^(8t) (< 2^49 each) come from 32 x 32 -> 64-bit
 // multiply-adds; x = W_0 + W_1 2^32 < 2^81 has a high word below 2^17, so
 // one Barrett step (s >= 32) reduces it.
-__device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const PrimeConst& P) {
+// an output prime's constants, staged in shared memory once per CTA
+struct TcOut {
+  uint64_t q, mu, sh, one_sh;
+};
+
+__device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const TcOut& c, const PrimeConst* P) {
   uint64_t W0 = v[0], W1 = v[4];
   asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(W0) : "r"(v[1]));
   asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(W1) : "r"(v[5]));
@@ -219,8 +224,14 @@ __device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const PrimeCon
       : "=r"(r1), "=r"(r2)
       : "r"((uint32_t)(W0 >> 32)), "r"((uint32_t)W1), "r"((uint32_t)(W1 >> 32)));
   const uint64_t lo = ((uint64_t)r1 << 32) | (uint32_t)W0;
-  if (P.bar_sh) return barrett_wide(lo, r2, P.q, P.bar_mu, (uint32_t)P.bar_sh);
-  return reduce128(lo, r2, P);
+  if (c.sh) return barrett_wide(lo, r2, c.q, c.mu, (uint32_t)c.sh);
+  return reduce128(lo, r2, *P);
+}
+
+// x mod q_out for x < p (another prime): one subtraction when p < 2 q_out
+__device__ __forceinline__ uint64_t tc_cross(uint64_t x, uint64_t p, const TcOut& c) {
+  if (p < 2 * c.q) return x >= c.q ? x - c.q : x;
+  return shoup(x, 1, c.one_sh, c.q);
 }
 
 // Persistent: CTA b handles tiles b, b + grid, ...  Per tile: the inputs (loaded
@@ -236,6 +247,9 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   extern __shared__ __align__(1024) uint8_t tcs[];
   __shared__ __align__(8) uint64_t mbar[2];                // [0] image loaded, [1] MMA done
   __shared__ uint32_t tmem_slot;
+  __shared__ ShoupW s_zc[32];                              // input scalings
+  __shared__ uint64_t s_qin[32];                           // input primes
+  __shared__ TcOut s_out[32];                              // output primes' constants
   uint8_t* As = tcs;
   uint8_t* Bs = tcs + kTcA;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -249,6 +263,17 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
     mbar_init_fence();
+  }
+  if (threadIdx.x < 32) {
+    const int i = threadIdx.x;
+    if (i < a.nin) {
+      s_zc[i] = a.zc[i];
+      s_qin[i] = a.pc[a.in_prime0 + i].q;
+    }
+    if (i < j_end) {
+      const PrimeConst& P = a.pc[a.out_prime0 + i];
+      s_out[i] = TcOut{P.q, P.bar_mu, P.bar_sh, P.one_sh};
+    }
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -298,8 +323,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       const int p = ap + m * (kTcThreads / kTcRows);
       if (p < npairs) {
         const int i0 = 2 * p, i1 = 2 * p + 1;
-        const uint64_t z0 = shoup(xa[m], a.zc[i0], a.pc[a.in_prime0 + i0].q);
-        const uint64_t z1 = i1 < a.nin ? shoup(xb[m], a.zc[i1], a.pc[a.in_prime0 + i1].q) : 0;
+        const uint64_t z0 = shoup(xa[m], s_zc[i0], s_qin[i0]);
+        const uint64_t z1 = i1 < a.nin ? shoup(xb[m], s_zc[i1], s_qin[i1]) : 0;
         *(uint4*)(As + (size_t)p * (kTcRows * 16) + ar * 16) =
             make_uint4((uint32_t)z0, (uint32_t)(z0 >> 32), (uint32_t)z1, (uint32_t)(z1 >> 32));
       }
@@ -334,10 +359,11 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     if (MODE == kRescaleFused) {
       const int l = j_end - 1;                 // outputs 0..l-1 from c_l (j_first = 0)
       tc_ld16(t_lane + (l & ~1) * 8, v);
-      const PrimeConst& Pl = a.pc[a.out_prime0 + l];
+      const TcOut cpl = s_out[l];
+      const PrimeConst* Pl = a.pc + a.out_prime0 + l;
       // the rescale modes read the table with B^-1 folded in: sums are conv * B^-1
-      const uint64_t sl = (l & 1) ? tc_combine(v + 8, Pl) : tc_combine(v, Pl);
-      const uint64_t cl = sub_mod(dv, sl, Pl.q);
+      const uint64_t sl = (l & 1) ? tc_combine(v + 8, cpl, Pl) : tc_combine(v, cpl, Pl);
+      const uint64_t cl = sub_mod(dv, sl, cpl.q);
       const int per = (((l + 3) / 4) + 1) & ~1;
       const int jb = par * per, je = min(l, jb + per);
       for (int j = jb; j < je; j += 2) {
@@ -345,8 +371,9 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
 #pragma unroll
         for (int u = 0; u < 2; u++) {
           if (j + u < je) {
-            const PrimeConst& P = a.pc[a.out_prime0 + j + u];
-            out[(long)(j + u - a.out_shift) * N] = add_mod(tc_combine(v + 8 * u, P), cross_mod(cl, Pl.q, P), P.q);
+            const TcOut cp = s_out[j + u];
+            out[(long)(j + u - a.out_shift) * N] =
+                add_mod(tc_combine(v + 8 * u, cp, a.pc + a.out_prime0 + j + u), tc_cross(cl, cpl.q, cp), cp.q);
           }
         }
       }
@@ -360,15 +387,15 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
         for (int u = 0; u < 2; u++) {
           const int o = jj + u;
           if (o >= jb && o < je) {
-            const PrimeConst& P = a.pc[a.out_prime0 + o];
-            uint64_t r = tc_combine(v + 8 * u, P);
+            const TcOut cp = s_out[o];
+            uint64_t r = tc_combine(v + 8 * u, cp, a.pc + a.out_prime0 + o);
             if (MODE == kModDown) {
               const uint64_t x = a.x[poly * a.x_poly_stride + (long)(o - a.x_shift) * N + c];
-              r = shoup(sub_mod(x, r, P.q), a.binv[o], P.q);
+              r = shoup(sub_mod(x, r, cp.q), a.binv[o], cp.q);
             } else if (MODE == kRescaleTop) {
-              r = sub_mod(dv, r, P.q);                             // folded table: r = conv * B^-1
+              r = sub_mod(dv, r, cp.q);                            // folded table: r = conv * B^-1
             } else if (MODE == kRescaleY) {
-              r = add_mod(r, shoup(dv, 1, P.one_sh, P.q), P.q);    // folded table: r = conv * B^-1
+              r = add_mod(r, shoup(dv, 1, cp.one_sh, cp.q), cp.q); // folded table: r = conv * B^-1
             }
             out[(long)(o - a.out_shift) * N] = r;
           }
