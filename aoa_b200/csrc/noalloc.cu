@@ -16,15 +16,22 @@
 //    loads the library until the process exits;
 //  - the parameter set must need at most that much workspace, otherwise the
 //    call fails with AOA_ERR_BAD_PARAM and says how much it would need;
-//  - the array's device address is looked up once per device on the first call
-//    made on that device (with the engine's device current); make that first
-//    call before any stream capture;
+//  - the array's device address is looked up once per CUDA context on the
+//    first call made in that context (with the engine's device current) and
+//    cached under the context's handle, so a caller that switches between the
+//    primary context and contexts of its own gets the address that belongs to
+//    the current one; make that first call before any stream capture.  After
+//    cudaDeviceReset the next call looks the address up again only if the new
+//    primary context has a new handle, so do not reset a device between calls;
 //  - every call on a device shares the one array and leaves its contents
 //    behind: calls whose work overlaps on the GPU (other streams, other
 //    contexts, other threads) race on it and must be serialised by the caller;
 //  - no part of the scratch has to start at zero: the pipeline writes every
 //    scratch word it reads earlier in the same call.
+#include <cuda.h>   // CUcontext and CUresult (types only: the driver call is fetched through the runtime)
+
 #include <mutex>
+#include <vector>
 
 #include "aoa_internal.h"
 
@@ -43,22 +50,49 @@ constexpr size_t kScratchBytes = kScratchWords * sizeof(uint64_t);   // 32 MiB
 
 static __device__ __align__(256) uint64_t g_noalloc_scratch[kScratchWords];
 
-constexpr int kMaxDevices = 64;
+struct ScratchSlot {
+  CUcontext ctx;
+  uint64_t* addr;
+};
 std::mutex g_setup_mu;
-uint64_t* g_scratch_addr[kMaxDevices] = {};
+std::vector<ScratchSlot> g_slots;     // one entry per CUDA context that has made a call
 
-// Device address of the scratch array on `device` (which must be current).
-uint64_t* scratch_on(int device) {
-  if (device < 0 || device >= kMaxDevices) throw AoaError(AOA_ERR_BAD_PARAM, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_addr[device]) {
+// The calling thread's current CUDA context (cuCtxGetCurrent, fetched once
+// through the runtime so the library needs no link against libcuda).
+CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = [] {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      throw AoaError(AOA_ERR_CUDA, std::string("no-alloc scratch address lookup failed: ") + cudaGetErrorString(e));
-    g_scratch_addr[device] = (uint64_t*)p;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (Fn) nullptr;
+    return (Fn)p;
+  }();
+  if (!fn) throw AoaError(AOA_ERR_CUDA, "cuCtxGetCurrent is not available from the driver");
+  CUcontext ctx = nullptr;
+  if (fn(&ctx) != CUDA_SUCCESS) throw AoaError(AOA_ERR_CUDA, "cuCtxGetCurrent failed");
+  return ctx;
+}
+
+// Device address of the scratch array in the current context (whose device
+// is the engine's, `device`).
+uint64_t* scratch_here(int device) {
+  CUcontext ctx = current_context();
+  if (!ctx) {                         // a thread without a current context: bind the device's primary one
+    AOA_CUDA(cudaSetDevice(device));
+    ctx = current_context();
+    if (!ctx) throw AoaError(AOA_ERR_CUDA, "no current CUDA context");
   }
-  return g_scratch_addr[device];
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  for (const ScratchSlot& s : g_slots)
+    if (s.ctx == ctx) return s.addr;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    throw AoaError(AOA_ERR_CUDA, std::string("no-alloc scratch address lookup failed: ") + cudaGetErrorString(e));
+  g_slots.push_back({ctx, (uint64_t*)p});
+  return (uint64_t*)p;
 }
 
 }  // namespace
@@ -78,7 +112,7 @@ int aoa_hmult_relin_rescale_noalloc(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* 
     AOA_CUDA(cudaGetDevice(&cur));
     if (cur != E.device)
       throw AoaError(AOA_ERR_BAD_PARAM, "make the engine's device current before calling the no-alloc HMult");
-    hmult_with_scratch(c->c, out, a, b, evk, true, scratch_on(cur));
+    hmult_with_scratch(c->c, out, a, b, evk, true, scratch_here(cur));
   });
 }
 

@@ -12,8 +12,9 @@
 //   body: 2 polys x nlimbs x N residues, u64
 // A ciphertext carries its live limbs 0..level in its current domain (no
 // transform on either side); a switching key carries both (k + kl)-limb polys
-// in its transform domain.  Reading checks the magic, kind, ring, fingerprint
-// and length, and rejects anything else.
+// in its transform domain.  Reading checks the magic, kind, ring, fingerprint,
+// length, level and slot count, and that every residue is below its prime,
+// and rejects anything else.
 #include <cstring>
 
 #include "aoa_internal.h"
@@ -77,6 +78,25 @@ WireHeader read_header(const Engine& E, const uint8_t* buf, size_t len, uint32_t
   return h;
 }
 
+// Every word of the body must be a canonical residue of its limb's prime:
+// the kernels' lazy bounds assume inputs below q, so a corrupted or foreign
+// buffer is rejected here instead of giving wrong results later.
+void check_residues(const Engine& E, const uint8_t* body, int npolys, int nlimbs) {
+  const size_t N = (size_t)E.N;
+  for (int p = 0; p < npolys; p++)
+    for (int i = 0; i < nlimbs; i++) {
+      const uint64_t q = E.primes[i];
+      const uint8_t* limb = body + ((size_t)p * nlimbs + i) * N * 8;
+      for (size_t j = 0; j < N; j++) {
+        uint64_t v;
+        memcpy(&v, limb + j * 8, 8);
+        if (v >= q)
+          throw AoaError(AOA_ERR_BAD_PARAM, "wire buffer holds a residue >= its prime (poly " + std::to_string(p) +
+                                                ", limb " + std::to_string(i) + ", word " + std::to_string(j) + ")");
+      }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -116,6 +136,9 @@ int aoa_ct_deserialize(aoa_ctx* c, aoa_ct* ct, const uint8_t* buf, size_t len) {
     const WireHeader h = read_header(E, buf, len, kKindCt);
     if (h.nlimbs < 1 || h.nlimbs > (uint32_t)E.k || h.level != (int32_t)h.nlimbs - 1)
       throw AoaError(AOA_ERR_BAD_PARAM, "wire ciphertext has a bad level");
+    if (h.slots < 0 || h.slots > E.N / 2 || (h.slots & (h.slots - 1)) != 0)
+      throw AoaError(AOA_ERR_BAD_PARAM, "wire ciphertext has a bad slot count (0 or a power of two <= N/2)");
+    check_residues(E, buf + sizeof h, 2, (int)h.nlimbs);
     const size_t poly = (size_t)h.nlimbs * E.N * 8;
     for (int p = 0; p < 2; p++)
       AOA_CUDA(cudaMemcpyAsync(ct->d + (size_t)p * E.k * E.N, buf + sizeof h + p * poly, poly, cudaMemcpyHostToDevice,
@@ -159,6 +182,7 @@ int aoa_swk_deserialize(aoa_ctx* c, const uint8_t* buf, size_t len, aoa_swk** ou
       throw AoaError(AOA_ERR_BAD_PARAM, "wire key has a bad shape or domain");
     if (h.domain != c->c.transform)
       throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
+    check_residues(E, buf + sizeof h, 2, E.nprimes);
     aoa_swk* k = new aoa_swk();
     if (cudaMallocAsync(&k->d, len - sizeof h, c->c.stream) != cudaSuccess) {
       cudaGetLastError();

@@ -39,6 +39,13 @@ def primes():
     return params.ntt_primes(60, 2 << LOG_N, K + KL)
 
 
+def oracle_primes():
+    """The same primes from the oracle's own prime search (the reference arm
+    loads no library of the product)."""
+    import oracle
+    return oracle.gen_ntt_primes(60, 2 << LOG_N, K + KL)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -105,8 +112,16 @@ def issue_roofline(issue, clk, sms):
 
 
 def dist_setup():
-    from aoa_b200.replicas import ranks
-    return ranks()
+    """(world_size, rank, local_rank) from the launcher's environment."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def workload_config(batch):
+    return {"workload": "hmult_relin_rescale", "log_n": LOG_N, "q_limbs": K, "special_limbs": KL,
+            "dnum": 1, "level": K - 1, "prime_bits": 60, "scale_bits": SCALE_BITS,
+            "batch_per_gpu": batch, "parallelism": "replicas",
+            "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % batch}
 
 
 def run_reference(args, world, rank):
@@ -117,7 +132,7 @@ def run_reference(args, world, rank):
     from oracle import Oracle
     threads = os.cpu_count() or 1
     oracle.lib().oc_set_threads(threads)
-    ps = primes()
+    ps = oracle_primes()
     o = Oracle(1 << LOG_N, ps[:K], ps[K:])
     rng = np.random.default_rng(1)
     N = 1 << LOG_N
@@ -135,10 +150,11 @@ def run_reference(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic",
-            "config": {"workload": "hmult_relin_rescale", "log_n": LOG_N, "q_limbs": K, "special_limbs": KL,
-                       "dnum": 1, "level": K - 1, "prime_bits": 60, "batch": 1},
+            "config": workload_config(args.batch),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": "1 HMult+relin+rescale per step (reference op sequence, oracle/ckks_oracle.cpp)"},
+                             "sample": "1 of the step's %d HMult+relin+rescale per timed step (bounded sample; "
+                                       "reference op sequence restated in oracle/ckks_oracle.cpp, OpenMP)"
+                                       % args.batch},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -563,7 +579,7 @@ def main():
             # per clock per SM), at the SM clock sampled during the timed region
             wi = tj["ntt_fwd_warp_instructions_per_limb"] * npolys * K
             issue = {"warp_instructions": wi, "achieved_per_s": wi / (fwd_ms / 1000.0),
-                     "source": "instructions per limb from the ncu capture in profiles/ntt_n65536.md"}
+                     "source": "warp instructions per limb from an ncu capture of the same forward transform"}
     del buf
 
     # ---- DGT variant: transform rate and per-call HMult on a DGT context -----------
@@ -729,12 +745,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "hmult_relin_rescale", "log_n": LOG_N, "q_limbs": K, "special_limbs": KL,
-                       "dnum": 1, "level": K - 1, "prime_bits": 60, "scale_bits": SCALE_BITS,
-                       "batch_per_gpu": B, "input_domain": "transform (state left by the previous HMult)",
-                       "parallelism": "replicas",
-                       "l2": "inputs exceed L2 (60 MiB per ciphertext pair, %d pairs)" % B,
-                       "transform_tuning": tuning},
+            "config": dict(workload_config(B), input_domain="transform (state left by the previous HMult)",
+                           transform_tuning=tuning),
             "accuracy": acc,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "single_op_ops_per_s": float(1000.0 / np.mean(lat))},
@@ -743,6 +755,11 @@ def main():
                                "speedup_of_value": value / (world * B / (plain_ms / 1000.0))},
             "pipeline_per_call_ops_per_s": world * B / (percall_ms / 1000.0),
             "batched_coefficient_inputs_ops_per_s": world * B / (coef_ms / 1000.0),
+            "speedup_vs_plain": {
+                "transform_domain_inputs": value / (world * B / (plain_ms / 1000.0)),
+                "coefficient_inputs": plain_ms / coef_ms,
+                "note": "plain path: reference op sequence with coefficient inputs; batched path with the "
+                        "inputs its previous HMult leaves (transform domain) and with the same coefficient inputs"},
             "ntt": {"fwd_ms": fwd_ms, "inv_ms": inv_ms, "polys": npolys, "limbs": K,
                     "fwd_gbs": achieved, "inv_gbs": algo_bytes / (inv_ms / 1000.0) / 1e9,
                     "hbm_frac": achieved / peak, "inverse_of_forward_is_identity": roundtrip_ok,

@@ -259,9 +259,11 @@ int aoa_hmult_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk
  * as aoa_hmult_relin_rescale, with their workspace in a fixed 32 MiB device
  * array built into the library (held by every device that loads it until the
  * process exits).  Parameter sets needing more workspace fail with
- * AOA_ERR_BAD_PARAM.  The first call on a device looks the array up (make it
- * with the engine's device current and before any stream capture).  All calls
- * share the one array: calls whose work overlaps on the GPU race.            */
+ * AOA_ERR_BAD_PARAM.  The first call in a CUDA context looks the array's
+ * address up and caches it under that context (make it with the engine's
+ * device current and before any stream capture; do not reset the device
+ * between calls).  All calls share the one array: calls whose work overlaps
+ * on the GPU race.                                                           */
 int aoa_hmult_relin_rescale_noalloc(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
 /* ckks_rescale (ckks.cpp:220-230) */
 int aoa_rescale(aoa_ctx* c, aoa_ct* ct);

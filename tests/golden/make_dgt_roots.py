@@ -12,7 +12,7 @@ generator (PROOTS) and its roots for every tabulated size.  INVNTHROOT is not
 stored: it is the unique inverse of r, which the reference asserts.  It runs
 only where the reference checkout exists; the fixture it wrote is committed.
 
-Usage: python tests/golden/make_dgt_roots.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_dgt_roots.py REFERENCE_ROOT
 """
 import json
 import os
@@ -23,7 +23,9 @@ KEEP = {63: 1, 55: 40, 52: 30, 48: 40, 45: 40}
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s REFERENCE_ROOT (the pdroalves/aoa checkout)" % sys.argv[0])
+    root = sys.argv[1]
     src = open(os.path.join(root, "aoa-dgt/src/arithmetic/coprimes.cu")).read()
     i0 = src.index("std::map<uint64_t, std::map<int, GaussianInteger>> NTHROOT")
     i1 = src.index("std::map<uint64_t, std::map<int, GaussianInteger>> INVNTHROOT")

@@ -10,7 +10,7 @@ needs these numbers.  This script reads the table as text and writes a small
 JSON fixture (a prefix of each bucket plus the generators); it runs only where
 the reference checkout exists, the fixture it wrote is committed.
 
-Usage: python tests/golden/make_reference_primes.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_reference_primes.py REFERENCE_ROOT
 """
 import json
 import os
@@ -21,7 +21,9 @@ KEEP = {63: 4, 55: 128, 52: 30, 48: 64, 45: 32}
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s REFERENCE_ROOT (the pdroalves/aoa checkout)" % sys.argv[0])
+    root = sys.argv[1]
     src = open(os.path.join(root, "aoa-ntt/src/cuda/htrans/coprimes.cu")).read()
     proots = {int(a): int(b) for a, b in re.findall(r"\{\(uint64_t\)(\d+), (\d+)\}", src)}
     out = {"source": "aoa-ntt/src/cuda/htrans/coprimes.cu", "buckets": {}, "proots": {}}

@@ -57,6 +57,19 @@ def test_wire_format_round_trip_and_rejections():
     aoa2, E2, ctx2, _ = _setup(k=5, kl=2)                 # other prime set
     with pytest.raises(aoa.capi.AoaError):
         ser.ct_from_bytes(ctx2, data)
+    # a residue >= its prime (last word of poly 1, limb 2), a slot count that
+    # is not a power of two, one above N/2: each rejected with its reason
+    body = np.frombuffer(data, dtype=np.uint64, offset=64).copy()
+    body[-1] = E.q_primes[2]
+    with pytest.raises(aoa.capi.AoaError) as ei:
+        ser.ct_from_bytes(ctx, data[:64] + body.tobytes())
+    assert "residue" in str(ei.value)
+    for slots in (48, N):
+        hdr = bytearray(data[:64])
+        hdr[28:32] = int(slots).to_bytes(4, "little")     # slots field of the header
+        with pytest.raises(aoa.capi.AoaError) as ei:
+            ser.ct_from_bytes(ctx, bytes(hdr) + data[64:])
+        assert "slot" in str(ei.value)
     # a key survives the trip and relinearises exactly as before
     keys = make_keys(o, seed=4)
     evk = aoa.SwitchKey(ctx, *keys["evk"])
