@@ -53,6 +53,7 @@ SIGNATURES = {
     "aoa_ctx_create": (c_int, [c_void_p, c_void_p, vpp]),
     "aoa_ctx_destroy": (c_int, [c_void_p]),
     "aoa_ctx_sync": (c_int, [c_void_p]),
+    "aoa_ctx_wait_check": (c_int, [c_void_p, c_int]),
     "aoa_ctx_stream": (c_int, [c_void_p, vpp]),
     "aoa_device_alloc": (c_int, [c_void_p, c_size_t, vpp]),
     "aoa_device_free": (c_int, [c_void_p, c_void_p]),

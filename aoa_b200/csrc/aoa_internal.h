@@ -53,6 +53,10 @@ struct Tune {
   // transform, 4 key-switch combine in the corrections' forward transform
   int fuse = 1;
   int batch_streams = 2;              // streams a large HMult batch is split over (1 or 2)
+  // polls of a kernel's bounded mbarrier waits before it gives up, sets
+  // kErrWaitTimeout in the error word and returns (aoa_ctx_sync then reports
+  // AOA_ERR_TIMEOUT); the default 2^20 polls is far beyond any healthy wait
+  int spin_limit = 1 << 20;
 };
 
 // Device copy of the basis-conversion / rescale constants.

@@ -8,7 +8,7 @@ namespace aoa {
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-constexpr int kSpinLimit = 1 << 20;     // bounded mbarrier waits
+constexpr int kSpinLimit = 1 << 20;     // bounded mbarrier waits (default; engine knob "spin_limit")
 
 __device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mb)), "r"(count) : "memory");
@@ -45,9 +45,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mb, unsigned parity) {
   return ok != 0;
 }
 
-// Waits for phase `parity` of the barrier; gives up after kSpinLimit tries.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity) {
-  for (int i = 0; i < kSpinLimit; i++)
+// Waits for phase `parity` of the barrier; gives up after `limit` tries.
+// The waits for a kernel's own work use the engine's limit (a kernel
+// argument); the drain after an expired wait, which lets copies and MMAs in
+// flight land before the CTA exits, always uses the default bound.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned parity, int limit = kSpinLimit) {
+  for (int i = 0; i < limit; i++)
     if (mbar_try_wait(mb, parity)) return true;
   return false;
 }

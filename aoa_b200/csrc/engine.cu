@@ -8,8 +8,23 @@
 #endif
 
 #include "aoa_internal.h"
+#include "async.cuh"
 
 namespace aoa {
+
+// One warp; thread 0 waits on a barrier that expects one arrival which
+// nothing makes, with `spins` polls, and records the expiry like every other
+// bounded wait of the engine (no copy or MMA targets the barrier, so nothing
+// is in flight when the kernel returns).
+__global__ void wait_check_kernel(unsigned* err, int spins) {
+  __shared__ __align__(8) uint64_t mb;
+  if (threadIdx.x == 0) {
+    mbar_init(&mb, 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  if (threadIdx.x == 0 && !mbar_wait(&mb, 0, spins)) atomicOr(err, kErrWaitTimeout);
+}
 
 static thread_local std::string g_last_error;
 static std::atomic<long> g_launches{0};
@@ -315,6 +330,8 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   else if (k == "ntt_cols_kind" && (value == 0 || value == 1)) h->e.tune.ntt_cols_kind = (int)value;
   else if (k == "batch_streams" && (value == 1 || value == 2)) h->e.tune.batch_streams = (int)value;
   else if (k == "fuse" && value >= 0 && value <= 7 && value == (int)value) h->e.tune.fuse = (int)value;
+  else if (k == "spin_limit" && value >= 0 && value <= (1 << 30) && value == (int)value)
+    h->e.tune.spin_limit = (int)value;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob or value out of range: " + k);
   return AOA_OK;
 }
@@ -333,6 +350,7 @@ int aoa_engine_tune_get(const aoa_engine* h, const char* knob, double* value) {
   else if (k == "ntt_cols_kind") *value = t.ntt_cols_kind;
   else if (k == "batch_streams") *value = t.batch_streams;
   else if (k == "fuse") *value = t.fuse;
+  else if (k == "spin_limit") *value = t.spin_limit;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob: " + k);
   return AOA_OK;
 }
@@ -383,6 +401,15 @@ int aoa_ctx_destroy(aoa_ctx* h) {
   });
   delete h;
   return st;
+}
+
+int aoa_ctx_wait_check(aoa_ctx* h, int spins) {
+  if (!h || spins < 0) return fail(AOA_ERR_BAD_PARAM, "bad argument");
+  return guarded([&] {
+    wait_check_kernel<<<1, 32, 0, h->c.stream>>>(h->c.E->d_err, spins);
+    AOA_CHECK_LAUNCH();
+    note_launch();
+  });
 }
 
 int aoa_ctx_sync(aoa_ctx* h) {

@@ -328,6 +328,7 @@ struct NttBatch {
   const uint64_t* src;     // this pass loads from src (out of place) when set
   long src_poly_stride;
   int poly_base;           // poly index of the launch's first poly within the call
+  int spin;                // polls of a bounded wait for this kernel's own copies (engine knob)
 };
 
 // Tile widths: a column-pass CTA takes W = PER_CTA >> DIV columns (at least 2,
@@ -420,7 +421,7 @@ ntt_cols(NttBatch b) {
       for (int e = threadIdx.x; e < D::S; e += blockDim.x) tws[tb * D::S + e] = tw[e];
       cur_limb = limb;
     }
-    const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
+    const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1, b.spin);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
         atomicOr(b.err, kErrWaitTimeout);
@@ -542,7 +543,7 @@ ntt_cols_wo(NttBatch b) {
     bool ok = true;
     for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
       const int bi = it & 1;
-      if (it >= 2 && !mbar_wait(&empty[bi], ((it - 2) >> 1) & 1)) {
+      if (it >= 2 && !mbar_wait(&empty[bi], ((it - 2) >> 1) & 1, b.spin)) {
         ok = false;
         break;
       }
@@ -575,7 +576,7 @@ ntt_cols_wo(NttBatch b) {
   const int w = warp * CW + lane / D::T;
   for (int j = j_lo, it = 0; j < j_hi; j++, it++) {
     const int bi = it & 1;
-    if (!mbar_wait(&full[bi], (it >> 1) & 1)) {
+    if (!mbar_wait(&full[bi], (it >> 1) & 1, b.spin)) {
       if (lane == 0) atomicOr(b.err, kErrWaitTimeout);
       return;
     }
@@ -699,7 +700,7 @@ ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
       q = b.pc[prime].q;
       cur_limb = limb;
     }
-    const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1);
+    const bool ok = mbar_wait(&mbar[bi], (it >> 1) & 1, b.spin);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
         atomicOr(b.err, kErrWaitTimeout);
@@ -986,6 +987,7 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   if (epi.mode != kEpiStore && !forward) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: epilogues are for forward transforms");
   NttBatch b;
   b.tw = T.tw; b.itw = T.itw; b.pc = T.pc; b.err = E.d_err;
+  b.spin = E.tune.spin_limit;
   b.log_n = T.log_n;
   b.log_c = T.log_n / 2 + E.tune.ntt_split;
   b.log_c = std::max(std::max(5, T.log_n - 10), std::min(std::min(10, T.log_n - 5), b.log_c));

@@ -58,6 +58,7 @@ struct ConvArgs {
   const uint8_t* tc_b;      // tensor-core image of `mat` (null: CUDA-core kernel only)
   unsigned* err;            // device error word
   int npolys;
+  int spin;                 // polls of a bounded wait for this kernel's own copies and MMAs (engine knob)
 };
 
 // Epilogue of the non-fused modes for output jj with the reduced sum r.
@@ -309,7 +310,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     if (MODE >= kRescaleTop) dv_next = a.d[poly * a.d_poly_stride + c0 + erow];
   };
   if (blockIdx.x < ntiles) load_inputs(blockIdx.x);
-  bool ok = __syncthreads_and(mbar_wait(&mbar[0], 0));
+  bool ok = __syncthreads_and(mbar_wait(&mbar[0], 0, a.spin));
   bool in_flight = false;                                  // an MMA group not yet waited for
   const uint32_t a_base = smem_u32(As), b_base = smem_u32(Bs);
   const int ksteps = (a.nin + 3) / 4;                      // 4 inputs (32 bytes) per MMA K step
@@ -343,7 +344,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
     in_flight = true;
     const uint64_t dv_cur = dv_next;                       // this tile's word, loaded with its inputs
     if (tile + gridDim.x < ntiles) load_inputs(tile + gridDim.x);   // overlaps the MMAs and the epilogue
-    ok = !__syncthreads_or(!mbar_wait(&mbar[1], phase));
+    ok = !__syncthreads_or(!mbar_wait(&mbar[1], phase, a.spin));
     if (!ok) break;
     in_flight = false;
     phase ^= 1;
@@ -425,6 +426,7 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
   if (a.tc_b && E.tune.conv_tensor_cores && a.nin <= 32 && j_end <= 32 && N % kTcRows == 0) {
     ConvArgs t = a;
     t.err = E.d_err;
+    t.spin = E.tune.spin_limit;
     t.npolys = npolys;
     const long tiles = (N / kTcRows) * npolys;
     const unsigned grid_tc = (unsigned)std::min<long>(tiles, E.num_sms);

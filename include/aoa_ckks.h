@@ -101,9 +101,13 @@ int aoa_engine_destroy(aoa_engine* e);
  * "ntt_cols_kind" (0 CTA-wide exchange, 1 warp-owned columns; default 0),
  * "fuse" (bit mask of fused transform ends: 1 out-of-place inverse, 2 key
  * products, 4 key-switch combine; default 1), "batch_streams" (1 or 2
- * streams for a batched HMult group of 8 or more; default 2) and
+ * streams for a batched HMult group of 8 or more; default 2),
  * "conv_tensor_cores"
- * (0/1: basis conversion on the int8 tensor cores where it applies).      */
+ * (0/1: basis conversion on the int8 tensor cores where it applies) and
+ * "spin_limit" (polls of the kernels' bounded mbarrier waits before they
+ * give up and report AOA_ERR_TIMEOUT at the next aoa_ctx_sync, 0..2^30;
+ * default 2^20; the drain of copies and MMAs in flight after an expired
+ * wait always uses the default bound).                                     */
 int aoa_engine_tune(aoa_engine* e, const char* knob, double value);
 /* current value of a knob (names as for aoa_engine_tune) */
 int aoa_engine_tune_get(const aoa_engine* e, const char* knob, double* value);
@@ -125,8 +129,21 @@ int aoa_engine_info(const aoa_engine* e, int* log_n, int* k, int* kl, uint64_t* 
  *     stream == NULL creates a private stream.                                 */
 int aoa_ctx_create(aoa_engine* e, void* cuda_stream, aoa_ctx** out);
 int aoa_ctx_destroy(aoa_ctx* c);
+/* Waits for the context's stream and reports device-side errors: a bounded
+ * wait that expired in any kernel of the engine since the last report gives
+ * AOA_ERR_TIMEOUT (and clears the record); the reference reports device
+ * failures through cudaCheckError(), which exits the process
+ * (include/newckks/cuda/htrans/common.h:20-29).                              */
 int aoa_ctx_sync(aoa_ctx* c);
 int aoa_ctx_stream(aoa_ctx* c, void** stream_out);
+/* Check of the failure-detection path, no reference counterpart: launches on
+ * the context's stream one kernel whose mbarrier wait can never complete (the
+ * barrier expects an arrival that no thread, copy or MMA makes), with a limit
+ * of `spins` polls; the wait runs out, the kernel records it in the engine's
+ * error word exactly as the transform and conversion kernels do, and
+ * returns with nothing in flight.  The next aoa_ctx_sync returns
+ * AOA_ERR_TIMEOUT; the context stays usable.                                  */
+int aoa_ctx_wait_check(aoa_ctx* c, int spins);
 
 /* --- device memory on the context stream (poly_init / poly_copy_to_device /
  *     poly_copy_to_host, src/arithmetic/poly_t.cpp:10-100).                    */
