@@ -33,6 +33,12 @@ struct AoaError : public std::runtime_error {
   } while (0)
 
 constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration limit
+// Lazy transforms need every prime below 2^kLazyPrimeBits: forward values
+// stay below 16q < 2^64 (primes of more bits take canonical butterflies)
+#ifndef AOA_LAZY_PRIME_BITS
+#define AOA_LAZY_PRIME_BITS 60
+#endif
+constexpr int kLazyPrimeBits = AOA_LAZY_PRIME_BITS;
 constexpr int kLargeItems = 1536;           // limb-transform launches this large use ntt_waves_large
 
 struct Tune {
@@ -92,7 +98,7 @@ struct Engine {
   long N = 0;
   int k = 0, kl = 0, nprimes = 0;
   int scale_bits = 0;
-  bool lazy = false;          // every prime < 2^61: Harvey lazy butterflies
+  bool lazy = false;          // every prime < 2^kLazyPrimeBits: Harvey lazy butterflies
   std::vector<uint64_t> primes, gens;
   std::vector<PrimeConst> h_pc;
   PrimeConst* d_pc = nullptr;

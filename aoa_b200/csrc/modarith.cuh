@@ -59,6 +59,48 @@ AOA_HD uint64_t shoup_lazy(uint64_t a, uint64_t w, uint64_t wp, uint64_t q) {
   return a * w - t * q;
 }
 
+// Shoup product for the limb transforms, which are bound by the integer
+// multiply pipe, written as 32 x 32-bit multiply-adds.  With y = y1 2^32 + y0
+// and wp = p1 2^32 + p0, the quotient is estimated from the three high partial
+// products, t' = y1 p1 + hi(y0 p1) + hi(y1 p0): the dropped terms (the low
+// words of the cross products and y0 p0) are below 3 * 2^64, so t - 2 <= t'
+// <= t for t = floor(y wp / 2^64), and the remainder y w - t' q, formed as
+// y w + t' (2^64 - q) mod 2^64 (nq = 2^64 - q) with its high word summed in
+// 32 bits, lies in [0, 4q).
+__device__ __forceinline__ uint64_t shoup_lazy_mad3(uint64_t y, uint64_t w, uint64_t wp, uint64_t nq) {
+  uint64_t r;
+#ifdef __CUDA_ARCH__
+  asm("{\n\t"
+      ".reg .u32 y0, y1, w0, w1, p0, p1, n0, n1, a1, b1, s0, s1, t0, t1, r0, r1;\n\t"
+      ".reg .u64 S, T, R;\n\t"
+      "mov.b64 {y0, y1}, %1;\n\t"
+      "mov.b64 {w0, w1}, %2;\n\t"
+      "mov.b64 {p0, p1}, %3;\n\t"
+      "mov.b64 {n0, n1}, %4;\n\t"
+      "mul.hi.u32 a1, y0, p1;\n\t"
+      "mul.hi.u32 b1, y1, p0;\n\t"
+      "add.cc.u32 s0, a1, b1;\n\t"
+      "addc.u32 s1, 0, 0;\n\t"
+      "mov.b64 S, {s0, s1};\n\t"
+      "mad.wide.u32 T, y1, p1, S;\n\t"
+      "mov.b64 {t0, t1}, T;\n\t"
+      "mul.wide.u32 R, y0, w0;\n\t"
+      "mad.wide.u32 R, t0, n0, R;\n\t"
+      "mov.b64 {r0, r1}, R;\n\t"
+      "mad.lo.u32 r1, y0, w1, r1;\n\t"
+      "mad.lo.u32 r1, y1, w0, r1;\n\t"
+      "mad.lo.u32 r1, t0, n1, r1;\n\t"
+      "mad.lo.u32 r1, t1, n0, r1;\n\t"
+      "mov.b64 %0, {r0, r1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(y), "l"(w), "l"(wp), "l"(nq));
+#else
+  r = y * w + mulhi64(y, wp) * nq;
+#endif
+  return r;
+}
+
 AOA_HD uint64_t shoup(uint64_t a, uint64_t w, uint64_t wp, uint64_t q) {
   uint64_t r = shoup_lazy(a, w, wp, q);
   return r >= q ? r - q : r;

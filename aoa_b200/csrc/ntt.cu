@@ -42,13 +42,10 @@ struct Sub {
 };
 
 // ---- butterflies ------------------------------------------------------------
-// Strict mode keeps every value canonical in [0, q) (any q < 2^63).  Lazy mode
-// (all primes < 2^61) follows Harvey's bounds with the forward reduction
-// taken every second stage: a reducing stage (even stage index within its
-// pass) maps inputs in [0, 8q) to [0, 6q) (U = x - 4q when x >= 4q), the
-// stage after it maps [0, 6q) to [0, 8q) without reducing, so 8q < 2^64 holds
-// throughout; inverse values live in [0, 2q).  The last stage of each
-// transform reduces to [0, q).
+// Strict mode keeps every value canonical in [0, q) (any q < 2^63); lazy mode
+// (all primes < 2^60) lets values grow between reductions (Harvey's lazy
+// butterflies; bounds below).  The last stage of each transform reduces to
+// [0, q).
 
 template <bool LAZY>
 struct Bf;
@@ -74,37 +71,55 @@ struct Bf<false> {
   static __device__ __forceinline__ uint64_t fwd_out(uint64_t x, uint64_t) { return x; }
 };
 
+// Lazy butterflies (every prime below 2^60).  The Shoup products take their
+// quotient from the three high 32 x 32-bit partial products
+// (shoup_lazy_mad3): one wide multiply fewer than the exact quotient on the
+// integer multiply pipe, which bounds these kernels, for products in [0, 4q)
+// instead of [0, 2q) (measured 1255 -> 1412 GB/s for the forward transform of
+// 256 x 30 limbs at 2^16; the exact quotient written the same way measured
+// no faster than the compiler's lowering).  Forward values stay below 16q
+// (< 2^64): a reducing stage (even stage index within its pass) maps [0, 16q)
+// to [0, 12q) (U reduced by 8q), the stage after it maps [0, 12q) to
+// [0, 16q).  Inverse values stay in [0, 4q), reduced at every stage.
 template <>
 struct Bf<true> {
+  static __device__ __forceinline__ uint64_t mulw(uint64_t y, ShoupW w, uint64_t q) {
+    return shoup_lazy_mad3(y, w.w, w.wp, 0 - q);   // [0, 4q)
+  }
+  // x - b if x >= b else x, for x < 2^63 + b, b < 2^63 (sign of the difference)
+  static __device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t b) {
+    const int64_t d = (int64_t)(x - b);
+    return d < 0 ? x : (uint64_t)d;
+  }
   // red (a compile-time constant after unrolling): reducing stage
   static __device__ __forceinline__ void ct(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q, bool red) {
-    const uint64_t q2 = q << 1, q4 = q << 2;
-    uint64_t U = x;                             // [0, 8q) if red, else [0, 6q)
-    if (red) U = U >= q4 ? U - q4 : U;          // [0, 4q)
-    uint64_t V = shoup_lazy(y, w.w, w.wp, q);   // [0, 2q)
-    x = U + V;                                  // [0, 6q) if red, else [0, 8q)
-    y = U - V + q2;                             // likewise
+    const uint64_t q4 = q << 2;
+    uint64_t U = x;                             // [0, 16q) if red, else [0, 12q)
+    if (red) U = csub(U, q << 3);               // [0, 8q)
+    const uint64_t V = mulw(y, w, q);           // [0, 4q)
+    x = U + V;                                  // [0, 12q) if red, else [0, 16q)
+    y = U - V + q4;                             // likewise
   }
+  // inputs and outputs in [0, 4q)
   static __device__ __forceinline__ void gs(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q) {
-    const uint64_t q2 = q << 1;
-    uint64_t U = x, V = y;                      // [0, 2q)
-    uint64_t s = U + V;
-    x = s >= q2 ? s - q2 : s;                   // [0, 2q)
-    y = shoup_lazy(U - V + q2, w.w, w.wp, q);   // [0, 2q)
+    const uint64_t q4 = q << 2;
+    const uint64_t U = x, V = y;
+    x = csub(U + V, q4);
+    y = mulw(U - V + q4, w, q);
   }
+  // final inverse stage with N^-1 folded in: outputs in [0, q)
   static __device__ __forceinline__ void gs_last(uint64_t& x, uint64_t& y, ShoupW n0, ShoupW n1, uint64_t q) {
-    const uint64_t q2 = q << 1;
-    uint64_t U = x, V = y;
-    uint64_t a = shoup_lazy(U + V, n0.w, n0.wp, q);
-    uint64_t b = shoup_lazy(U - V + q2, n1.w, n1.wp, q);
-    x = a >= q ? a - q : a;
-    y = b >= q ? b - q : b;
+    const uint64_t U = x, V = y;
+    const uint64_t a = mulw(U + V, n0, q);
+    const uint64_t b = mulw(U - V + (q << 2), n1, q);
+    x = csub(csub(a, q << 1), q);
+    y = csub(csub(b, q << 1), q);
   }
-  static __device__ __forceinline__ uint64_t fwd_out(uint64_t x, uint64_t q) {   // [0, 8q) -> [0, q)
-    const uint64_t q2 = q << 1, q4 = q << 2;
-    x = x >= q4 ? x - q4 : x;
-    x = x >= q2 ? x - q2 : x;
-    return x >= q ? x - q : x;
+  static __device__ __forceinline__ uint64_t fwd_out(uint64_t x, uint64_t q) {   // [0, 16q) -> [0, q)
+    x = csub(x, q << 3);
+    x = csub(x, q << 2);
+    x = csub(x, q << 1);
+    return csub(x, q);
   }
 };
 
@@ -331,6 +346,14 @@ struct NttBatch {
   int spin;                // polls of a bounded wait for this kernel's own copies (engine knob)
 };
 
+// Threads per SM the pass kernels are compiled for (register budget).
+#ifndef AOA_COLS_TPSM
+#define AOA_COLS_TPSM 768
+#endif
+#ifndef AOA_ROWS_TPSM
+#define AOA_ROWS_TPSM 384
+#endif
+
 // Tile widths: a column-pass CTA takes W = PER_CTA >> DIV columns (at least 2,
 // so that a row segment is a multiple of 16 bytes), a row-pass CTA takes
 // PER_CTA >> DIV rows (at least 1).  DIV is a tuning choice (0, 1, 2).
@@ -339,7 +362,7 @@ struct ColTile {
   static constexpr int W0 = Sub<LOG_S>::PER_CTA >> DIV;
   static constexpr int W = W0 < 2 ? 2 : W0;
   static constexpr int THREADS = Sub<LOG_S>::T * W;
-  static constexpr int MIN_BLOCKS = 768 / THREADS < 1 ? 1 : (768 / THREADS > 32 ? 32 : 768 / THREADS);
+  static constexpr int MIN_BLOCKS = AOA_COLS_TPSM / THREADS < 1 ? 1 : (AOA_COLS_TPSM / THREADS > 32 ? 32 : AOA_COLS_TPSM / THREADS);
   static constexpr size_t SMEM = 2 * (size_t)Sub<LOG_S>::S * W * 8 + 2 * (size_t)Sub<LOG_S>::S * sizeof(ShoupW);
 };
 
@@ -350,7 +373,7 @@ struct RowTile {
   static constexpr int THREADS = Sub<LOG_S>::T * ROWS;
   // 384 threads per SM: up to 170 registers, so the low-digit twiddles held in
   // registers do not spill (measured 1% faster than 512 threads with spills)
-  static constexpr int MIN_BLOCKS = 384 / THREADS < 1 ? 1 : (384 / THREADS > 32 ? 32 : 384 / THREADS);
+  static constexpr int MIN_BLOCKS = AOA_ROWS_TPSM / THREADS < 1 ? 1 : (AOA_ROWS_TPSM / THREADS > 32 ? 32 : AOA_ROWS_TPSM / THREADS);
   static constexpr size_t SMEM =
       2 * (size_t)ROWS * Sub<LOG_S>::S * 8 + 2 * (size_t)ROWS * (Sub<LOG_S>::E - 1) * sizeof(ShoupW);
 };

@@ -1,0 +1,68 @@
+#!/usr/bin/env python3
+"""Golden outputs of the reference evaluator's own kernels.
+
+oracle/_ref/ref_harness runs pdroalves/aoa's aoa-ntt transform and RNS
+kernels (built from its sources by oracle/ref/Makefile, where the reference
+checkout exists) through the reference's API on seeded inputs.  This script
+runs it on one GPU for each configuration below and packs its outputs into
+tests/golden/reference_outputs.npz, which tests/test_oracle_reference_outputs.py
+compares with the oracle (the inputs are regenerated there from the seeds the
+harness documents, so the fixture holds outputs only).
+
+Usage (on a machine with a GPU and the built harness):
+    python tests/golden/make_reference_outputs.py OUT_DIR
+writes OUT_DIR/reference_outputs.npz (copy it into tests/golden/).
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+# (log2 N, k, kl, prec, transforms only): the reference's hierarchical
+# transforms at 2^10 (32 x 32) and 2^12 (64 x 64) on its own prime choice
+# (a 63-bit q0, then its 55- or 52-bit bucket; special primes from the
+# 55-bit bucket), ModUp / ModDown / rescale at 2^10
+CONFIGS = [(10, 4, 5, 55, 0), (12, 3, 4, 52, 1)]
+TAGS = {1: "ntt_fwd", 2: "ntt_inv", 3: "modup", 4: "moddown", 5: "rescale", 6: "modup_max", 7: "ntt_fwd_max"}
+
+
+def parse(path):
+    w = np.fromfile(path, dtype=np.uint64)
+    assert w[:1].tobytes() == b"AOAREF01", "not a harness output"
+    N, k, kl, prec = (int(v) for v in w[1:5])
+    primes = w[5:5 + k + kl].copy()
+    at = 5 + k + kl
+    recs = {}
+    while at < w.size:
+        tag, level, n = (int(v) for v in w[at:at + 3])
+        recs["%s_l%d" % (TAGS[tag], level)] = w[at + 3:at + 3 + n].copy()
+        at += 3 + n
+    return N, k, kl, prec, primes, recs
+
+
+def main():
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    out_dir = sys.argv[1]
+    os.makedirs(out_dir, exist_ok=True)
+    arrays = {}
+    for log_n, k, kl, prec, tonly in CONFIGS:
+        path = os.path.join(out_dir, "ref_n%d.bin" % (1 << log_n))
+        subprocess.check_call([HARNESS, path, str(log_n), str(k), str(kl), str(prec), str(tonly)])
+        N, k2, kl2, prec2, primes, recs = parse(path)
+        tag = "n%d" % N
+        arrays[tag + "_params"] = np.array([N, k2, kl2, prec2], dtype=np.uint64)
+        arrays[tag + "_primes"] = primes
+        for name, v in recs.items():
+            arrays["%s_%s" % (tag, name)] = v
+    dst = os.path.join(out_dir, "reference_outputs.npz")
+    np.savez_compressed(dst, **arrays)
+    print("wrote", dst, sorted(arrays))
+
+
+if __name__ == "__main__":
+    main()

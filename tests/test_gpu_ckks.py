@@ -471,12 +471,12 @@ def test_tensor_core_and_cuda_core_conversions_agree(ref_table):
         assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
 
 
-@pytest.mark.parametrize("bits", [33, 34, 40, 61, 62])
+@pytest.mark.parametrize("bits", [33, 34, 40, 60, 61, 62])
 def test_hmult_prime_sizes_bit_exact(bits):
     """Per-call and batched HMult + relinearise + rescale at prime sizes on
     both sides of every arithmetic switch: Montgomery products below 2^33,
     Barrett from 2^33 (funnel-shift quotient), the one-reduction cross term up
-    to 61 bits, two reductions at 62 bits, lazy transforms below 2^61."""
+    to 61 bits, two reductions at 62 bits, lazy transforms below 2^60."""
     require_gpu()
     ps = oracle.gen_ntt_primes(bits, 1 << 13, 11)
     Q, B = ps[:5], ps[5:]

@@ -114,12 +114,13 @@ def test_ntt_launch_shapes_bit_exact(log_n, shape):
     assert np.array_equal(d.numpy(), x), "inverse(forward(x)) != x"
 
 
-@pytest.mark.parametrize("bits", [61, 62])
+@pytest.mark.parametrize("bits", [60, 61, 62])
 @pytest.mark.parametrize("shape", [(0, 0), (-1, 0), (1, 0), (0, 1), (1, 1)])
 def test_ntt_prime_size_edges(bits, shape):
-    """The largest primes below 2^61 (lazy butterflies: forward values up to
-    8q just below 2^64) and below 2^62 (strict butterflies), with all-(q-1)
-    and random inputs, for even and odd column-pass stage counts."""
+    """The largest primes below 2^60 (lazy butterflies: forward values up to
+    16q just below 2^64, products from the three-product Shoup quotient up to
+    4q), below 2^61 and below 2^62 (strict butterflies), with all-(q-1) and
+    random inputs, for even and odd column-pass stage counts."""
     require_gpu()
     split, kind = shape
     log_n = 15
