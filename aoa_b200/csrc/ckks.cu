@@ -359,9 +359,17 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
     sb[z] = b[z]->scale;
     slots[z] = a[z]->slots;
   }
-  tensor_batch_op(E, ptr, half, D, n, m, st);
+  // the DGT context (aoa-dgt, ckks.cpp:275-360) runs the same pipeline on its
+  // transform with Gaussian-integer products; the fused transform ends are NTT only
+  const int tk = C.transform;
   uint64_t* D2 = D + 2L * n * half;
-  const int fuse = E.tune.fuse;
+  if (tk == AOA_DGT) {
+    for (int z = 0; z < n; z++)
+      gi_tensor_op(E, a[z]->d, half, b[z]->d, half, D + z * half, D + (n + z) * half, D2 + z * half, m, st);
+  } else {
+    tensor_batch_op(E, ptr, half, D, n, m, st);
+  }
+  const int fuse = tk == AOA_NTT ? E.tune.fuse : 0;
   if (fuse & kFuseSource) {
     NttIo io;                                  // inverse of d2 read in place of a copy
     io.src = D2;
@@ -369,10 +377,14 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
     ntt_batch_io(E, T, n, 0, m, k, false, io, st);
   } else {
     AOA_CUDA(cudaMemcpy2DAsync(T, half * 8, D2, half * 8, (size_t)m * N * 8, n, cudaMemcpyDeviceToDevice, st));
-    ntt_batch(E, T, n, 0, m, k, false, st);
+    xform(E, tk, T, n, 0, m, k, false, st);
   }
   modup(E, T, half, UB, (long)kl * N, n, level, st);
-  if (fuse & kFuseKeyProduct) {
+  if (tk == AOA_DGT) {
+    xform(E, tk, UB, n, k, kl, kl, true, st);
+    for (int z = 0; z < n; z++)
+      gi_keyswitch_mul_op(E, D2 + z * half, UB + (long)z * kl * N, evk->d, KS + z * ks, KS + (n + z) * ks, m, st);
+  } else if (fuse & kFuseKeyProduct) {
     NttIo io;                                  // special-limb transform with the key products fused
     io.epi.mode = kEpiKeyProduct;
     io.epi.out = KS + (long)m * N;
@@ -386,7 +398,7 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
     ntt_batch(E, UB, n, k, kl, kl, true, st);
     keyswitch_mul_batch_op(E, D2, half, UB, (long)kl * N, evk->d, KS, ks, n, m, st);
   }
-  ntt_batch(E, KS + (long)m * N, 2 * n, k, kl, k + kl, false, st);
+  xform(E, tk, KS + (long)m * N, 2 * n, k, kl, k + kl, false, st);
   OutPtrs outp;
   for (int z = 0; z < n; z++) {
     outp.p[z] = out[z]->d;
@@ -394,12 +406,12 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
   }
   if (do_rescale) {
     ks_combine(E, U, N, D + (long)level * N, half, KS + (long)level * N, ks, nullptr, 0, 1, 2 * n, 0, st, level);
-    ntt_batch(E, U, 2 * n, level, 1, 1, false, st);
+    xform(E, tk, U, 2 * n, level, 1, 1, false, st);
     rescale_corrections(E, KS + (long)m * N, ks, U, N, CL, N, Y, half, 2 * n, level, st);
     if (fuse & kFuseCombine) {
       combine_into(C, Y, 2 * n, level, D, half, 2 * n, KS, ks, level, nullptr, 0, &outp, st);
     } else {
-      ntt_batch(E, Y, 2 * n, 0, level, k, true, st);
+      xform(E, tk, Y, 2 * n, 0, level, k, true, st);
       ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, level, 2 * n, level, st);
     }
   } else {
@@ -407,7 +419,7 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
     if (fuse & kFuseCombine) {
       combine_into(C, Y, 2 * n, m, D, half, 2 * n, KS, ks, 0, nullptr, 0, &outp, st);
     } else {
-      ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
+      xform(E, tk, Y, 2 * n, 0, m, k, true, st);
       ks_combine_ptr(E, outp, D, half, KS, ks, Y, half, m, 2 * n, 0, st);
     }
   }
@@ -415,7 +427,7 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
     out[z]->level = do_rescale ? level - 1 : level;
     out[z]->slots = slots[z];
     out[z]->scale = scale_after_mult(E, sa[z], sb[z], level);
-    out[z]->domain = AOA_NTT;
+    out[z]->domain = tk;
   }
 }
 
@@ -467,8 +479,8 @@ static void run_grouped(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa
 void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b, const aoa_swk* evk,
                  bool do_rescale) {
   const Engine& E = *C.E;
-  if (C.transform != AOA_NTT || (evk && evk->domain != AOA_NTT))
-    throw AoaError(AOA_ERR_BAD_PARAM, "batched HMult runs on the NTT transform only");
+  if (evk && evk->domain != C.transform)
+    throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
   if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
   if (n == 0) return;
   if (!out || !a || !b) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
@@ -482,8 +494,8 @@ void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* co
       throw AoaError(AOA_ERR_SLOT_MISMATCH, "Ciphertexts must have the same number of slots.");
   }
   for (int z = 0; z < n; z++) {                  // operands to the transform domain (poly_mul's rule)
-    to_domain(C, a[z], AOA_NTT, a[z]->level + 1);
-    to_domain(C, b[z], AOA_NTT, b[z]->level + 1);
+    to_domain(C, a[z], C.transform, a[z]->level + 1);
+    to_domain(C, b[z], C.transform, b[z]->level + 1);
   }
   // group by level (the operands' common limb count), chunks of kMaxBatch
   run_grouped(C, n, out, a, b, [&](int z) { return std::min(a[z]->level, b[z]->level); },

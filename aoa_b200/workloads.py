@@ -4,16 +4,21 @@ Batched uneven workload: many ciphertexts of different ring degree and live
 limb count with a mix of HMult + relinearise + rescale, rotations and
 additions.  The grouped schedule runs one context (stream) per ring degree,
 batches every HMult of a degree into grouped launches (aoa_hmult_batch groups
-by limb count) and is captured once per context into a CUDA graph that is
-replayed; the plain schedule issues the reference's per-call operation
-sequence one op at a time.
+by limb count) and every rotation by one step into one batched call
+(aoa_rotate_batch, grouped by limb count, one key per step), and is captured
+once per context into a CUDA graph that is replayed; the plain schedule
+issues the reference's per-call operation sequence one op at a time.
 
 Serving loop: requests (a plaintext-weight multiply with rescale, a
 rotate-and-sum over the slots, a rescale) arrive as a Poisson process;
 requests are admitted while a slot (a context of the request's ring degree)
 and the HBM budget allow, run asynchronously next to the requests already on
-the device, and complete in any order.  Keys stay resident.  Latency is
-arrival to completion on the host clock.
+the device, and complete in any order.  Keys stay resident and count against
+the budget first (they dominate it: 15 Galois keys of 2 x 61 limbs at 2^16
+are 0.94 GB); a request's three ciphertexts count while it is in flight.
+Latency is arrival to completion on the host clock; each run records how
+many requests were admitted and how many had to wait for a slot or for
+budget.
 """
 import time
 
@@ -55,8 +60,11 @@ class UnevenBatch:
             N = 1 << ln
             self.engines[ln], self.ctx[ln] = E, ctx
             self.evk[ln] = SwitchKey(ctx, _rand_residues(rng, primes, N), _rand_residues(rng, primes, N))
-            # one key serves every rotation step of this degree (the kernels' work does not depend on the key)
-            self.rtk[ln] = SwitchKey(ctx, _rand_residues(rng, primes, N), _rand_residues(rng, primes, N))
+            # a distinct rotation key for every step 2^j the mix can draw (the reference's
+            # ckks_new_rtk_left makes one per power of two, ckkskeys.cpp:146-181): the key
+            # traffic of distinct keys is paid as in a real mix
+            self.rtk[ln] = {1 << j: SwitchKey(ctx, _rand_residues(rng, primes, N), _rand_residues(rng, primes, N))
+                            for j in range(ln - 1)}
             self.inputs[ln] = [Ciphertext.from_residues(ctx, _rand_residues(rng, primes[:k], N),
                                                         _rand_residues(rng, primes[:k], N), slots=N // 2,
                                                         scale=1 << scale_bits, domain=AOA_NTT)
@@ -89,21 +97,25 @@ class UnevenBatch:
 
     def run_grouped(self, ln):
         """Every op of degree 2^ln on its context: the HMults in grouped batched
-        launches (grouped by limb count inside the call), then the rotations and
-        additions."""
+        launches (grouped by limb count inside the call), the rotations in one
+        batched call per step (grouped by limb count inside the call, each step
+        with its own key), then the additions."""
         ctx = self.ctx[ln]
         muls = [z for z, op in enumerate(self.ops) if op["log_n"] == ln and op["kind"] == "mul"]
         if muls:
             pairs = [self._args(z) for z in muls]
             ckks_mul_batch(ctx, [self.outs[z] for z in muls], [p[0] for p in pairs], [p[1] for p in pairs],
                            self.evk[ln])
+        by_step = {}
         for z, op in enumerate(self.ops):
-            if op["log_n"] != ln or op["kind"] == "mul":
-                continue
-            args = self._args(z)
-            if op["kind"] == "rot":
-                ckks_rotate_left(ctx, self.outs[z], args[0], op["step"], self.rtk[ln])
-            else:
+            if op["log_n"] == ln and op["kind"] == "rot":
+                by_step.setdefault(op["step"], []).append(z)
+        for step, zs in sorted(by_step.items()):
+            ckks_rotate_batch(ctx, [self.outs[z] for z in zs], [self._args(z)[0] for z in zs], step,
+                              self.rtk[ln][step])
+        for z, op in enumerate(self.ops):
+            if op["log_n"] == ln and op["kind"] == "add":
+                args = self._args(z)
                 ckks_add(ctx, self.outs[z], args[0], args[1])
 
     def run_plain(self):
@@ -116,7 +128,7 @@ class UnevenBatch:
             if op["kind"] == "mul":
                 ckks_mul_plain(ctx, self.outs[z], args[0], args[1], self.evk[ln])
             elif op["kind"] == "rot":
-                ckks_rotate_left(ctx, self.outs[z], args[0], op["step"], self.rtk[ln])
+                ckks_rotate_left(ctx, self.outs[z], args[0], op["step"], self.rtk[ln][op["step"]])
             else:
                 ckks_add(ctx, self.outs[z], args[0], args[1])
 
@@ -154,6 +166,7 @@ class Server:
         primes = params.ntt_primes(60, 2 << max(log_ns), k + kl)
         self.engines, self.pool, self.keys, self.weights = {}, {}, {}, {}
         self.hbm_budget, self.hbm_used = hbm_budget, 0
+        self.stats = {}
         for ln in log_ns:
             E = Engine(ln, primes[:k], primes[k:], scale_bits=scale_bits)
             if autotune:
@@ -172,9 +185,30 @@ class Server:
             ctxs[0].sync()
         self.slots = {ln: n_slots_used or (1 << ln) // 2 for ln in log_ns}
         self.scale = 1 << scale_bits
+        # resident for the server's lifetime: every degree's Galois keys (2 polys
+        # of k + kl limbs each) and its encoded weights (k limbs); they count
+        # against the HBM budget before any request is admitted
+        self.resident_bytes = sum(len(self.keys[ln]) * 2 * (k + kl) * (1 << ln) * 8 + k * (1 << ln) * 8
+                                  for ln in log_ns)
 
     def footprint(self, ln):
         return 3 * 2 * self.k * (1 << ln) * 8          # input, product and output ciphertexts
+
+    def fits(self, ln):
+        """Whether a request of degree 2^ln fits the HBM budget next to the
+        resident keys and the requests in flight."""
+        return self.resident_bytes + self.hbm_used + self.footprint(ln) <= self.hbm_budget
+
+    def _reset_stats(self):
+        self.stats = {"admitted": 0, "deferred_by_budget": 0, "deferred_by_slots": 0, "max_in_flight": 0,
+                      "max_hbm_bytes": 0, "in_flight": 0}
+
+    def _admitted(self, ln):
+        st = self.stats
+        st["admitted"] += 1
+        st["in_flight"] += 1
+        st["max_in_flight"] = max(st["max_in_flight"], st["in_flight"])
+        st["max_hbm_bytes"] = max(st["max_hbm_bytes"], self.resident_bytes + self.hbm_used)
 
     def submit(self, ctx_index, req):
         """Enqueue a request's chain on its context (asynchronous)."""
@@ -199,6 +233,8 @@ class Server:
         events = {}
         pending = list(range(n))
         done_at = np.zeros(n)
+        self._reset_stats()
+        waited = set()
         t0 = time.perf_counter()
         remaining = n
         while remaining:
@@ -210,8 +246,10 @@ class Server:
                         done_at[r] = time.perf_counter() - t0
                         busy[ln][i] = None
                         self.hbm_used -= self.footprint(ln)
+                        self.stats["in_flight"] -= 1
                         remaining -= 1
-            # admissions (arrival order, skipping requests whose degree has no free slot)
+            # admissions (arrival order, skipping requests whose degree has no free
+            # slot or that do not fit the HBM budget next to the resident keys)
             still = []
             for r in pending:
                 req = requests[r]
@@ -220,7 +258,10 @@ class Server:
                     still.append(r)
                     continue
                 free = [i for i, x in enumerate(busy[ln]) if x is None]
-                if not free or self.hbm_used + self.footprint(ln) > self.hbm_budget:
+                if not free or not self.fits(ln):
+                    if r not in waited:
+                        waited.add(r)
+                        self.stats["deferred_by_slots" if not free else "deferred_by_budget"] += 1
                     still.append(r)
                     continue
                 i = free[0]
@@ -230,14 +271,26 @@ class Server:
                 events[r] = ev
                 busy[ln][i] = r
                 self.hbm_used += self.footprint(ln)
+                self._admitted(ln)
             pending = still
             if poll:
                 time.sleep(poll)
         wall = time.perf_counter() - t0
         return done_at - arrivals, wall
 
-    def make_requests(self, n, seed=6, min_limbs=6):
+    def make_requests(self, n, seed=6, min_limbs=6, templates=None):
+        """n requests (degree, live limbs, input ciphertext, product and output
+        buffers).  With `templates` = t, each degree draws t distinct random
+        inputs and every request gets a device copy of one of them (fast to
+        make in the hundreds); otherwise every request draws its own."""
         rng = np.random.default_rng(seed)
+        tmpl = {}
+        if templates:
+            for ln in self.log_ns:
+                ctx, N, primes = self.pool[ln][0], 1 << ln, self.engines[ln].q_primes
+                tmpl[ln] = [Ciphertext.from_residues(ctx, _rand_residues(rng, primes, N),
+                                                     _rand_residues(rng, primes, N), slots=self.slots[ln],
+                                                     scale=self.scale, domain=AOA_COEF) for _ in range(templates)]
         reqs = []
         for _ in range(n):
             ln = int(rng.choice(self.log_ns))
@@ -245,8 +298,11 @@ class Server:
             ctx = self.pool[ln][0]
             N = 1 << ln
             primes = self.engines[ln].q_primes
-            ct = Ciphertext.from_residues(ctx, _rand_residues(rng, primes, N), _rand_residues(rng, primes, N),
-                                          slots=self.slots[ln], scale=self.scale, domain=AOA_COEF)
+            if templates:
+                ct = tmpl[ln][int(rng.integers(0, templates))].copy()
+            else:
+                ct = Ciphertext.from_residues(ctx, _rand_residues(rng, primes, N), _rand_residues(rng, primes, N),
+                                              slots=self.slots[ln], scale=self.scale, domain=AOA_COEF)
             reqs.append({"log_n": ln, "m": m, "ct": ct, "prod": Ciphertext(ctx), "out": Ciphertext(ctx)})
         for c in (c for cs in self.pool.values() for c in cs):
             c.sync()
@@ -326,6 +382,8 @@ class BatchServer(Server):
         pending = list(range(n))
         done_at = np.zeros(n)
         ids = {id(r): i for i, r in enumerate(requests)}
+        self._reset_stats()
+        waited = set()
         t0 = time.perf_counter()
         remaining = n
         while remaining:
@@ -339,18 +397,26 @@ class BatchServer(Server):
                             done_at[i] = t
                             remaining -= 1
                             self.hbm_used -= self.footprint(ln)
+                            self.stats["in_flight"] -= 1
                     else:
                         keep.append((ev, fin))
                 inflight[ln] = keep
             still = []
-            for i in pending:                               # admissions
+            for i in pending:                               # admissions: the HBM budget binds
                 r = requests[i]
                 ln = r["log_n"]
-                if arrivals[i] > now or self.hbm_used + self.footprint(ln) > self.hbm_budget:
+                if arrivals[i] > now:
+                    still.append(i)
+                    continue
+                if not self.fits(ln):
+                    if i not in waited:
+                        waited.add(i)
+                        self.stats["deferred_by_budget"] += 1
                     still.append(i)
                     continue
                 active[ln].append(r)
                 self.hbm_used += self.footprint(ln)
+                self._admitted(ln)
             pending = still
             for ln in self.log_ns:                          # one iteration per degree
                 if not active[ln] or len(inflight[ln]) >= self.max_inflight:

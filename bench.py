@@ -337,39 +337,49 @@ def systems_workloads(aoa, torch):
               "plain_ops_per_s": n_ops / (plain_ms / 1000.0), "speedup_vs_plain": plain_ms / graph_ms,
               "graph_nodes": nodes, "algorithmic_bytes": wb.bytes,
               "achieved_gbs": wb.bytes / (graph_ms / 1000.0) / 1e9,
-              "schedule": "one stream per N, HMults grouped by limb count (<=64 per launch), CUDA graph per stream"}
+              "rotation_keys": "a distinct key per step 2^j and degree",
+              "schedule": "one stream per N; HMults grouped by limb count (<=64 per launch), rotations batched "
+                          "per step (grouped by limb count), additions; one CUDA graph per stream"}
     del wb
+    n_req = 500
+
+    def serve(server, reqs, factors):
+        server.run(reqs[:16], rate=None)                  # warm the contexts' workspaces
+        lat, wall = server.run(reqs, rate=None)
+        sat = len(reqs) / wall
+        out = {"saturation_req_per_s": sat, "saturation_stats": dict(server.stats), "rates": []}
+        for f in factors:
+            lat, wall = server.run(reqs, rate=f * sat)
+            out["rates"].append({"rate_factor": f, "offered_req_per_s": f * sat, "requests": len(reqs),
+                                 "served_req_per_s": len(reqs) / wall,
+                                 "p50_ms": float(np.percentile(lat, 50) * 1000),
+                                 "p99_ms": float(np.percentile(lat, 99) * 1000),
+                                 "max_ms": float(np.max(lat) * 1000), **server.stats})
+        return out
+
     srv = Server(log_ns=(15, 16), slots_per_degree=4, hbm_budget=8 << 30, autotune=True)
-    reqs = srv.make_requests(48, seed=6)
-    srv.run(reqs[:8], rate=None)                         # warm the contexts' workspaces
-    lat, wall = srv.run(reqs, rate=None)
-    sat = len(reqs) / wall
-    rates = []
-    for f in (0.25, 0.5, 0.75, 0.9, 1.1):
-        lat, wall = srv.run(reqs, rate=f * sat)
-        rates.append({"rate_factor": f, "offered_req_per_s": f * sat, "served_req_per_s": len(reqs) / wall,
-                      "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000)})
-    serving = {"saturation_req_per_s": sat, "requests_per_rate": len(reqs), "streams_per_degree": 4,
-               "hbm_budget_bytes": 8 << 30, "rates": rates,
-               "request": "ct*w (plaintext, rescale) + rotate-and-sum over N/2 slots + rescale; N in {2^15,2^16}, "
-                          "live limbs 6..30; latency = arrival to completion (host clock)"}
+    reqs = srv.make_requests(n_req, seed=6, templates=8)
+    serving = serve(srv, reqs, (0.25, 0.5, 0.75, 0.9, 1.1))
+    serving.update({"requests_per_rate": n_req, "streams_per_degree": 4, "hbm_budget_bytes": 8 << 30,
+                    "resident_key_bytes": srv.resident_bytes,
+                    "request": "ct*w (plaintext, rescale) + rotate-and-sum over N/2 slots + rescale; N in "
+                               "{2^15,2^16}, live limbs 6..30; latency = arrival to completion (host clock)"})
     del srv, reqs
     # the same requests with iteration-level batching (one context per degree)
     bsrv = BatchServer(log_ns=(15, 16), hbm_budget=8 << 30, autotune=True)
-    breqs = bsrv.make_requests(48, seed=6)
-    bsrv.run(breqs[:8], rate=None)
-    lat, wall = bsrv.run(breqs, rate=None)
-    bsat = len(breqs) / wall
-    brates = []
-    for f in (0.25, 0.5, 0.75, 0.9, 1.1):
-        lat, wall = bsrv.run(breqs, rate=f * bsat)
-        brates.append({"rate_factor": f, "offered_req_per_s": f * bsat, "served_req_per_s": len(breqs) / wall,
-                       "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000)})
-    serving["iteration_batched"] = {
-        "saturation_req_per_s": bsat, "rates": brates,
-        "schedule": "one context per degree; each iteration advances every active request one stage, the "
-                    "rotations of a stage in one batched launch sequence (aoa_rotate_batch); arrivals join at "
-                    "the next iteration"}
+    breqs = bsrv.make_requests(n_req, seed=6, templates=8)
+    serving["iteration_batched"] = serve(bsrv, breqs, (0.25, 0.5, 0.75, 0.9, 1.1))
+    serving["iteration_batched"]["schedule"] = (
+        "one context per degree; each iteration advances every active request one stage, the rotations of a "
+        "stage in one batched launch sequence (aoa_rotate_batch); arrivals join at the next iteration")
+    # a budget that binds: the resident keys plus room for six 2^16 requests
+    budget = bsrv.resident_bytes + 6 * bsrv.footprint(16)
+    bsrv.hbm_budget = budget
+    bound = serve(bsrv, breqs, (0.9,))
+    bound.update({"hbm_budget_bytes": budget, "resident_key_bytes": bsrv.resident_bytes,
+                  "note": "HBM budget = resident Galois keys and weights + 6 requests at 2^16; admission waits "
+                          "for budget (deferred_by_budget), not for slots"})
+    serving["iteration_batched_budget_bound"] = bound
     return uneven, serving
 
 

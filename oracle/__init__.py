@@ -6,10 +6,16 @@ ctypes.  Only tests/, the smoke check in __graft_entry__.py and the CPU
 baseline / reference arm of bench.py may import this package.  The product
 (aoa_b200) never does: its path fails loudly without its CUDA library.
 
-Parity status: pinned.  The oracle's arithmetic is checked against exact
-big-integer results and its transforms and products against an independent
-Python model and the schoolbook negacyclic product (the reference's own
-NTL-based tests, aoa-ntt/tests/tests.cpp:300-694); see tests/test_oracle_*.py.
+Parity status: pinned on the reference's own outputs.  The reference's
+aoa-ntt kernels, built from its sources (oracle/ref/Makefile) and run through
+its API on a B200, produced tests/golden/reference_outputs.npz (forward and
+inverse hierarchical transforms at 2^10 and 2^12, ModUp, ModDown and rescale
+at two levels, on the reference's own primes and precompute); the oracle
+equals them word for word (tests/test_oracle_reference_outputs.py).  Its
+arithmetic is also checked against exact big-integer results and its
+transforms and products against an independent Python model and the
+schoolbook negacyclic product (the reference's own NTL-based tests,
+aoa-ntt/tests/tests.cpp:300-694); see tests/test_oracle_*.py.
 """
 import ctypes
 import os

@@ -202,3 +202,49 @@ def test_dgt_context_rejects_ntt_key(dgt_table):
     with pytest.raises(aoa.AoaError) as ei:
         aoa.ckks_mul(ctx, out, ca, ca, evk_ntt)
     assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("rescale", [True, False])
+def test_dgt_hmult_batch_matches_oracle_and_per_call(dgt_table, rescale):
+    """Batched HMult on a DGT context (aoa-dgt ckks_mul, src/ckks.cpp:275-360,
+    one launch per stage over the batch; 10 products at mixed levels, inputs
+    in coefficients and in the DGT domain, an output aliasing an input; the
+    group of 8 runs as two halves on two streams): every product equals the
+    per-call DGT HMult and the oracle."""
+    require_gpu()
+    aoa, E, ctx, D, o = _setup(dgt_table, 12, 4, 4, 55, transform=3)
+    keys = make_keys(o, seed=33)
+    evk = aoa.SwitchKey(ctx, o.ntt_inv(keys["evk"][0]), o.ntt_inv(keys["evk"][1]), domain=aoa.AOA_COEF)
+    rng = np.random.default_rng(12)
+    N, k = E.N, E.k
+    levels = [3, 3, 2, 3, 3, 3, 3, 3, 2, 3]
+    data = [tuple(uniform_residues(rng, E.q_primes, N) for _ in range(4)) for _ in levels]
+
+    def make(z, x):
+        dom = aoa.AOA_DGT if z % 2 else aoa.AOA_COEF
+        conv = (lambda v: unfold(D.fwd(fold(v)))) if dom == aoa.AOA_DGT else (lambda v: v)
+        ca = aoa.Ciphertext.from_residues(ctx, conv(x[0]), conv(x[1]), slots=8, scale=1 << 40, domain=dom)
+        cb = aoa.Ciphertext.from_residues(ctx, conv(x[2]), conv(x[3]), slots=8, scale=(1 << 40) + 3, domain=dom)
+        ca.set(levels[z], 8, 1 << 40, dom)
+        cb.set(levels[z], 8, (1 << 40) + 3, dom)
+        return ca, cb
+
+    pairs = [make(z, x) for z, x in enumerate(data)]
+    outs = [aoa.Ciphertext(ctx) for _ in data]
+    outs[4] = pairs[4][0]                                  # output aliases an input
+    aoa.ckks_mul_batch(ctx, outs, [p[0] for p in pairs], [p[1] for p in pairs], evk, rescale=rescale)
+    for z, x in enumerate(data):
+        lv = levels[z]
+        nl = lv if rescale else lv + 1
+        pad = lambda v: np.concatenate([v[: lv + 1], np.zeros((k - lv - 1, N), dtype=np.uint64)])
+        w0, w1, wsc = o.hmult((pad(x[0]), pad(x[1])), (pad(x[2]), pad(x[3])), keys["evk"], lv, 1 << 40,
+                              (1 << 40) + 3, rescale=rescale)
+        assert outs[z].domain == aoa.AOA_DGT and outs[z].level == nl - 1 and outs[z].scale == wsc, z
+        g0, g1 = outs[z].download(nlimbs=nl, domain=aoa.AOA_COEF)
+        assert np.array_equal(g0, w0[:nl]) and np.array_equal(g1, w1[:nl]), z
+        ca, cb = make(z, x)
+        single = aoa.Ciphertext(ctx)
+        (aoa.ckks_mul if rescale else aoa.ckks_mul_without_rescale)(ctx, single, ca, cb, evk)
+        s0, s1 = single.download(nlimbs=nl, domain=aoa.AOA_DGT)
+        b0, b1 = outs[z].download(nlimbs=nl, domain=aoa.AOA_DGT)
+        assert np.array_equal(s0, b0) and np.array_equal(s1, b1), z
