@@ -432,8 +432,12 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
 }
 
 // Runs `group(stream, workspace, bytes, count, outs, as, bs, level)` over groups of
-// equal level, a group of 8 or more as two halves on the context's two
-// streams unless an output of one half is an input of the other.
+// equal level (at most kMaxBatch ops each).  With the engine's two streams, a
+// group of 8 or more runs as two halves on the context's two streams, and
+// smaller groups go whole to the stream with less queued work (ops x limbs),
+// so the groups of a mix of levels overlap on the device; each stream keeps
+// its own stream-ordered workspace.  If an output of an op on one stream is an
+// operand or an output of an op on the other, every group runs on one stream.
 template <class F>
 static void run_grouped(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b,
                         const std::function<int(int)>& lvl, F&& group) {
@@ -441,39 +445,76 @@ static void run_grouped(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa
   std::vector<int> idx(n);
   for (int z = 0; z < n; z++) idx[z] = z;
   std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lvl(x) > lvl(y); });
-  std::vector<aoa_ct*> go, ga, gb;
+  std::vector<aoa_ct*> go(n), ga(n), gb(n);
+  for (int t = 0; t < n; t++) {
+    go[t] = out[idx[t]];
+    ga[t] = a[idx[t]];
+    gb[t] = b ? b[idx[t]] : a[idx[t]];
+  }
+  struct Unit {
+    int s, e, stream;
+  };
+  std::vector<Unit> groups, units;
   for (int s = 0; s < n;) {
     int e = s;
     while (e < n && lvl(idx[e]) == lvl(idx[s]) && e - s < kMaxBatch) e++;
-    go.clear(); ga.clear(); gb.clear();
-    for (int t = s; t < e; t++) {
-      go.push_back(out[idx[t]]);
-      ga.push_back(a[idx[t]]);
-      gb.push_back(b ? b[idx[t]] : a[idx[t]]);
-    }
-    const int g = e - s;
-    bool cross = false;
-    for (int u = 0; u < g && !cross; u++)
-      for (int v = 0; v < g && !cross; v++)
-        cross = (u < g / 2) != (v < g / 2) && (go[u] == ga[v] || go[u] == gb[v]);
-    if (E.tune.batch_streams == 2 && g >= 8 && !cross) {
-      if (!C.aux) {
-        AOA_CUDA(cudaStreamCreateWithFlags(&C.aux, cudaStreamNonBlocking));
-        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_fork, cudaEventDisableTiming));
-        AOA_CUDA(cudaEventCreateWithFlags(&C.ev_join, cudaEventDisableTiming));
-      }
-      const int h = g / 2;
-      AOA_CUDA(cudaEventRecord(C.ev_fork, C.stream));
-      AOA_CUDA(cudaStreamWaitEvent(C.aux, C.ev_fork, 0));
-      group(C.stream, C.batch, C.batch_bytes, h, go.data(), ga.data(), gb.data(), lvl(idx[s]));
-      group(C.aux, C.batch2, C.batch2_bytes, g - h, go.data() + h, ga.data() + h, gb.data() + h, lvl(idx[s]));
-      AOA_CUDA(cudaEventRecord(C.ev_join, C.aux));
-      AOA_CUDA(cudaStreamWaitEvent(C.stream, C.ev_join, 0));
-    } else {
-      group(C.stream, C.batch, C.batch_bytes, g, go.data(), ga.data(), gb.data(), lvl(idx[s]));
-    }
+    groups.push_back({s, e, 0});
     s = e;
   }
+  bool use_aux = false;
+  if (E.tune.batch_streams == 2) {
+    double queued[2] = {0, 0};
+    for (const Unit& g : groups) {
+      const int cnt = g.e - g.s;
+      const double cost = (double)cnt * (lvl(idx[g.s]) + 1);
+      if (cnt >= 8) {
+        units.push_back({g.s, g.s + cnt / 2, 0});
+        units.push_back({g.s + cnt / 2, g.e, 1});
+        queued[0] += cost / 2;
+        queued[1] += cost / 2;
+      } else {
+        const int st = queued[1] < queued[0] ? 1 : 0;
+        units.push_back({g.s, g.e, st});
+        queued[st] += cost;
+      }
+    }
+    for (const Unit& u : units) use_aux = use_aux || u.stream == 1;
+  }
+  if (use_aux) {                      // cross-stream hazards: outputs of one stream read or written by the other
+    std::vector<const aoa_ct*> outs[2], ins[2];
+    for (const Unit& u : units)
+      for (int t = u.s; t < u.e; t++) {
+        outs[u.stream].push_back(go[t]);
+        ins[u.stream].push_back(ga[t]);
+        ins[u.stream].push_back(gb[t]);
+      }
+    for (int x = 0; x < 2 && use_aux; x++)
+      for (const aoa_ct* o : outs[x]) {
+        for (const aoa_ct* i : ins[1 - x]) use_aux = use_aux && o != i;
+        for (const aoa_ct* o2 : outs[1 - x]) use_aux = use_aux && o != o2;
+        if (!use_aux) break;
+      }
+  }
+  if (!use_aux) {
+    for (const Unit& g : groups)
+      group(C.stream, C.batch, C.batch_bytes, g.e - g.s, go.data() + g.s, ga.data() + g.s, gb.data() + g.s,
+            lvl(idx[g.s]));
+    return;
+  }
+  if (!C.aux) {
+    AOA_CUDA(cudaStreamCreateWithFlags(&C.aux, cudaStreamNonBlocking));
+    AOA_CUDA(cudaEventCreateWithFlags(&C.ev_fork, cudaEventDisableTiming));
+    AOA_CUDA(cudaEventCreateWithFlags(&C.ev_join, cudaEventDisableTiming));
+  }
+  AOA_CUDA(cudaEventRecord(C.ev_fork, C.stream));
+  AOA_CUDA(cudaStreamWaitEvent(C.aux, C.ev_fork, 0));
+  for (const Unit& u : units) {
+    const bool aux = u.stream == 1;
+    group(aux ? C.aux : C.stream, aux ? C.batch2 : C.batch, aux ? C.batch2_bytes : C.batch_bytes, u.e - u.s,
+          go.data() + u.s, ga.data() + u.s, gb.data() + u.s, lvl(idx[u.s]));
+  }
+  AOA_CUDA(cudaEventRecord(C.ev_join, C.aux));
+  AOA_CUDA(cudaStreamWaitEvent(C.stream, C.ev_join, 0));
 }
 
 void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* const* b, const aoa_swk* evk,
