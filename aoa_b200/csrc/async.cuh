@@ -35,6 +35,17 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, unsigned
       : "memory");
 }
 
+// 4-D tensor-map tile load into shared memory (no multicast); the tensor map
+// is a __grid_constant__ kernel parameter, x * element size a multiple of 16
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int x, int y, int z, int w,
+                                            uint64_t* mb) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}],"
+      " [%6];" ::"r"(dst),
+      "l"((uint64_t)tmap), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(mb))
+      : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* mb, unsigned parity) {
   uint32_t ok;
   asm volatile(

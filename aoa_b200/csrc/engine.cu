@@ -330,6 +330,7 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   else if (k == "ntt_cols_kind" && (value == 0 || value == 1)) h->e.tune.ntt_cols_kind = (int)value;
   else if (k == "batch_streams" && (value == 1 || value == 2)) h->e.tune.batch_streams = (int)value;
   else if (k == "fuse" && value >= 0 && value <= 7 && value == (int)value) h->e.tune.fuse = (int)value;
+  else if (k == "ntt_cols_tma" && (value == 0 || value == 1)) h->e.tune.ntt_cols_tma = (int)value;
   else if (k == "spin_limit" && value >= 0 && value <= (1 << 30) && value == (int)value)
     h->e.tune.spin_limit = (int)value;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob or value out of range: " + k);
@@ -351,6 +352,7 @@ int aoa_engine_tune_get(const aoa_engine* h, const char* knob, double* value) {
   else if (k == "batch_streams") *value = t.batch_streams;
   else if (k == "fuse") *value = t.fuse;
   else if (k == "spin_limit") *value = t.spin_limit;
+  else if (k == "ntt_cols_tma") *value = t.ntt_cols_tma;
   else return fail(AOA_ERR_BAD_PARAM, "unknown knob: " + k);
   return AOA_OK;
 }

@@ -22,6 +22,8 @@
 // polys of at most the engine's chunk size (default 1 GiB: the passes are bound
 // by integer arithmetic, so fewer launch tails pay more than keeping the
 // column-pass output in L2 for the row pass).
+#include <cuda.h>   // CUtensorMap and its enums (types only; the encoder is fetched through the runtime)
+
 #include "aoa_internal.h"
 #include "async.cuh"
 
@@ -344,6 +346,7 @@ struct NttBatch {
   long src_poly_stride;
   int poly_base;           // poly index of the launch's first poly within the call
   int spin;                // polls of a bounded wait for this kernel's own copies (engine knob)
+  int use_tma;             // column pass: tiles by one tensor-map load (the kernel's tmap argument)
 };
 
 // Threads per SM the pass kernels are compiled for (register budget).
@@ -389,7 +392,7 @@ struct RowTile {
 // earlier.
 template <int LOG_R, int DIV, bool LAZY, bool FWD>
 __global__ void __launch_bounds__(ColTile<LOG_R, DIV>::THREADS, ColTile<LOG_R, DIV>::MIN_BLOCKS)
-ntt_cols(NttBatch b) {
+ntt_cols(NttBatch b, const __grid_constant__ CUtensorMap tmap) {
   using D = Sub<LOG_R>;
   constexpr int W = ColTile<LOG_R, DIV>::W;
   constexpr int TILE = D::S * W;
@@ -427,6 +430,13 @@ ntt_cols(NttBatch b) {
   // a copy may complete before thread 0's expect_tx (the transaction count
   // may go below zero until then)
   auto issue = [&](int j, int bi) {
+    if (b.use_tma) {                     // one tensor-map load of the S x W tile (rows in order: M == 0)
+      if (threadIdx.x == 0) {
+        mbar_expect_tx(&mbar[bi], TILE * 8);
+        tma_load_4d(sbuf + bi * TILE * 8, &tmap, (int)blockIdx.x * W, 0, j / b.npolys, j % b.npolys, &mbar[bi]);
+      }
+      return;
+    }
     if (threadIdx.x == 0) mbar_expect_tx(&mbar[bi], TILE * 8);
     const uint64_t* src = src_of(j);
     for (int r = threadIdx.x; r < D::S; r += blockDim.x)
@@ -828,14 +838,47 @@ static int ctas_per_tile(const Engine& E, int tiles, int items, int blocks_per_s
   return std::max(1, std::min(items, target));
 }
 
+// The column pass's tile as a 4-D tensor map over the launch's limbs: (column,
+// row, limb, poly) with strides 8 B, 8C B, 8N B and 8 N poly_stride B, box
+// (W, R, 1, 1); x = blockIdx.x W is a multiple of 16 bytes.  False when the
+// tile does not fit a box (R > 256) or the driver has no encoder.
+static bool col_tensor_map(const NttBatch& b, int W, CUtensorMap* map) {
+  using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeFn) nullptr;
+    return (EncodeFn)p;
+  }();
+  const long R = 1L << b.log_r, C = 1L << b.log_c, N = 1L << b.log_n;
+  if (!encode || R > 256 || W * 8 % 16) return false;
+  const uint64_t* base = b.src ? b.src : b.data;
+  const long pstride = b.src ? b.src_poly_stride : b.poly_stride;
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)R, (cuuint64_t)(b.nitems / b.npolys), (cuuint64_t)b.npolys};
+  const cuuint64_t strides[3] = {(cuuint64_t)C * 8, (cuuint64_t)N * 8, (cuuint64_t)pstride * N * 8};
+  const cuuint32_t box[4] = {(cuuint32_t)W, (cuuint32_t)R, 1, 1};
+  const cuuint32_t estride[4] = {1, 1, 1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, (void*)base, dims, strides, box, estride,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int LOG_R, int DIV, bool LAZY>
-static void launch_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
+static void launch_cols(const Engine& E, const NttBatch& b0, bool fwd, cudaStream_t st) {
   using Tl = ColTile<LOG_R, DIV>;
-  const int C = 1 << b.log_c;
+  const int C = 1 << b0.log_c;
   if (C % Tl::W) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: column tile does not divide C");
+  NttBatch b = b0;
+  CUtensorMap map{};
+  // a tensor-map tile load needs the rows of the tile in order (no row swizzle: W = 16)
+  b.use_tma = E.tune.ntt_cols_tma && Tl::W == 16 && col_tensor_map(b, Tl::W, &map) ? 1 : 0;
   dim3 grid(C / Tl::W, ctas_per_tile(E, C / Tl::W, b.nitems, Tl::MIN_BLOCKS));
-  if (fwd) ntt_cols<LOG_R, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
-  else ntt_cols<LOG_R, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b);
+  if (fwd) ntt_cols<LOG_R, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, map);
+  else ntt_cols<LOG_R, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, map);
   note_launch();
 }
 
@@ -1016,7 +1059,7 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   b.log_c = std::max(std::max(5, T.log_n - 10), std::min(std::min(10, T.log_n - 5), b.log_c));
   b.log_r = T.log_n - b.log_c;
   b.first_prime = first_prime; b.prime_shift = T.prime_shift; b.poly_stride = poly_stride;
-  b.src = nullptr; b.src_poly_stride = 0; b.poly_base = 0;
+  b.src = nullptr; b.src_poly_stride = 0; b.poly_base = 0; b.use_tma = 0;
   const long n = 1L << T.log_n;
   if (T.log_n < 10) {
     // small rings: the out-of-place source is copied first and the epilogue

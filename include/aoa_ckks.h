@@ -99,6 +99,8 @@ int aoa_engine_destroy(aoa_engine* e);
  * -2..2, default 0), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width
  * and row-pass tile height = widest >> div, 0..2, defaults 0 / 1),
  * "ntt_cols_kind" (0 CTA-wide exchange, 1 warp-owned columns; default 0),
+ * "ntt_cols_tma" (1: the column pass loads 16-column tiles with one
+ * tensor-map load, 0: one bulk copy per tile row; default 1),
  * "fuse" (bit mask of fused transform ends: 1 out-of-place inverse, 2 key
  * products, 4 key-switch combine; default 1), "batch_streams" (1 or 2
  * streams for a batched HMult group of 8 or more; default 2),

@@ -140,6 +140,47 @@ def test_ntt_prime_size_edges(bits, shape):
     assert np.array_equal(d.numpy(), x), "inverse(forward(x)) != x"
 
 
+@pytest.mark.parametrize("log_n,split", [(12, 0), (15, -1), (16, 0), (16, 1), (17, 0)])
+@pytest.mark.parametrize("src", [False, True])
+def test_column_tiles_by_tensor_map_equal_row_copies(log_n, split, src):
+    """The column pass's 16-column tiles loaded by one tensor-map (TMA) load
+    (knob ntt_cols_tma, the default) and by one bulk copy per tile row give
+    the oracle's transforms, for strided polys in several launch chunks and
+    for the out-of-place first pass of HMult's inverse of d2."""
+    require_gpu()
+    import aoa_b200 as aoa
+    ps = oracle.gen_ntt_primes(60, 2 << log_n, 5)
+    E, ctx, o = _engine_and_oracle(log_n, ps[:3], ps[3:])
+    E.tune("ntt_split", split)
+    E.tune("ntt_chunk_bytes", max(1 << 20, 2 * 4 * (8 << log_n)))   # two polys per launch pair from 2^15
+    rng = np.random.default_rng(log_n + 3 * split)
+    x = _rand(rng, ps, 1 << log_n, npolys=5)
+    res = []
+    for tma in (1, 0):
+        E.tune("ntt_cols_tma", tma)
+        d = ctx.upload(x)
+        ctx.ntt_fwd(d, 5, 0, 4, poly_stride=5)                    # limbs 0..3 of stride-5 polys
+        res.append(d.numpy())
+        ctx.ntt_inv(d, 5, 0, 4, poly_stride=5)
+        assert np.array_equal(d.numpy(), x), tma
+    assert np.array_equal(res[0], res[1])
+    for p in range(5):
+        assert np.array_equal(res[0][p, :4], o.ntt_fwd(x[p, :4]))
+        assert np.array_equal(res[0][p, 4], x[p, 4])              # untouched limb
+    if src:                                                      # HMult with the out-of-place inverse
+        keys_rng = np.random.default_rng(5)
+        evk = aoa.SwitchKey(ctx, _rand(keys_rng, ps, 1 << log_n)[0], _rand(keys_rng, ps, 1 << log_n)[0])
+        outs = []
+        for tma in (1, 0):
+            E.tune("ntt_cols_tma", tma)
+            ca = aoa.Ciphertext.from_residues(ctx, x[0, :3], x[1, :3], slots=4, domain=aoa.AOA_NTT)
+            cb = aoa.Ciphertext.from_residues(ctx, x[2, :3], x[3, :3], slots=4, domain=aoa.AOA_NTT)
+            out = aoa.Ciphertext(ctx)
+            aoa.ckks_mul(ctx, out, ca, cb, evk)
+            outs.append(out.download(nlimbs=2))
+        assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
 def test_autotune_keeps_results_bit_exact():
     require_gpu()
     ps = oracle.gen_ntt_primes(60, 1 << 15, 6)
