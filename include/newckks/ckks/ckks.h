@@ -28,6 +28,12 @@
 
 #include "aoa_ckks.h"
 
+// The transform of the evaluator this header stands in for: the NTT of
+// newckks, or the DGT of AOADGT (set by AOADGT/ckks.h before including this).
+#ifndef AOA_SHIM_TRANSFORM
+#define AOA_SHIM_TRANSFORM AOA_NTT
+#endif
+
 namespace aoa_shim {
 
 // The reference's exceptions for the same conditions (ckks.cpp:224-227, 284-290).
@@ -114,6 +120,7 @@ class CKKSContext {
   CKKSContext() {
     if (!CUDAManager::is_init) throw std::runtime_error("CUDAManager::init must come first");
     aoa_shim::check(aoa_ctx_create(CUDAManager::engine, nullptr, &ctx));
+    if (AOA_SHIM_TRANSFORM == AOA_DGT) aoa_shim::check(aoa_ctx_set_transform(ctx, AOA_DGT));
   }
   ~CKKSContext() {
     if (ctx) aoa_ctx_destroy(ctx);
@@ -180,10 +187,12 @@ inline void cipher_copy_to_host(CKKSContext* x, const cipher_t* c, uint64_t* hos
   aoa_shim::check(aoa_ct_download(x->ctx, c->ct, host, nlimbs, AOA_COEF));
 }
 // Switching keys given as residues (b then a, (k + kl) limbs each), in the
-// reference's storage domain (its keys are kept in TRANSSTATE)
-inline SwitchKey* ckks_load_switchkey(CKKSContext* x, const uint64_t* b, const uint64_t* a, bool ntt_domain = true) {
+// reference's storage domain (its keys are kept in TRANSSTATE: the NTT domain
+// of newckks, the DGT domain of AOADGT) or in coefficients
+inline SwitchKey* ckks_load_switchkey(CKKSContext* x, const uint64_t* b, const uint64_t* a,
+                                      bool transform_domain = true) {
   SwitchKey* k = new SwitchKey;
-  aoa_shim::check(aoa_swk_create(x->ctx, b, a, ntt_domain ? AOA_NTT : AOA_COEF, &k->k));
+  aoa_shim::check(aoa_swk_create(x->ctx, b, a, transform_domain ? AOA_SHIM_TRANSFORM : AOA_COEF, &k->k));
   return k;
 }
 inline void ckks_free_switchkey(CKKSContext* x, SwitchKey* k) {

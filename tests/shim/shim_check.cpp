@@ -1,17 +1,24 @@
 // A caller written against the reference evaluator's signatures
 // (aoa-ntt include/newckks/ckks/ckks.h), compiled against the shim header
-// include/newckks/ckks/ckks.h and linked with libaoa_b200.so.
+// include/newckks/ckks/ckks.h and linked with libaoa_b200.so; built with
+// -DSHIM_DGT it includes AOADGT/ckks.h instead and initialises through
+// CUDAEngine::init, as a caller of aoa-dgt does.
 //
 // usage: shim_check <input file> <output file>
-// input (u64 words): log_n k kl prec slots r scale1 scale2 | k + kl primes |
-//   evk b, a | rtk_left[r] b, a | rtk_right[r] b, a   ((k + kl) x N each, NTT domain)
+// input (u64 words): log_n k kl prec slots r scale1 scale2 keys_in_transform_domain |
+//   k + kl primes | evk b, a | rtk_left[r] b, a | rtk_right[r] b, a
+//   ((k + kl) x N each, in the evaluator's transform domain or in coefficients)
 //   | c1 (2 x k x N) | c2 (2 x k x N)                   (coefficients)
 // output (u64 words): for ckks_mul, ckks_rotate_left, ckks_rotate_right,
 //   ckks_rescale (of c1), ckks_add (c1 + c2), ckks_sub (c1 - c2): level,
 //   slots, scale, then 2 x (level + 1) x N coefficient residues.
 // Exit status 0 only if every call ran and every error case threw as the
 // reference does; messages go to stderr.
+#ifdef SHIM_DGT
+#include <AOADGT/ckks.h>
+#else
 #include <newckks/ckks/ckks.h>
+#endif
 
 #include <cstdio>
 #include <cstring>
@@ -62,10 +69,11 @@ int main(int argc, char** argv) {
     at += n;
     return p;
   };
-  const uint64_t* hdr = take(8);
+  const uint64_t* hdr = take(9);
   const int log_n = (int)hdr[0], k = (int)hdr[1], kl = (int)hdr[2], prec = (int)hdr[3], slots = (int)hdr[4];
   const int r = (int)hdr[5];
   const int64_t scale1 = (int64_t)hdr[6], scale2 = (int64_t)hdr[7];
+  const bool keys_transform = hdr[8] != 0;
   const long N = 1L << log_n;
   const size_t qb = (size_t)(k + kl) * N, ct = (size_t)2 * k * N;
   const uint64_t* p = take(k + kl);
@@ -77,11 +85,15 @@ int main(int argc, char** argv) {
 
   bool ok = true;
   try {
+#ifdef SHIM_DGT
+    CUDAEngine::init(k, kl, (int)(2 * N), (uint64_t)prec, primes);
+#else
     CUDAManager::init(k, kl, (int)N, prec, primes);
+#endif
     CKKSContext* ctx = new CKKSContext();
-    ctx->keys.evk = ckks_load_switchkey(ctx, evk_b, evk_a);
-    ctx->keys.rtk_left[r] = ckks_load_switchkey(ctx, rl_b, rl_a);
-    ctx->keys.rtk_right[r] = ckks_load_switchkey(ctx, rr_b, rr_a);
+    ctx->keys.evk = ckks_load_switchkey(ctx, evk_b, evk_a, keys_transform);
+    ctx->keys.rtk_left[r] = ckks_load_switchkey(ctx, rl_b, rl_a, keys_transform);
+    ctx->keys.rtk_right[r] = ckks_load_switchkey(ctx, rr_b, rr_a, keys_transform);
 
     cipher_t c1, c2;
     cipher_init(ctx, &c1, slots);
@@ -155,7 +167,11 @@ int main(int argc, char** argv) {
     ckks_free_switchkey(ctx, ctx->keys.rtk_left[r]);
     ckks_free_switchkey(ctx, ctx->keys.rtk_right[r]);
     delete ctx;
+#ifdef SHIM_DGT
+    CUDAEngine::destroy();
+#else
     CUDAManager::destroy();
+#endif
   } catch (const std::exception& e) {
     std::cerr << "shim_check: " << e.what() << "\n";
     return 1;

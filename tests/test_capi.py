@@ -44,13 +44,16 @@ def test_engine_create_fails_cleanly_without_gpu_or_bad_params():
 
 
 def test_reference_signature_shim_compiles_and_links(tmp_path):
-    """The C++ shim (include/newckks/ckks/ckks.h) and a caller written against
-    the reference's signatures build and link against libaoa_b200.so with
-    plain g++ (running it needs a GPU: tests/test_gpu_shim.py)."""
+    """The C++ shims (include/newckks/ckks/ckks.h, include/AOADGT/ckks.h) and a
+    caller written against the reference's signatures build and link against
+    libaoa_b200.so with plain g++ (running it needs a GPU:
+    tests/test_gpu_shim.py)."""
     import subprocess
     import aoa_b200.build as build
     lib = os.path.dirname(build.build())
-    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
-                           os.path.join(ROOT, "tests", "shim", "shim_check.cpp"), "-L", lib, "-laoa_b200",
-                           "-Wl,-rpath," + lib, "-o", str(tmp_path / "shim_check")])
-    assert os.path.exists(tmp_path / "shim_check")
+    for flags, exe in (([], "shim_check"), (["-DSHIM_DGT"], "shim_check_dgt")):
+        subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Werror"] + flags +
+                              ["-I", os.path.join(ROOT, "include"),
+                               os.path.join(ROOT, "tests", "shim", "shim_check.cpp"), "-L", lib, "-laoa_b200",
+                               "-Wl,-rpath," + lib, "-o", str(tmp_path / exe)])
+        assert os.path.exists(tmp_path / exe)

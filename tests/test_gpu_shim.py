@@ -1,6 +1,7 @@
 """The drop-in boundary compiled: a C++ caller written against the reference
-evaluator's signatures (aoa-ntt include/newckks/ckks/ckks.h:116-314) builds
-against the shim header include/newckks/ckks/ckks.h, links libaoa_b200.so and
+evaluator's signatures (aoa-ntt include/newckks/ckks/ckks.h:116-314; the
+same names in aoa-dgt include/AOADGT/ckks.h) builds against the shim headers
+include/newckks/ckks/ckks.h and include/AOADGT/ckks.h, links libaoa_b200.so and
 runs ckks_mul, ckks_rotate_left / ckks_rotate_right, ckks_rescale,
 ckks_add / ckks_sub and the reference's error cases on the GPU
 (tests/shim/shim_check.cpp).  Its outputs must equal the oracle's."""
@@ -20,18 +21,22 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _build(tmp_path):
+def _build(tmp_path, dgt=False):
     lib = os.path.join(ROOT, "aoa_b200", "lib")
-    exe = str(tmp_path / "shim_check")
-    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+    exe = str(tmp_path / ("shim_check_dgt" if dgt else "shim_check"))
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-Wall", "-Werror"] + (["-DSHIM_DGT"] if dgt else []) +
+                          ["-I", os.path.join(ROOT, "include"),
                            os.path.join(ROOT, "tests", "shim", "shim_check.cpp"), "-L", lib, "-laoa_b200",
                            "-Wl,-rpath," + lib, "-o", exe])
     return exe
 
 
-def test_reference_signature_caller_compiles_and_matches_oracle(tmp_path):
+@pytest.mark.parametrize("dgt", [False, True])
+def test_reference_signature_caller_compiles_and_matches_oracle(tmp_path, dgt):
+    """newckks callers (NTT) and, with -DSHIM_DGT, AOADGT callers (the same
+    names on a DGT context, CUDAEngine::init, keys given in coefficients)."""
     require_gpu()
-    exe = _build(tmp_path)
+    exe = _build(tmp_path, dgt)
     log_n, k, kl, prec = 12, 5, 6, 40
     N = 1 << log_n
     ps = oracle.gen_ntt_primes(60, 1 << 13, k + kl)
@@ -42,9 +47,10 @@ def test_reference_signature_caller_compiles_and_matches_oracle(tmp_path):
     c1 = (uniform_residues(rng, ps[:k], N), uniform_residues(rng, ps[:k], N))
     c2 = (uniform_residues(rng, ps[:k], N), uniform_residues(rng, ps[:k], N))
     slots, s1, s2 = 8, (1 << 40) + 5, (1 << 40) + 9
-    words = [np.array([log_n, k, kl, prec, slots, r, s1, s2] + ps, dtype=np.uint64)]
+    words = [np.array([log_n, k, kl, prec, slots, r, s1, s2, 0 if dgt else 1] + ps, dtype=np.uint64)]
     for key in (keys["evk"], keys["rtk"][r], keys["rtk"][N // 2 - r]):
-        words += [key[0].ravel(), key[1].ravel()]
+        kb, ka = (o.ntt_inv(key[0]), o.ntt_inv(key[1])) if dgt else key
+        words += [kb.ravel(), ka.ravel()]
     words += [np.concatenate([c1[0], c1[1]]).ravel(), np.concatenate([c2[0], c2[1]]).ravel()]
     src, dst = tmp_path / "in.bin", tmp_path / "out.bin"
     np.concatenate(words).astype(np.uint64).tofile(src)
