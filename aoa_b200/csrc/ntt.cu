@@ -1051,6 +1051,10 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   const NttEpi no_epi{};
   const NttEpi& epi = io ? io->epi : no_epi;
   if (epi.mode != kEpiStore && !forward) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: epilogues are for forward transforms");
+  // the passes move tiles with bulk / tensor-map copies, which need 16-byte
+  // aligned addresses: limbs start at data + multiples of N words (N >= 2^10)
+  if (((uintptr_t)data & 15) || (io && io->src && ((uintptr_t)io->src & 15)))
+    throw AoaError(AOA_ERR_BAD_PARAM, "ntt: device data must be 16-byte aligned");
   NttBatch b;
   b.tw = T.tw; b.itw = T.itw; b.pc = T.pc; b.err = E.d_err;
   b.spin = E.tune.spin_limit;

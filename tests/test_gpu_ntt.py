@@ -194,3 +194,26 @@ def test_autotune_keeps_results_bit_exact():
     d = ctx.upload(x)
     ctx.ntt_fwd(d, 2, 0, 6)
     assert np.array_equal(d.numpy()[1], o.ntt_fwd(x[1]))
+
+
+def test_misaligned_device_pointer_is_rejected():
+    """The transform passes copy tiles with bulk / tensor-map copies, which need
+    16-byte aligned addresses: a pointer 8 bytes into an allocation is refused
+    on the host (AOA_ERR_BAD_PARAM) before any kernel runs, and the context
+    stays usable."""
+    require_gpu()
+    import ctypes
+    import aoa_b200 as aoa
+    ps = oracle.gen_ntt_primes(60, 1 << 13, 3)
+    E, ctx, o = _engine_and_oracle(12, ps[:2], ps[2:])
+    rng = np.random.default_rng(9)
+    x = _rand(rng, ps, 1 << 12)
+    d = ctx.upload(np.concatenate([np.zeros(1, np.uint64), x.ravel()]))
+    lib = aoa.capi.load()
+    for fn in (lib.aoa_ntt_fwd, lib.aoa_ntt_inv):
+        st = fn(ctx.handle, ctypes.c_void_p(d.ptr.value + 8), 1, 0, 3, 3)
+        assert st == 1 and "aligned" in lib.aoa_last_error().decode()
+    ctx.sync()
+    d2 = ctx.upload(x)
+    ctx.ntt_fwd(d2, 1, 0, 3)
+    assert np.array_equal(d2.numpy()[0], o.ntt_fwd(x[0]))
