@@ -232,3 +232,6 @@ inline ZZ PowerMod(const ZZ& a, const ZZ& e, const ZZ& n) {
 inline ZZ PowerMod(const ZZ& a, long e, const ZZ& n) { return PowerMod(a, ZZ(e), n); }
 
 }  // namespace NTL
+
+// NTL_CLIENT brings both namespaces into scope, as NTL's own definition does
+#define NTL_CLIENT using namespace std; using namespace NTL;

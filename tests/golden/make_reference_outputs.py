@@ -9,9 +9,16 @@ tests/golden/reference_outputs.npz, which tests/test_oracle_reference_outputs.py
 compares with the oracle (the inputs are regenerated there from the seeds the
 harness documents, so the fixture holds outputs only).
 
-Usage (on a machine with a GPU and the built harness):
+oracle/_ref/ref_ckks_harness runs the reference's CKKS layer (HMult with and
+without rescale, rotation, conjugation, addition, subtraction and the encoder
+on seeded operands; then its own key generation, encryption, HMult, rotation
+and decryption) for CKKS_CONFIGS; its records go to
+tests/golden/reference_ckks_outputs.npz (tests/test_oracle_reference_ckks.py).
+
+Usage (on a machine with a GPU and the built harnesses):
     python tests/golden/make_reference_outputs.py OUT_DIR
-writes OUT_DIR/reference_outputs.npz (copy it into tests/golden/).
+writes OUT_DIR/reference_outputs.npz and OUT_DIR/reference_ckks_outputs.npz
+(copy them into tests/golden/).
 """
 import os
 import subprocess
@@ -21,6 +28,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+CKKS_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_ckks_harness")
 
 # (log2 N, k, kl, prec, transforms only): the reference's hierarchical
 # transforms at 2^10 (32 x 32) and 2^12 (64 x 64) on its own prime choice
@@ -28,6 +36,12 @@ HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 # 55-bit bucket), ModUp / ModDown / rescale at 2^10
 CONFIGS = [(10, 4, 5, 55, 0), (12, 3, 4, 52, 1)]
 TAGS = {1: "ntt_fwd", 2: "ntt_inv", 3: "modup", 4: "moddown", 5: "rescale", 6: "modup_max", 7: "ntt_fwd_max"}
+
+# (log2 N, k, kl, prec) of the CKKS-layer records
+CKKS_CONFIGS = [(10, 4, 5, 55)]
+CKKS_TAGS = {20: "hmult_l%d", 21: "hmult_norescale_l%d", 23: "conjugate_l%d", 24: "add_l%d", 25: "sub_l%d",
+             26: "encode_s%d", 40: "sk", 41: "evk", 42: "enc300", 43: "enc301", 44: "mul_keys", 45: "dec300",
+             46: "dec_mul", 47: "rot1_keys", 48: "dec_rot1"}
 
 
 def parse(path):
@@ -40,6 +54,28 @@ def parse(path):
     while at < w.size:
         tag, level, n = (int(v) for v in w[at:at + 3])
         recs["%s_l%d" % (TAGS[tag], level)] = w[at + 3:at + 3 + n].copy()
+        at += 3 + n
+    return N, k, kl, prec, primes, recs
+
+
+def parse_ckks(path):
+    """Records of ref_ckks_harness; ciphertext records keep their
+    [aux, scale, slots, c0 limbs, c1 limbs] words."""
+    w = np.fromfile(path, dtype=np.uint64)
+    assert w[:1].tobytes() == b"AOAREF02", "not a CKKS harness output"
+    N, k, kl, prec = (int(v) for v in w[1:5])
+    primes = w[5:5 + k + kl].copy()
+    at = 5 + k + kl
+    recs = {}
+    while at < w.size:
+        tag, level, n = (int(v) for v in w[at:at + 3])
+        words = w[at + 3:at + 3 + n].copy()
+        if tag == 22:
+            name = "rotate%d_l%d" % (int(words[0]), level)
+        else:
+            name = CKKS_TAGS[tag] % level if "%d" in CKKS_TAGS[tag] else CKKS_TAGS[tag]
+        assert name not in recs, name
+        recs[name] = words
         at += 3 + n
     return N, k, kl, prec, primes, recs
 
@@ -60,6 +96,19 @@ def main():
         for name, v in recs.items():
             arrays["%s_%s" % (tag, name)] = v
     dst = os.path.join(out_dir, "reference_outputs.npz")
+    np.savez_compressed(dst, **arrays)
+    print("wrote", dst, sorted(arrays))
+    arrays = {}
+    for log_n, k, kl, prec in CKKS_CONFIGS:
+        path = os.path.join(out_dir, "ref_ckks_n%d.bin" % (1 << log_n))
+        subprocess.check_call([CKKS_HARNESS, path, str(log_n), str(k), str(kl), str(prec)])
+        N, k2, kl2, prec2, primes, recs = parse_ckks(path)
+        tag = "n%d" % N
+        arrays[tag + "_params"] = np.array([N, k2, kl2, prec2], dtype=np.uint64)
+        arrays[tag + "_primes"] = primes
+        for name, v in recs.items():
+            arrays["%s_%s" % (tag, name)] = v
+    dst = os.path.join(out_dir, "reference_ckks_outputs.npz")
     np.savez_compressed(dst, **arrays)
     print("wrote", dst, sorted(arrays))
 
