@@ -383,6 +383,17 @@ def ckks_mul_plain(ctx, c3, c1, c2, evk):
     capi.check(capi.load().aoa_hmult_plain(ctx.handle, c3.handle, c1.handle, c2.handle, _h(evk)))
 
 
+def ckks_rotate_plain(ctx, c2, c1, steps, rtk):
+    """The reference's per-call ckks_rotate_left sequence on this engine
+    (comparison path; output in coefficients)."""
+    capi.check(capi.load().aoa_rotate_plain(ctx.handle, c2.handle, c1.handle, steps, _h(rtk)))
+
+
+def ckks_conjugate_plain(ctx, c2, c1, cjk):
+    """The reference's per-call ckks_conjugate sequence on this engine (comparison path)."""
+    capi.check(capi.load().aoa_conjugate_plain(ctx.handle, c2.handle, c1.handle, _h(cjk)))
+
+
 def ckks_mul_batch(ctx, outs, c1s, c2s, evk, rescale=True):
     """outs[i] = c1s[i] * c2s[i] (+ relinearise, + rescale) in grouped batched launches."""
     n = len(outs)

@@ -80,6 +80,8 @@ SIGNATURES = {
     "aoa_hmult": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_hmult_relin_rescale": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_hmult_plain": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "aoa_rotate_plain": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "aoa_conjugate_plain": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_hmult_relin_rescale_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_hmult_batch": (c_int, [c_void_p, c_int, vpp, vpp, vpp, c_void_p, c_int]),
     "aoa_rescale": (c_int, [c_void_p, c_void_p]),

@@ -642,6 +642,23 @@ struct PlainWs {
   uint64_t *axbx1, *axbx2, *bxbx, *axax, *qb, *t0, *t1;
 };
 
+// the plain paths' workspace: four Q polys and three QB polys
+static PlainWs plain_ws(Ctx& C) {
+  const Engine& E = *C.E;
+  const long half = (long)E.k * E.N, qb = (long)(E.k + E.kl) * E.N;
+  if (!C.plain || C.plain_bytes < (size_t)(4 * half + 3 * qb) * 8) {
+    if (C.plain) AOA_CUDA(cudaFreeAsync(C.plain, C.stream));
+    C.plain = nullptr;
+    if (cudaMallocAsync(&C.plain, (size_t)(4 * half + 3 * qb) * 8, C.stream) != cudaSuccess) {
+      cudaGetLastError();
+      throw AoaError(AOA_ERR_OOM, "plain-path workspace allocation failed");
+    }
+    C.plain_bytes = (size_t)(4 * half + 3 * qb) * 8;
+  }
+  uint64_t* p = (uint64_t*)C.plain;
+  return PlainWs{p, p + half, p + 2 * half, p + 3 * half, p + 4 * half, p + 4 * half + qb, p + 4 * half + 2 * qb};
+}
+
 void hmult_plain(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) {
   const Engine& E = *C.E;
   const long N = E.N;
@@ -656,17 +673,7 @@ void hmult_plain(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) 
   const int k = E.k, nqb = E.k + E.kl;
   const int level = std::min(a->level, b->level);
   const long half = (long)k * N, qb = (long)nqb * N;
-  if (!C.plain || C.plain_bytes < (size_t)(4 * half + 3 * qb) * 8) {
-    if (C.plain) AOA_CUDA(cudaFreeAsync(C.plain, C.stream));
-    C.plain = nullptr;
-    if (cudaMallocAsync(&C.plain, (size_t)(4 * half + 3 * qb) * 8, C.stream) != cudaSuccess) {
-      cudaGetLastError();
-      throw AoaError(AOA_ERR_OOM, "plain-path workspace allocation failed");
-    }
-    C.plain_bytes = (size_t)(4 * half + 3 * qb) * 8;
-  }
-  uint64_t* p = (uint64_t*)C.plain;
-  PlainWs s{p, p + half, p + 2 * half, p + 3 * half, p + 4 * half, p + 4 * half + qb, p + 4 * half + 2 * qb};
+  const PlainWs s = plain_ws(C);
   cudaStream_t st = C.stream;
   int a_dom = a->domain, b_dom = b->domain;
   // poly_add_add(axbx1 = c1[1] + c1[0], axbx2 = c2[1] + c2[0]) in the operands' domain
@@ -709,6 +716,62 @@ void hmult_plain(Ctx& C, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk) 
   out->level = level - 1;
   out->slots = slots;
   out->scale = scale_after_mult(E, sa, sb, level);
+  out->domain = AOA_COEF;
+}
+
+// The reference's per-call rotation / conjugation sequence on this engine's
+// kernels (ckks_rotate_left, ckks.cpp:982-1009, with rotate_slots_left,
+// encoder.cu:325-350; ckks_conjugate, ckks.cpp:1011-1040): both input polys
+// back to coefficients over the whole Q base, the coefficient permutation
+// X -> X^g with its sign, ModUp of the permuted c1 into a QB poly, a forward
+// transform of the whole QB poly, the two key products, inverse transforms
+// of both whole QB products, two ModDowns, and c0' + ks0; the output is in
+// coefficients.  The reference transforms its input in place; here the
+// inverse reads the input out of place (the same work), so the input keeps
+// its domain.  The plain per-call baseline of the uneven benchmark beside
+// hmult_plain; apply_galois is the engine's own path.
+void galois_plain(Ctx& C, aoa_ct* out, aoa_ct* in, long galois, const aoa_swk* key) {
+  const Engine& E = *C.E;
+  const long N = E.N;
+  if (!key || !key->d) throw AoaError(AOA_ERR_NO_KEY, "missing switching key for this automorphism");
+  if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
+  if (C.transform != AOA_NTT || key->domain != AOA_NTT)
+    throw AoaError(AOA_ERR_BAD_PARAM, "the reference-structured path runs on the NTT transform only");
+  const int k = E.k, nqb = E.k + E.kl;
+  const int level = in->level, slots = in->slots;
+  const uint64_t scale = in->scale;
+  const long half = (long)k * N, qb = (long)nqb * N;
+  const PlainWs s = plain_ws(C);
+  cudaStream_t st = C.stream;
+  // rotate_slots_left on c0 and c1: the input in coefficients (full base), then the map
+  if (in->domain == AOA_DGT) throw AoaError(AOA_ERR_BAD_PARAM, "the reference-structured path runs on the NTT transform only");
+  const uint64_t* coef = in->d;
+  if (in->domain == AOA_NTT) {
+    NttIo io;
+    io.src = in->d;
+    io.src_poly_stride = k;
+    ntt_batch_io(E, s.t0, 2, 0, k, k, false, io, st);     // both polys into t0 / t0 + half
+    coef = s.t0;
+  }
+  automorph_coef_op(E, s.bxbx, coef, 0, galois, k, 1, st);
+  automorph_coef_op(E, s.axax, coef + half, 0, galois, k, 1, st);
+  // poly_modup(d2axaxQB, axax, level)
+  copy_limbs(C, s.qb, s.axax, half);
+  modup(E, s.qb, 0, s.qb + half, 0, 1, level, st);
+  // poly_mul with rtk.b / rtk.a over QB: the QB poly to the transform domain
+  ntt_batch(E, s.qb, 1, 0, nqb, nqb, true, st);
+  ew_binary_op(E, s.t0, 0, s.qb, 0, key->d, 0, 2, 0, nqb, 1, st);
+  ew_binary_op(E, s.t1, 0, s.qb, 0, key->d + qb, 0, 2, 0, nqb, 1, st);
+  // poly_moddown x2: full QB inverse transforms, then B -> Q
+  ntt_batch(E, s.t0, 2, 0, nqb, nqb, false, st);
+  moddown(E, s.t0, s.t0 + half, 0, s.t0, 0, 1, level, st);
+  moddown(E, s.t1, s.t1 + half, 0, s.t1, 0, 1, level, st);
+  // c2.c0 = rotated c0 + ks0; c2.c1 = ks1
+  ew_binary_op(E, out->d, 0, s.bxbx, 0, s.t0, 0, 0, 0, k, 1, st);
+  copy_limbs(C, out->d + half, s.t1, half);
+  out->level = level;
+  out->slots = slots;
+  out->scale = scale;
   out->domain = AOA_COEF;
 }
 
@@ -954,6 +1017,21 @@ int aoa_conjugate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk) {
   if (!c || !out || !in) return fail(AOA_ERR_BAD_PARAM, "null argument");
   return guarded([&] { apply_galois(c->c, out, in, 2 * c->c.E->N - 1, cjk); });
+}
+
+int aoa_rotate_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk) {
+  if (!c || !out || !in) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    long r = steps % (E.N / 2);
+    if (r < 0) r += E.N / 2;
+    galois_plain(c->c, out, in, (long)h_powmod(5, (uint64_t)r, (uint64_t)(2 * E.N)), rtk);
+  });
+}
+
+int aoa_conjugate_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk) {
+  if (!c || !out || !in) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] { galois_plain(c->c, out, in, 2 * c->c.E->N - 1, cjk); });
 }
 
 // Standalone basis conversions on device buffers (coefficient domain):

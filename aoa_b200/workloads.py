@@ -25,7 +25,7 @@ import time
 import numpy as np
 
 from . import (AOA_COEF, AOA_NTT, Ciphertext, Context, Engine, Graph, SwitchKey, ckks_add, ckks_encode,
-               ckks_mul_batch, ckks_mul_plain, ckks_mul_pt, ckks_rescale, ckks_rotate_batch, ckks_rotate_left,
+               ckks_mul_batch, ckks_mul_plain, ckks_mul_pt, ckks_rescale, ckks_rotate_batch, ckks_rotate_plain,
                ckks_sumslots, params)
 
 
@@ -120,7 +120,7 @@ class UnevenBatch:
 
     def run_plain(self):
         """The reference's per-call sequence, one op at a time in input order
-        (HMult through the reference-structured path)."""
+        (HMult and rotations through the reference-structured paths)."""
         for z, op in enumerate(self.ops):
             ln = op["log_n"]
             ctx = self.ctx[ln]
@@ -128,7 +128,7 @@ class UnevenBatch:
             if op["kind"] == "mul":
                 ckks_mul_plain(ctx, self.outs[z], args[0], args[1], self.evk[ln])
             elif op["kind"] == "rot":
-                ckks_rotate_left(ctx, self.outs[z], args[0], op["step"], self.rtk[ln][op["step"]])
+                ckks_rotate_plain(ctx, self.outs[z], args[0], op["step"], self.rtk[ln][op["step"]])
             else:
                 ckks_add(ctx, self.outs[z], args[0], args[1])
 

@@ -338,6 +338,8 @@ def systems_workloads(aoa, torch):
               "graph_nodes": nodes, "algorithmic_bytes": wb.bytes,
               "achieved_gbs": wb.bytes / (graph_ms / 1000.0) / 1e9,
               "rotation_keys": "a distinct key per step 2^j and degree",
+              "plain": "one op at a time in input order: HMult and rotations through the reference's per-call "
+                       "sequences on this engine (aoa_hmult_plain, aoa_rotate_plain), additions as ckks_add",
               "schedule": "one stream per N; HMults grouped by limb count (<=64 per launch), rotations batched "
                           "per step (grouped by limb count), additions; one CUDA graph per stream"}
     del wb

@@ -270,6 +270,16 @@ int aoa_hmult_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* a, aoa
  * on this engine's kernels; same residues as aoa_hmult_relin_rescale, output
  * in coefficients.  The plain per-call baseline of the benchmarks.           */
 int aoa_hmult_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* a, aoa_ct* b, const aoa_swk* evk);
+/* The reference's per-call rotation and conjugation sequences
+ * (ckks_rotate_left, ckks.cpp:982-1009, with rotate_slots_left,
+ * encoder.cu:325-350; ckks_conjugate, ckks.cpp:1011-1040: the input back to
+ * coefficients over the full base, the coefficient permutation, ModUp, whole-
+ * QB transforms, unfused key products and ModDowns) on this engine's kernels;
+ * same residues as aoa_rotate / aoa_conjugate, output in coefficients.  The
+ * input keeps its domain (its inverse transform reads it out of place).  Steps
+ * as in aoa_rotate.  The plain per-call baselines beside aoa_hmult_plain.    */
+int aoa_rotate_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rtk);
+int aoa_conjugate_plain(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk);
 /* HMult + relinearise + rescale that allocates nothing.  No counterpart in the
  * reference.  For callers that may not allocate device memory while they
  * evaluate (an application that owns the whole device memory budget through

@@ -168,6 +168,15 @@ def test_rotate_conjugate_bit_exact(ref_table, pset):
         w0, w1 = o.rotate_left((c0, c1), r, keys["rtk"][r], k - 1, state=ST_COEF)
         g0, g1 = out.download(nlimbs=k)
         assert np.array_equal(g0, w0) and np.array_equal(g1, w1), r
+        # the reference's per-call sequence, from coefficient and transform-domain inputs
+        for dom in (aoa.AOA_COEF, aoa.AOA_NTT):
+            ct = aoa.Ciphertext.from_residues(ctx, c0, c1, slots=N // 2)
+            ct.upload(*(ct.download(nlimbs=k, domain=dom)), domain=dom)
+            out = aoa.Ciphertext(ctx)
+            aoa.ckks_rotate_plain(ctx, out, ct, r, rtk)
+            assert out.domain == aoa.AOA_COEF and ct.domain == dom
+            g0, g1 = out.download(nlimbs=k)
+            assert np.array_equal(g0, w0) and np.array_equal(g1, w1), (r, dom)
     cjk = aoa.SwitchKey(ctx, *keys["cjk"])
     ct = aoa.Ciphertext.from_residues(ctx, c0, c1, slots=N // 2)
     out = aoa.Ciphertext(ctx)
@@ -175,6 +184,13 @@ def test_rotate_conjugate_bit_exact(ref_table, pset):
     w0, w1 = o.conjugate((c0, c1), keys["cjk"], k - 1, state=ST_COEF)
     g0, g1 = out.download(nlimbs=k)
     assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+    ct = aoa.Ciphertext.from_residues(ctx, c0, c1, slots=N // 2)
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_conjugate_plain(ctx, out, ct, cjk)
+    g0, g1 = out.download(nlimbs=k)
+    assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+    with pytest.raises(aoa.capi.AoaError):
+        aoa.ckks_rotate_plain(ctx, out, ct, 1, None)              # no key
 
 
 def test_add_sub_mixed_domains(ref_table):

@@ -3,7 +3,8 @@
 The golden outputs of pdroalves/aoa's own aoa-ntt CKKS layer that pin the
 oracle (tests/test_oracle_reference_ckks.py) are compared here with this
 library's kernels, through the C ABI, on the reference's primes: HMult with and
-without rescale (per call and batched), rotations, conjugation, addition,
+without rescale (per call, batched, and the reference's own per-call
+sequence), rotations and conjugation (the same three ways), addition,
 subtraction and the encoder on seeded operands, then HMult and decryption of
 ciphertexts the reference encrypted under its own keys, word for word."""
 import numpy as np
@@ -80,10 +81,17 @@ def test_rotations_and_conjugation_equal_reference(env, level):
         aoa.ckks_rotate_batch(ctx, outs, [_ct(aoa, ctx, c_in, level, SCALE_A, N // 2) for _ in range(2)], r, rtk)
         for o in outs:
             _check(o, g["n1024_rotate%d_l%d" % (r, level)], N, "rotate %d batched" % r)
+        out = aoa.Ciphertext(ctx)                # the reference's own per-call sequence
+        aoa.ckks_rotate_plain(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), r, rtk)
+        assert out.domain == aoa.AOA_COEF
+        _check(out, g["n1024_rotate%d_l%d" % (r, level)], N, "rotate %d per-call sequence" % r)
     cjk = _key(aoa, ctx, seeded_key(115, 116, primes, N))
     out = aoa.Ciphertext(ctx)
     aoa.ckks_conjugate(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), cjk)
     _check(out, g["n1024_conjugate_l%d" % level], N, "conjugate")
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_conjugate_plain(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), cjk)
+    _check(out, g["n1024_conjugate_l%d" % level], N, "conjugate per-call sequence")
 
 
 @pytest.mark.parametrize("level", LEVELS)
