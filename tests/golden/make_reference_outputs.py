@@ -15,10 +15,15 @@ on seeded operands; then its own key generation, encryption, HMult, rotation
 and decryption) for CKKS_CONFIGS; its records go to
 tests/golden/reference_ckks_outputs.npz (tests/test_oracle_reference_ckks.py).
 
+oracle/_ref/ref_dgt_harness runs aoa-dgt's DGT (single-kernel and
+hierarchical), its product, and ModUp / ModDown / rescale on its DGT engine
+for DGT_CONFIGS; its records go to tests/golden/reference_dgt_outputs.npz
+(tests/test_oracle_reference_dgt.py).
+
 Usage (on a machine with a GPU and the built harnesses):
     python tests/golden/make_reference_outputs.py OUT_DIR
-writes OUT_DIR/reference_outputs.npz and OUT_DIR/reference_ckks_outputs.npz
-(copy them into tests/golden/).
+writes OUT_DIR/reference_outputs.npz, OUT_DIR/reference_ckks_outputs.npz and
+OUT_DIR/reference_dgt_outputs.npz (copy them into tests/golden/).
 """
 import os
 import subprocess
@@ -29,6 +34,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 CKKS_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_ckks_harness")
+DGT_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_dgt_harness")
 
 # (log2 N, k, kl, prec, transforms only): the reference's hierarchical
 # transforms at 2^10 (32 x 32) and 2^12 (64 x 64) on its own prime choice
@@ -37,6 +43,13 @@ CKKS_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_ckks_harness")
 CONFIGS = [(10, 4, 5, 55, 0), (12, 3, 4, 52, 1)]
 TAGS = {1: "ntt_fwd", 2: "ntt_inv", 3: "modup", 4: "moddown", 5: "rescale", 6: "modup_max", 7: "ntt_fwd_max"}
 
+# (log2 nphi, k, kl, prec, transforms only) of the DGT records: aoa-dgt's
+# single-kernel DGT at nphi = 2^10 (512 Gaussian integers) with its product,
+# ModUp / ModDown / rescale on the DGT engine, and its hierarchical DGT at
+# 2^13 (64 x 64)
+DGT_CONFIGS = [(10, 3, 4, 45, 0), (13, 2, 2, 48, 1)]
+DGT_TAGS = {1: "dgt_fwd", 2: "dgt_inv", 3: "mul", 4: "modup", 5: "moddown", 6: "rescale"}
+
 # (log2 N, k, kl, prec) of the CKKS-layer records
 CKKS_CONFIGS = [(10, 4, 5, 55)]
 CKKS_TAGS = {20: "hmult_l%d", 21: "hmult_norescale_l%d", 23: "conjugate_l%d", 24: "add_l%d", 25: "sub_l%d",
@@ -44,16 +57,16 @@ CKKS_TAGS = {20: "hmult_l%d", 21: "hmult_norescale_l%d", 23: "conjugate_l%d", 24
              46: "dec_mul", 47: "rot1_keys", 48: "dec_rot1"}
 
 
-def parse(path):
+def parse(path, magic=b"AOAREF01", tags=TAGS):
     w = np.fromfile(path, dtype=np.uint64)
-    assert w[:1].tobytes() == b"AOAREF01", "not a harness output"
+    assert w[:1].tobytes() == magic, "not a harness output"
     N, k, kl, prec = (int(v) for v in w[1:5])
     primes = w[5:5 + k + kl].copy()
     at = 5 + k + kl
     recs = {}
     while at < w.size:
         tag, level, n = (int(v) for v in w[at:at + 3])
-        recs["%s_l%d" % (TAGS[tag], level)] = w[at + 3:at + 3 + n].copy()
+        recs["%s_l%d" % (tags[tag], level)] = w[at + 3:at + 3 + n].copy()
         at += 3 + n
     return N, k, kl, prec, primes, recs
 
@@ -109,6 +122,19 @@ def main():
         for name, v in recs.items():
             arrays["%s_%s" % (tag, name)] = v
     dst = os.path.join(out_dir, "reference_ckks_outputs.npz")
+    np.savez_compressed(dst, **arrays)
+    print("wrote", dst, sorted(arrays))
+    arrays = {}
+    for log_n, k, kl, prec, tonly in DGT_CONFIGS:
+        path = os.path.join(out_dir, "ref_dgt_n%d.bin" % (1 << log_n))
+        subprocess.check_call([DGT_HARNESS, path, str(log_n), str(k), str(kl), str(prec), str(tonly)])
+        N, k2, kl2, prec2, primes, recs = parse(path, b"AOAREF03", DGT_TAGS)
+        tag = "n%d" % N
+        arrays[tag + "_params"] = np.array([N, k2, kl2, prec2], dtype=np.uint64)
+        arrays[tag + "_primes"] = primes
+        for name, v in recs.items():
+            arrays["%s_%s" % (tag, name)] = v
+    dst = os.path.join(out_dir, "reference_dgt_outputs.npz")
     np.savez_compressed(dst, **arrays)
     print("wrote", dst, sorted(arrays))
 
