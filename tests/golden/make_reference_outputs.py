@@ -18,12 +18,15 @@ tests/golden/reference_ckks_outputs.npz (tests/test_oracle_reference_ckks.py).
 oracle/_ref/ref_dgt_harness runs aoa-dgt's DGT (single-kernel and
 hierarchical), its product, and ModUp / ModDown / rescale on its DGT engine
 for DGT_CONFIGS; its records go to tests/golden/reference_dgt_outputs.npz
-(tests/test_oracle_reference_dgt.py).
+(tests/test_oracle_reference_dgt.py).  oracle/_ref/ref_dgt_ckks_harness runs
+aoa-dgt's CKKS layer with ref_ckks_harness's records for DGT_CKKS_CONFIGS
+(tests/golden/reference_dgt_ckks_outputs.npz, tests/test_gpu_reference_dgt.py).
 
 Usage (on a machine with a GPU and the built harnesses):
     python tests/golden/make_reference_outputs.py OUT_DIR
-writes OUT_DIR/reference_outputs.npz, OUT_DIR/reference_ckks_outputs.npz and
-OUT_DIR/reference_dgt_outputs.npz (copy them into tests/golden/).
+writes OUT_DIR/reference_outputs.npz, reference_ckks_outputs.npz,
+reference_dgt_outputs.npz and reference_dgt_ckks_outputs.npz (copy them into
+tests/golden/).
 """
 import os
 import subprocess
@@ -35,6 +38,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 CKKS_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_ckks_harness")
 DGT_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_dgt_harness")
+DGT_CKKS_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_dgt_ckks_harness")
 
 # (log2 N, k, kl, prec, transforms only): the reference's hierarchical
 # transforms at 2^10 (32 x 32) and 2^12 (64 x 64) on its own prime choice
@@ -50,8 +54,9 @@ TAGS = {1: "ntt_fwd", 2: "ntt_inv", 3: "modup", 4: "moddown", 5: "rescale", 6: "
 DGT_CONFIGS = [(10, 3, 4, 45, 0), (13, 2, 2, 48, 1)]
 DGT_TAGS = {1: "dgt_fwd", 2: "dgt_inv", 3: "mul", 4: "modup", 5: "moddown", 6: "rescale"}
 
-# (log2 N, k, kl, prec) of the CKKS-layer records
+# (log2 N, k, kl, prec) of the CKKS-layer records (aoa-ntt, then aoa-dgt)
 CKKS_CONFIGS = [(10, 4, 5, 55)]
+DGT_CKKS_CONFIGS = [(10, 4, 4, 48)]
 CKKS_TAGS = {20: "hmult_l%d", 21: "hmult_norescale_l%d", 23: "conjugate_l%d", 24: "add_l%d", 25: "sub_l%d",
              26: "encode_s%d", 40: "sk", 41: "evk", 42: "enc300", 43: "enc301", 44: "mul_keys", 45: "dec300",
              46: "dec_mul", 47: "rot1_keys", 48: "dec_rot1"}
@@ -71,11 +76,11 @@ def parse(path, magic=b"AOAREF01", tags=TAGS):
     return N, k, kl, prec, primes, recs
 
 
-def parse_ckks(path):
-    """Records of ref_ckks_harness; ciphertext records keep their
-    [aux, scale, slots, c0 limbs, c1 limbs] words."""
+def parse_ckks(path, magic=b"AOAREF02"):
+    """Records of ref_ckks_harness / ref_dgt_ckks_harness; ciphertext records
+    keep their [aux, scale, slots, c0 limbs, c1 limbs] words."""
     w = np.fromfile(path, dtype=np.uint64)
-    assert w[:1].tobytes() == b"AOAREF02", "not a CKKS harness output"
+    assert w[:1].tobytes() == magic, "not a CKKS harness output"
     N, k, kl, prec = (int(v) for v in w[1:5])
     primes = w[5:5 + k + kl].copy()
     at = 5 + k + kl
@@ -135,6 +140,19 @@ def main():
         for name, v in recs.items():
             arrays["%s_%s" % (tag, name)] = v
     dst = os.path.join(out_dir, "reference_dgt_outputs.npz")
+    np.savez_compressed(dst, **arrays)
+    print("wrote", dst, sorted(arrays))
+    arrays = {}
+    for log_n, k, kl, prec in DGT_CKKS_CONFIGS:
+        path = os.path.join(out_dir, "ref_dgt_ckks_n%d.bin" % (1 << log_n))
+        subprocess.check_call([DGT_CKKS_HARNESS, path, str(log_n), str(k), str(kl), str(prec)])
+        N, k2, kl2, prec2, primes, recs = parse_ckks(path, b"AOAREF04")
+        tag = "n%d" % N
+        arrays[tag + "_params"] = np.array([N, k2, kl2, prec2], dtype=np.uint64)
+        arrays[tag + "_primes"] = primes
+        for name, v in recs.items():
+            arrays["%s_%s" % (tag, name)] = v
+    dst = os.path.join(out_dir, "reference_dgt_ckks_outputs.npz")
     np.savez_compressed(dst, **arrays)
     print("wrote", dst, sorted(arrays))
 

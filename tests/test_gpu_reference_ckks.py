@@ -1,8 +1,9 @@
-"""The CUDA engine's CKKS layer against outputs of the reference evaluator.
+"""The CUDA engine's CKKS layer against outputs of the reference evaluators.
 
-The golden outputs of pdroalves/aoa's own aoa-ntt CKKS layer that pin the
-oracle (tests/test_oracle_reference_ckks.py) are compared here with this
-library's kernels, through the C ABI, on the reference's primes: HMult with and
+The golden outputs of pdroalves/aoa's own aoa-ntt and aoa-dgt CKKS layers that
+pin the oracle (tests/test_oracle_reference_ckks.py) are compared here with
+this library's kernels, through the C ABI, on each reference's primes (the
+aoa-dgt records on a context whose transform is the DGT): HMult with and
 without rescale (per call, batched, and the reference's own per-call
 sequence), rotations and conjugation (the same three ways), addition,
 subtraction and the encoder on seeded operands, then HMult and decryption of
@@ -11,19 +12,31 @@ import numpy as np
 import pytest
 
 from tests.gpu_util import require_gpu
-from tests.test_oracle_reference_ckks import (LEVELS, ROTATIONS, SCALE_A, SCALE_B, ct_record, decoded, load,
-                                              seeded_ct, seeded_key, splitmix_values)
+from tests.test_oracle_reference_ckks import (FIXTURES, HERE, LEVELS, ROTATIONS, SCALE_A, SCALE_B, ct_record,
+                                              decoded, load, seeded_ct, seeded_key, splitmix_values)
 
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def env():
+@pytest.fixture(scope="module", params=FIXTURES)
+def env(request):
     require_gpu()
+    import json
+    import os
     import aoa_b200 as aoa
-    g, N, k, kl, prec, primes = load()
-    E = aoa.Engine(N.bit_length() - 1, primes[:k], primes[k:], scale_bits=prec)
-    ctx = aoa.Context(E)
+    from oracle import dgt_roots
+    g, N, k, kl, prec, primes = load(request.param)
+    if "dgt" in request.param:                   # the AOADGT evaluator: a DGT context on aoa-dgt's roots
+        with open(os.path.join(HERE, "golden", "dgt_roots.json")) as f:
+            gens, roots = dgt_roots(json.load(f), primes, N // 2)
+        E = aoa.Engine(N.bit_length() - 1, primes[:k], primes[k:], scale_bits=prec, generators=gens, dgt_roots=roots)
+        ctx = aoa.Context(E)
+        ctx.set_transform(aoa.AOA_DGT)
+        ctx.is_dgt = True
+    else:
+        E = aoa.Engine(N.bit_length() - 1, primes[:k], primes[k:], scale_bits=prec)
+        ctx = aoa.Context(E)
+        ctx.is_dgt = False
     return aoa, g, N, k, kl, prec, primes, ctx
 
 
@@ -54,7 +67,7 @@ def test_hmult_equals_reference(env, level):
         out = aoa.Ciphertext(ctx)
         (aoa.ckks_mul if rescale else aoa.ckks_mul_without_rescale)(ctx, out, a, b, evk)
         _check(out, g["n1024_" + name], N, name)
-        if rescale:       # the reference's own per-call op sequence on this engine
+        if rescale and not ctx.is_dgt:   # the reference's own per-call op sequence (NTT contexts)
             out = aoa.Ciphertext(ctx)
             aoa.ckks_mul_plain(ctx, out, _ct(aoa, ctx, a_in, level, SCALE_A, N // 2),
                                _ct(aoa, ctx, b_in, level, SCALE_B, N // 2), evk)
@@ -77,6 +90,8 @@ def test_rotations_and_conjugation_equal_reference(env, level):
         out = aoa.Ciphertext(ctx)
         aoa.ckks_rotate_left(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), r, rtk)
         _check(out, g["n1024_rotate%d_l%d" % (r, level)], N, "rotate %d" % r)
+        if ctx.is_dgt:          # batched rotations and the reference-sequence path: NTT contexts
+            continue
         outs = [aoa.Ciphertext(ctx) for _ in range(2)]
         aoa.ckks_rotate_batch(ctx, outs, [_ct(aoa, ctx, c_in, level, SCALE_A, N // 2) for _ in range(2)], r, rtk)
         for o in outs:
@@ -89,9 +104,10 @@ def test_rotations_and_conjugation_equal_reference(env, level):
     out = aoa.Ciphertext(ctx)
     aoa.ckks_conjugate(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), cjk)
     _check(out, g["n1024_conjugate_l%d" % level], N, "conjugate")
-    out = aoa.Ciphertext(ctx)
-    aoa.ckks_conjugate_plain(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), cjk)
-    _check(out, g["n1024_conjugate_l%d" % level], N, "conjugate per-call sequence")
+    if not ctx.is_dgt:
+        out = aoa.Ciphertext(ctx)
+        aoa.ckks_conjugate_plain(ctx, out, _ct(aoa, ctx, c_in, level, SCALE_A, N // 2), cjk)
+        _check(out, g["n1024_conjugate_l%d" % level], N, "conjugate per-call sequence")
 
 
 @pytest.mark.parametrize("level", LEVELS)

@@ -1,9 +1,12 @@
-"""The oracle's CKKS layer against outputs of the reference evaluator itself.
+"""The oracle's CKKS layer against outputs of the reference evaluators themselves.
 
 tests/golden/reference_ckks_outputs.npz holds what pdroalves/aoa's aoa-ntt
 CKKS layer computed on a B200 through its API (oracle/ref/ref_ckks_harness.cu,
 built from the reference's sources by oracle/ref/Makefile; fixture written by
-tests/golden/make_reference_outputs.py):
+tests/golden/make_reference_outputs.py), and
+tests/golden/reference_dgt_ckks_outputs.npz the same records from aoa-dgt's
+CKKS layer (oracle/ref/ref_dgt_ckks_harness.cu; src/ckks.cpp, src/keys.cpp,
+src/ckkscontext.cpp, src/tool/encoder.cu of aoa-dgt):
 - on seeded operands: ckks_mul and ckks_mul_without_rescale (src/ckks/ckks.cpp:
   273-347), ckks_rotate_left (ckks.cpp:982-1009), ckks_conjugate
   (ckks.cpp:1011-1040), ckks_add / ckks_sub (ckks.cpp:240-271) at two levels,
@@ -14,26 +17,35 @@ tests/golden/make_reference_outputs.py):
 Seeded operands are regenerated here from the seeds the harness documents;
 every residue the oracle computes must equal the reference's, and its decoded
 values the reference's decryptions."""
+import json
 import os
 
 import numpy as np
 import pytest
 
-from oracle import ST_COEF, Oracle
+from oracle import ST_COEF, Oracle, dgt_roots
 from tests.test_oracle_reference_outputs import splitmix_residues
 
-GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_ckks_outputs.npz")
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURES = ("reference_ckks_outputs.npz", "reference_dgt_ckks_outputs.npz")   # aoa-ntt, aoa-dgt
 SCALE_A, SCALE_B = (1 << 40) + 3, (1 << 40) + 5
 LEVELS = (3, 1)          # input levels of the seeded cases (k = 4)
 ROTATIONS = (1, 4)
 
 
-def load():
-    assert os.path.exists(GOLDEN), "missing fixture " + GOLDEN
-    g = np.load(GOLDEN)
+def load(name=FIXTURES[0]):
+    path = os.path.join(HERE, "golden", name)
+    assert os.path.exists(path), "missing fixture " + path
+    g = np.load(path)
     N, k, kl, prec = (int(v) for v in g["n1024_params"])
     primes = [int(p) for p in g["n1024_primes"]]
     return g, N, k, kl, prec, primes
+
+
+def dgt_generators(primes, N):
+    """aoa-dgt's generators for `primes` (tests/golden/dgt_roots.json)."""
+    with open(os.path.join(HERE, "golden", "dgt_roots.json")) as f:
+        return dgt_roots(json.load(f), primes, N // 2)[0]
 
 
 def splitmix_values(seed, slots):
@@ -78,10 +90,11 @@ def decoded(words):
     return v[0::2] + 1j * v[1::2]
 
 
-@pytest.fixture(scope="module")
-def ref():
-    g, N, k, kl, prec, primes = load()
-    o = Oracle(N, primes[:k], primes[k:])
+@pytest.fixture(scope="module", params=FIXTURES)
+def ref(request):
+    g, N, k, kl, prec, primes = load(request.param)
+    proots = dgt_generators(primes, N) if "dgt" in request.param else None
+    o = Oracle(N, primes[:k], primes[k:], proots=proots)
     return g, N, k, kl, prec, primes, o
 
 
