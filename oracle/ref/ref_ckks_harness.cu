@@ -11,6 +11,7 @@
 // Test infrastructure only: nothing in the product links or runs it.
 //
 // usage: ref_ckks_harness <out file> <log2 N> <k> <kl> <prec>
+//        ref_ckks_harness --time <log2 N> <k> <kl> <prec> <reps>   (see time_hmult)
 //
 // Part 1, seeded operands (the test regenerates them): every limb of every
 // polynomial is filled like ref_harness does (word j of limb i is output
@@ -43,6 +44,7 @@
 #include <newckks/ckks/ckkskeys.h>
 #include <newckks/ckks/cipher_t.h>
 
+#include <chrono>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -243,9 +245,46 @@ static void reference_keys() {
   ctx->sync();
 }
 
+// Timing mode: `reps` ckks_mul (HMult + relinearise + rescale) of two seeded
+// ciphertexts at level k - 1 with a seeded evaluation key, after 3 warm-up
+// calls (the inputs stay in the transform domain after the first call, as
+// they do in a chain of products).  Host clock around the loop, the device
+// synchronised on both sides: the reference's per-call cost as a caller sees
+// it.  Prints one JSON line with the primes and the time per product.
+static int time_hmult(int reps) {
+  CKKSContext* ctx = new CKKSContext();
+  set_key(ctx, ctx->keys.evk, 111, 112);
+  cipher_t a, b, out;
+  set_ct(ctx, &a, 101, 102, g_k - 1, kScaleA, g_N / 2);
+  set_ct(ctx, &b, 103, 104, g_k - 1, kScaleB, g_N / 2);
+  cipher_init(ctx, &out);
+  for (int i = 0; i < 3; i++) ckks_mul(ctx, &out, &a, &b);
+  if (!check_cuda("warm-up")) return 1;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0; i < reps; i++) ckks_mul(ctx, &out, &a, &b);
+  if (!check_cuda("timed calls")) return 1;
+  const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  printf("{\"N\": %d, \"k\": %d, \"kl\": %d, \"level\": %d, \"reps\": %d, \"ms_per_hmult\": %.6f, \"primes\": [",
+         g_N, g_k, g_kl, g_k - 1, reps, ms / reps);
+  for (size_t i = 0; i < g_primes.size(); i++) printf("%s%llu", i ? ", " : "", (unsigned long long)g_primes[i]);
+  printf("]}\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 7 && strcmp(argv[1], "--time") == 0) {
+    g_N = 1 << atoi(argv[2]);
+    g_k = atoi(argv[3]);
+    g_kl = atoi(argv[4]);
+    CUDAManager::init(g_k, g_kl, g_N, atoi(argv[5]));
+    if (!check_cuda("init")) return 1;
+    g_primes = CUDAManager::RNSQPrimes;
+    g_primes.insert(g_primes.end(), CUDAManager::RNSBPrimes.begin(), CUDAManager::RNSBPrimes.end());
+    return time_hmult(atoi(argv[6]));
+  }
   if (argc != 6) {
-    fprintf(stderr, "usage: ref_ckks_harness <out> <log2 N> <k> <kl> <prec>\n");
+    fprintf(stderr, "usage: ref_ckks_harness <out> <log2 N> <k> <kl> <prec>\n"
+                    "       ref_ckks_harness --time <log2 N> <k> <kl> <prec> <reps>\n");
     return 2;
   }
   g_N = 1 << atoi(argv[2]);
