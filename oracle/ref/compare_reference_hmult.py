@@ -1,6 +1,6 @@
 #!/usr/bin/env python3
-"""HMult + relinearise + rescale: the reference's own CUDA evaluator against
-this engine, on one GPU and the same primes.
+"""HMult + relinearise + rescale, and the limb transforms: the reference's own
+CUDA evaluators against this engine, on one GPU and the same primes.
 
 Runs oracle/_ref/ref_ckks_harness in its timing mode (pdroalves/aoa aoa-ntt's
 ckks_mul, built from its sources by oracle/ref/Makefile: seeded ciphertexts at
@@ -11,8 +11,13 @@ this engine's kernels (ckks_mul_plain), and batched HMult of 16 products
 (CUDA events on the context's stream).  The reference supports a 63-bit q0
 and 45/48/52/55-bit buckets only, so the comparison runs on its 55-bit set
 (the 63-bit q0 puts this engine on its strict, non-lazy butterflies).
-Comparison tooling beside the fixture harnesses: it is not the benchmark
-(bench.py) and nothing in the product runs it.
+Transforms: oracle/_ref/ref_harness and ref_dgt_harness in their timing modes
+run aoa-ntt's NTT (COMMONEngine::execute) and aoa-dgt's DGT
+(DGTEngine::execute_dgt) one call per poly over `--polys` polys of k limbs,
+forward then inverse; this engine runs the same shapes with ntt_fwd / ntt_inv
+and dgt_fwd / dgt_inv over the whole batch (its DGT roots derived from the
+primes).  Comparison tooling beside the fixture harnesses: it is not the
+benchmark (bench.py) and nothing in the product runs it.
 
 Usage (GPU machine, harness built):
     python oracle/ref/compare_reference_hmult.py [--log-n 16 --k 30 --kl 31 --prec 55 --reps 20]
@@ -29,6 +34,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_ckks_harness")
+NTT_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+DGT_HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_dgt_harness")
 
 
 def engine_times(log_n, q, b, reps, batch=16):
@@ -90,6 +97,44 @@ def engine_times(log_n, q, b, reps, batch=16):
             "lazy_butterflies": all(p < (1 << 60) for p in q + b)}
 
 
+def run_json(cmd):
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
+    return json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+
+
+def engine_transforms(log_n, primes, polys, dgt):
+    sys.path.insert(0, ROOT)
+    import torch
+    import aoa_b200 as aoa
+    k = len(primes)
+    E = aoa.Engine(log_n, primes, [])
+    ctx = aoa.Context(E)
+    N = E.N
+    rng = np.random.default_rng(2)
+    big = ctx.alloc((polys, k, N))
+    host = np.array([rng.integers(0, q, N, dtype=np.uint64) for q in primes], dtype=np.uint64)
+    for p in range(polys):
+        aoa.capi.check(aoa.capi.load().aoa_memcpy_h2d(ctx.handle, big.offset(p * k * N), aoa.capi.ptr(host),
+                                                      host.nbytes))
+    fwd, inv = (ctx.dgt_fwd, ctx.dgt_inv) if dgt else (ctx.ntt_fwd, ctx.ntt_inv)
+    st = torch.cuda.ExternalStream(ctx.stream)
+    fwd(big, polys, 0, k)
+    inv(big, polys, 0, k)
+    ctx.sync()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(st)
+    fwd(big, polys, 0, k)
+    e[1].record(st)
+    inv(big, polys, 0, k)
+    e[2].record(st)
+    ctx.sync()
+    torch.cuda.synchronize()
+    f, i = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    by = 16.0 * polys * k * N
+    big.free()
+    return {"fwd_ms": f, "inv_ms": i, "fwd_gbs": by / f / 1e6, "inv_gbs": by / i / 1e6}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--log-n", type=int, default=16)
@@ -97,10 +142,20 @@ def main():
     ap.add_argument("--kl", type=int, default=31)
     ap.add_argument("--prec", type=int, default=55)
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--polys", type=int, default=256)
+    ap.add_argument("--what", default="hmult", help="hmult, ntt or dgt")
     a = ap.parse_args()
-    out = subprocess.run([HARNESS, "--time", str(a.log_n), str(a.k), str(a.kl), str(a.prec), str(a.reps)],
-                         check=True, capture_output=True, text=True).stdout
-    ref = json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+    if a.what in ("ntt", "dgt"):
+        harness = NTT_HARNESS if a.what == "ntt" else DGT_HARNESS
+        ref = run_json([harness, "--time", str(a.log_n), str(a.k), "1", str(a.prec), str(a.polys)])
+        primes = [int(p) for p in ref.pop("primes")]
+        ours = engine_transforms(a.log_n, primes, a.polys, a.what == "dgt")
+        print(json.dumps({"workload": "%s forward + inverse, %d polys x %d limbs at N=2^%d (the reference's "
+                                      "%d-bit set, 63-bit q0)" % (a.what.upper(), a.polys, a.k, a.log_n, a.prec),
+                          "reference": ref, "engine": ours,
+                          "speedup_fwd": ref["fwd_ms"] / ours["fwd_ms"], "speedup_inv": ref["inv_ms"] / ours["inv_ms"]}))
+        return
+    ref = run_json([HARNESS, "--time", str(a.log_n), str(a.k), str(a.kl), str(a.prec), str(a.reps)])
     primes = [int(p) for p in ref.pop("primes")]
     ours = engine_times(a.log_n, primes[:a.k], primes[a.k:], a.reps)
     line = {"workload": "HMult+relin+rescale, N=2^%d, %d Q + %d special primes (the reference's %d-bit set, "

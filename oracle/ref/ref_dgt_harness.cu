@@ -12,6 +12,7 @@
 // infrastructure only: nothing in the product links or runs it.
 //
 // usage: ref_dgt_harness <out file> <log2 nphi> <k> <kl> <prec> <transform only 0|1>
+//        ref_dgt_harness --time <log2 nphi> <k> <kl> <prec> <polys>   (see time_transforms)
 // A polynomial of nphi coefficients is held folded as nphi / 2 Gaussian
 // integers per residue (a_j + i a_{j + nphi/2}, poly_copy_to_device).
 // Inputs: coefficient j of residue i of an input polynomial is output
@@ -33,6 +34,7 @@
 #include <AOADGT/cuda/cudaengine.h>
 #include <AOADGT/cuda/dgt.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -102,7 +104,44 @@ static bool check_cuda(const char* where) {
   return true;
 }
 
+// Timing mode: forward, then inverse DGTs (DGTEngine::execute_dgt, one call
+// per poly) of `polys` seeded polys of k residues, after one warm-up round;
+// host clock around each device-synchronised round.  Prints one JSON line
+// (16 bytes per coefficient per direction).
+static int time_transforms(int polys) {
+  Context* ctx = new Context();
+  std::vector<poly_t> p(polys);
+  for (int i = 0; i < polys; i++) upload(ctx, &p[i], QBase, residues(1 + i, g_k));
+  if (!check_cuda("upload")) return 1;
+  double ms[2] = {0, 0};
+  for (int round = 0; round < 2; round++) {
+    for (int dir = 0; dir < 2; dir++) {
+      const auto t0 = std::chrono::steady_clock::now();
+      for (int i = 0; i < polys; i++) DGTEngine::execute_dgt(ctx, &p[i], dir == 0 ? FORWARD : INVERSE);
+      if (!check_cuda("transforms")) return 1;
+      ms[dir] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+  const double bytes = 16.0 * polys * g_k * g_nphi;
+  printf("{\"nphi\": %d, \"polys\": %d, \"limbs\": %d, \"fwd_ms\": %.4f, \"inv_ms\": %.4f, "
+         "\"fwd_gbs\": %.2f, \"inv_gbs\": %.2f, \"primes\": [",
+         g_nphi, polys, g_k, ms[0], ms[1], bytes / ms[0] / 1e6, bytes / ms[1] / 1e6);
+  for (int i = 0; i < g_k; i++) printf("%s%llu", i ? ", " : "", (unsigned long long)g_primes[i]);
+  printf("]}\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 7 && strcmp(argv[1], "--time") == 0) {
+    g_nphi = 1 << atoi(argv[2]);
+    g_k = atoi(argv[3]);
+    g_kl = atoi(argv[4]);
+    CUDAEngine::init(g_k, g_kl, g_nphi, atoi(argv[5]));
+    if (!check_cuda("init")) return 1;
+    g_primes = CUDAEngine::RNSPrimes;
+    g_primes.insert(g_primes.end(), CUDAEngine::RNSBPrimes.begin(), CUDAEngine::RNSBPrimes.end());
+    return time_transforms(atoi(argv[6]));
+  }
   if (argc != 7) {
     fprintf(stderr, "usage: ref_dgt_harness <out> <log2 nphi> <k> <kl> <prec> <transform only 0|1>\n");
     return 2;

@@ -12,6 +12,7 @@
 // Test infrastructure only: nothing in the product links or runs it.
 //
 // usage: ref_harness <out file> <log2 N> <k> <kl> <prec> <transform only 0|1>
+//        ref_harness --time <log2 N> <k> <kl> <prec> <polys>   (see time_transforms)
 // Inputs: word j of limb i of an input polynomial is output i N + j of
 // splitmix64 seeded with the case's seed, reduced mod p_i; seeds: forward
 // transform 1, inverse transform 2, ModUp 2 + 1000 level, ModDown
@@ -30,6 +31,7 @@
 #include <newckks/arithmetic/poly_t.h>
 #include <newckks/tool/context.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -78,9 +80,51 @@ static bool check_cuda(const char* where) {
   return true;
 }
 
+// Timing mode: forward, then inverse transforms (COMMONEngine::execute, one
+// call per poly, as the reference's API runs them) of `polys` seeded polys
+// of k limbs, after one warm-up round; host clock around each
+// device-synchronised round.  Prints one JSON line with the primes, the
+// times and the algorithmic rate (16 bytes per coefficient per direction).
+static int time_transforms(int k, int polys) {
+  Context* ctx = new Context();
+  std::vector<poly_t> p(polys);
+  for (int i = 0; i < polys; i++) {
+    std::vector<uint64_t> x = residues(1 + i, 0, k, false);
+    poly_init(ctx, &p[i], QBase);
+    poly_copy_to_device(ctx, &p[i], x.data());
+  }
+  if (!check_cuda("upload")) return 1;
+  double ms[2] = {0, 0};
+  for (int round = 0; round < 2; round++) {
+    for (int dir = 0; dir < 2; dir++) {
+      const auto t0 = std::chrono::steady_clock::now();
+      for (int i = 0; i < polys; i++) COMMONEngine::execute(ctx, &p[i], dir == 0 ? FORWARD : INVERSE);
+      if (!check_cuda("transforms")) return 1;
+      ms[dir] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+  const double bytes = 16.0 * polys * k * g_N;
+  printf("{\"N\": %d, \"polys\": %d, \"limbs\": %d, \"fwd_ms\": %.4f, \"inv_ms\": %.4f, "
+         "\"fwd_gbs\": %.2f, \"inv_gbs\": %.2f, \"primes\": [",
+         g_N, polys, k, ms[0], ms[1], bytes / ms[0] / 1e6, bytes / ms[1] / 1e6);
+  for (int i = 0; i < k; i++) printf("%s%llu", i ? ", " : "", (unsigned long long)g_primes[i]);
+  printf("]}\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 7 && strcmp(argv[1], "--time") == 0) {
+    g_N = 1 << atoi(argv[2]);
+    const int k = atoi(argv[3]);
+    CUDAManager::init(k, atoi(argv[4]), g_N, atoi(argv[5]));
+    if (!check_cuda("init")) return 1;
+    g_primes = CUDAManager::RNSQPrimes;
+    g_primes.insert(g_primes.end(), CUDAManager::RNSBPrimes.begin(), CUDAManager::RNSBPrimes.end());
+    return time_transforms(k, atoi(argv[6]));
+  }
   if (argc != 7) {
-    fprintf(stderr, "usage: ref_harness <out> <log2 N> <k> <kl> <prec> <transform only 0|1>\n");
+    fprintf(stderr, "usage: ref_harness <out> <log2 N> <k> <kl> <prec> <transform only 0|1>\n"
+                    "       ref_harness --time <log2 N> <k> <kl> <prec> <polys>\n");
     return 2;
   }
   g_N = 1 << atoi(argv[2]);
