@@ -103,6 +103,7 @@ struct Engine {
   int k = 0, kl = 0, nprimes = 0;
   int scale_bits = 0;
   bool lazy = false;          // every prime < 2^kLazyPrimeBits: Harvey lazy butterflies
+  std::vector<char> lazy_prime;   // per prime: q < 2^kLazyPrimeBits
   std::vector<uint64_t> primes, gens;
   std::vector<PrimeConst> h_pc;
   PrimeConst* d_pc = nullptr;
@@ -197,6 +198,9 @@ struct NttTables {
   int log_n = 0;
   int prime_shift = 0;     // limb l uses prime first + (l >> prime_shift)
   bool lazy = false;
+  // per prime (q < 2^kLazyPrimeBits), when only some primes allow lazy
+  // butterflies: the limbs run in runs of one kind
+  const char* lazy_prime = nullptr;
 };
 // Fused ends of a limb transform.  NttIo::src: the first pass reads item
 // (p, l) from src + p * src_poly_stride + l * N instead of the data (an
@@ -228,6 +232,7 @@ struct NttEpi {
   const ShoupW* resc = nullptr;
   int use_ptrs = 0;
   OutPtrs outp;
+  int limb_base = 0;       // limb of the launch's first limb in out / ks / base
 };
 struct NttIo {
   const uint64_t* src = nullptr;

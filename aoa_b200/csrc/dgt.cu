@@ -175,6 +175,7 @@ NttTables dgt_tables(const Engine& E) {
   NttTables T;
   T.tw = E.d_dtw; T.itw = E.d_ditw; T.pc = E.d_dpc;
   T.log_n = E.log_n - 1; T.prime_shift = 1; T.lazy = E.lazy;
+  if (!E.lazy) T.lazy_prime = E.lazy_prime.data();
   return T;
 }
 

@@ -283,7 +283,11 @@ int aoa_engine_create(const aoa_params* p, aoa_engine** out) {
       for (int j = 0; j < i; j++)
         if (E.primes[i] == E.primes[j]) throw AoaError(AOA_ERR_BAD_PARAM, "primes must be distinct");
     E.lazy = true;
-    for (uint64_t q : E.primes) E.lazy = E.lazy && q < (1ull << kLazyPrimeBits);
+    E.lazy_prime.clear();
+    for (uint64_t q : E.primes) {
+      E.lazy = E.lazy && q < (1ull << kLazyPrimeBits);
+      E.lazy_prime.push_back(q < (1ull << kLazyPrimeBits) ? 1 : 0);
+    }
     E.gens.resize(E.nprimes);
     for (int i = 0; i < E.nprimes; i++)
       E.gens[i] = p->generators ? p->generators[i] : h_smallest_primitive_root(E.primes[i]);

@@ -290,7 +290,7 @@ __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
 // ---- fused epilogue of a forward transform ----------------------------------------
 __device__ __forceinline__ void epi_store(const NttEpi& e, long N, long p, int limb, int prime, long c, uint64_t v,
                                           const PrimeConst& P) {
-  const long off = (long)limb * N + c;
+  const long off = (long)(limb + e.limb_base) * N + c;
   if (e.mode == kEpiKeyProduct) {
     const uint64_t kb = e.key[(long)prime * N + c], ka = e.key[e.key_half + (long)prime * N + c];
     uint64_t* o = e.out + p * e.out_stride + off;
@@ -1048,6 +1048,35 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   if (npolys <= 0 || nlimbs <= 0) return;
   if (first_prime < 0 || first_prime + ((nlimbs - 1) >> T.prime_shift) >= E.nprimes)
     throw AoaError(AOA_ERR_BAD_PARAM, "ntt: prime range out of bounds");
+  if (T.lazy_prime && T.log_n >= 10) {
+    // Mixed prime sizes (the reference's prime sets put a 63-bit q0 before
+    // its 45..55-bit buckets): the limbs run in maximal runs of one kind, the
+    // lazy kernels for primes below 2^kLazyPrimeBits, the strict ones for the
+    // rest.  Runs start at prime boundaries; each run's data, source and
+    // epilogue limbs are offset by its first limb.
+    const long n = 1L << T.log_n;
+    auto lazy_at = [&](int l) { return T.lazy_prime[first_prime + (l >> T.prime_shift)] != 0; };
+    for (int l0 = 0; l0 < nlimbs;) {
+      const bool lz = lazy_at(l0);
+      int l1 = l0 + 1;
+      while (l1 < nlimbs && lazy_at(l1) == lz) l1++;
+      NttTables T2 = T;
+      T2.lazy = lz;
+      T2.lazy_prime = nullptr;
+      if (l0 == 0 && l1 == nlimbs) {
+        ntt_batch_tables(E, T2, data, npolys, first_prime, nlimbs, poly_stride, forward, st, io);
+        return;
+      }
+      NttIo run;
+      if (io) run = *io;
+      if (run.src) run.src += (long)l0 * n;
+      run.epi.limb_base += l0;
+      ntt_batch_tables(E, T2, data + (long)l0 * n, npolys, first_prime + (l0 >> T.prime_shift), l1 - l0,
+                       poly_stride, forward, st, &run);
+      l0 = l1;
+    }
+    return;
+  }
   const NttEpi no_epi{};
   const NttEpi& epi = io ? io->epi : no_epi;
   if (epi.mode != kEpiStore && !forward) throw AoaError(AOA_ERR_BAD_PARAM, "ntt: epilogues are for forward transforms");
@@ -1115,6 +1144,7 @@ void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
   T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
+  if (!E.lazy) T.lazy_prime = E.lazy_prime.data();
   ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, nullptr);
 }
 
@@ -1124,6 +1154,7 @@ void ntt_batch_io(const Engine& E, uint64_t* data, int npolys, int first_prime, 
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
   T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
+  if (!E.lazy) T.lazy_prime = E.lazy_prime.data();
   ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, &io);
 }
 

@@ -10,7 +10,8 @@ primes the reference chose: per-call ckks_mul, the reference's op sequence on
 this engine's kernels (ckks_mul_plain), and batched HMult of 16 products
 (CUDA events on the context's stream).  The reference supports a 63-bit q0
 and 45/48/52/55-bit buckets only, so the comparison runs on its 55-bit set
-(the 63-bit q0 puts this engine on its strict, non-lazy butterflies).
+(this engine runs the 63-bit q0's limbs with strict butterflies, the rest
+lazy).
 Transforms: oracle/_ref/ref_harness and ref_dgt_harness in their timing modes
 run aoa-ntt's NTT (COMMONEngine::execute) and aoa-dgt's DGT
 (DGTEngine::execute_dgt) one call per poly over `--polys` polys of k limbs,
@@ -94,7 +95,7 @@ def engine_times(log_n, q, b, reps, batch=16):
 
     return {"per_call_ms": timed(per_call, reps), "reference_sequence_ms": timed(plain, reps),
             "batched_ms_per_hmult": timed(batched, max(1, reps // 4)) / batch, "batch": batch,
-            "lazy_butterflies": all(p < (1 << 60) for p in q + b)}
+            "lazy_primes": "%d of %d" % (sum(p < (1 << 60) for p in q + b), len(q + b))}
 
 
 def run_json(cmd):

@@ -335,11 +335,14 @@ def test_hmult_batch_full_size_equals_pipeline():
 
 @pytest.mark.parametrize("log_n", [10, 12])
 @pytest.mark.parametrize("fuse", [1, 2, 4, 7])
-def test_fused_transform_ends_equal_separate_kernels(ref_table, log_n, fuse):
+@pytest.mark.parametrize("pset", ["p60", "ref55"])
+def test_fused_transform_ends_equal_separate_kernels(ref_table, log_n, fuse, pset):
     """Key products, key-switch combine and out-of-place inverses fused into the
-    transforms give the same residues as the separate kernels and the oracle."""
+    transforms give the same residues as the separate kernels and the oracle;
+    on the reference's set (63-bit q0, 55-bit rest) the transforms run as a
+    strict run (q0) and a lazy run, each with its source and epilogue offset."""
     require_gpu()
-    Q, B = _sets(ref_table)["p60"]
+    Q, B = _sets(ref_table)[pset]
     aoa, E, ctx, o = _setup(log_n, Q, B)
     keys = make_keys(o, seed=5, rotations=(3,))
     evk = aoa.SwitchKey(ctx, *keys["evk"])

@@ -217,3 +217,35 @@ def test_misaligned_device_pointer_is_rejected():
     d2 = ctx.upload(x)
     ctx.ntt_fwd(d2, 1, 0, 3)
     assert np.array_equal(d2.numpy()[0], o.ntt_fwd(x[0]))
+
+
+@pytest.mark.parametrize("log_n", [11, 16])
+def test_mixed_prime_sizes_run_lazy_and_strict_limbs(log_n):
+    """Primes above and below 2^60 interleaved: the limbs run in alternating
+    lazy and strict runs (several launches per pass), with a first prime other
+    than 0 and strided polys, and equal the oracle's transforms."""
+    require_gpu()
+    n = 1 << log_n
+    big = oracle.gen_ntt_primes(62, 2 * n, 3)
+    small = oracle.gen_ntt_primes(59, 2 * n, 4)
+    ps = [small[0], big[0], big[1], small[1], small[2], big[2], small[3]]
+    E, ctx, o = _engine_and_oracle(log_n, ps[:5], ps[5:])
+    rng = np.random.default_rng(log_n + 40)
+    x = _rand(rng, ps, n, npolys=3)
+    x[1] = np.array([[p - 1] * n for p in ps], dtype=np.uint64)
+    d = ctx.upload(x)
+    ctx.ntt_fwd(d, 3, 0, 7)
+    X = d.numpy()
+    for p in range(3):
+        assert np.array_equal(X[p], o.ntt_fwd(x[p])), p
+    ctx.ntt_inv(d, 3, 0, 7)
+    assert np.array_equal(d.numpy(), x)
+    import ctypes
+    lib = __import__("aoa_b200").capi.load()
+    d = ctx.upload(x)                                   # limbs 2..5 (primes 2..5) of each poly
+    st = lib.aoa_ntt_fwd(ctx.handle, ctypes.c_void_p(d.ptr.value + 2 * n * 8), 3, 2, 4, 7)
+    assert st == 0
+    X = d.numpy()
+    for p in range(3):
+        assert np.array_equal(X[p, 2:6], o.ntt_fwd(x[p, 2:6], first=2)), p
+        assert np.array_equal(X[p, :2], x[p, :2]) and np.array_equal(X[p, 6:], x[p, 6:])
