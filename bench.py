@@ -714,6 +714,23 @@ def main():
     h1.record(lanes[0][4])
     c0.sync()
     h2d_gbs = h2d / (h0.elapsed_time(h1) * 1e-3) / 1e9
+    # both directions at once, as in a step of the steady state: one step's
+    # uploads on lane 0 and one step's downloads on lane 1, started together;
+    # the host link's combined rate bounds the end-to-end rate
+    c1, los1, pouts1, st1 = lanes[1][0], lanes[1][2], lanes[1][3], lanes[1][4]
+    d0, d1 = torch.cuda.Event(enable_timing=True), [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    d0.record(lanes[0][4])
+    st1.wait_event(d0)
+    for i, (a, b) in enumerate(ins0):
+        aoa.capi.check(lib.aoa_ct_upload(c0.handle, a.handle, pin_in[2 * i].ptr, K, aoa.AOA_COEF))
+        aoa.capi.check(lib.aoa_ct_upload(c0.handle, b.handle, pin_in[2 * i + 1].ptr, K, aoa.AOA_COEF))
+    for o, po in zip(los1, pouts1):
+        aoa.capi.check(lib.aoa_ct_download_async(c1.handle, o.handle, po.ptr, K - 1, o.domain))
+    d1[0].record(lanes[0][4])
+    d1[1].record(st1)
+    c0.sync()
+    c1.sync()
+    duplex_gbs = (h2d + d2h) / (max(d0.elapsed_time(e) for e in d1) * 1e-3) / 1e9
     # the last lane-0 result equals a per-call HMult of the same host inputs
     x = host_in[0]
     a1 = aoa.Ciphertext.from_residues(ctx, x[0], x[1], slots=N // 2, scale=1 << SCALE_BITS)
@@ -803,6 +820,7 @@ def main():
             "issue_roofline": issue_roofline(issue, clk, torch.cuda.get_device_properties(local).multi_processor_count),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "h2d_copy_gbs": h2d_gbs, "h2d_bound_ops_per_s": B * h2d_gbs * 1e9 / h2d,
+                    "duplex_copy_gbs": duplex_gbs, "link_bound_ops_per_s": B * duplex_gbs * 1e9 / (h2d + d2h),
                     "path": "aoa_ct_upload (pinned) + aoa_hmult_batch + aoa_ct_download_async (coefficients) "
                             "per step, steps alternating over two contexts (streams)",
                     "result_equals_per_call": e2e_check},
