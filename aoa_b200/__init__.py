@@ -417,6 +417,19 @@ def ckks_rotate_batch(ctx, outs, cts, steps, rtk):
                                             arr(*[x.handle.value for x in cts]), steps, _h(rtk)))
 
 
+def ckks_rotate_batch_steps(ctx, outs, cts, steps, rtks):
+    """outs[i] = cts[i] rotated left by steps[i] slots with rtks[i], grouped by
+    level only (ops of different steps share the launches)."""
+    n = len(outs)
+    if not (len(cts) == len(steps) == len(rtks) == n):
+        raise ValueError("batch lists differ in length")
+    arr = ctypes.c_void_p * max(n, 1)
+    st = (ctypes.c_int * max(n, 1))(*[int(s) for s in steps])
+    capi.check(capi.load().aoa_rotate_batch_steps(ctx.handle, n, arr(*[x.handle.value for x in outs]),
+                                                  arr(*[x.handle.value for x in cts]), st,
+                                                  arr(*[None if k is None else k.handle.value for k in rtks])))
+
+
 def ckks_conjugate_batch(ctx, outs, cts, cjk):
     n = len(outs)
     if len(cts) != n:

@@ -89,6 +89,7 @@ SIGNATURES = {
     "aoa_sub": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_rotate": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "aoa_rotate_batch": (c_int, [c_void_p, c_int, vpp, vpp, c_int, c_void_p]),
+    "aoa_rotate_batch_steps": (c_int, [c_void_p, c_int, vpp, vpp, ctypes.POINTER(c_int), vpp]),
     "aoa_conjugate_batch": (c_int, [c_void_p, c_int, vpp, vpp, c_void_p]),
     "aoa_conjugate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "aoa_encode": (c_int, [c_void_p, c_void_p, c_int, c_int, c_u64, c_int, c_int, c_void_p]),

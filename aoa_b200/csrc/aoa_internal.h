@@ -167,6 +167,13 @@ struct CtPtrs {
 struct OutPtrs {
   uint64_t* p[2 * kMaxBatch];
 };
+// per-op Galois elements and switching keys of a batched automorphism
+struct GaloisList {
+  long g[kMaxBatch];
+};
+struct KeyPtrs {
+  const uint64_t* k[kMaxBatch];
+};
 
 // count of kernel launches issued by this library (engine.cu)
 void note_launch();
@@ -294,8 +301,11 @@ void keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride,
 void ks_combine_ptr(const Engine& E, const OutPtrs& outp, const uint64_t* base, long base_stride, const uint64_t* k,
                     long k_stride, const uint64_t* y, long y_stride, int nlimbs, int npolys, int rescale_level,
                     cudaStream_t st, int base_polys = -1);
-void automorph_ntt_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* out, int n, long galois,
-                            int nlimbs, cudaStream_t st);
+void automorph_ntt_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* out, int n,
+                            const GaloisList& galois, int nlimbs, cudaStream_t st);
+// key products with a key per op (keys.k[z], [b | a] over all primes)
+void keyswitch_mul_keys_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                           const KeyPtrs& keys, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st);
 void keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
                       uint64_t* k1, int nq, cudaStream_t st, int nb = -1);
 void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long poly_stride, long galois,

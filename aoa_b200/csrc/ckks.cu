@@ -498,7 +498,7 @@ static void run_grouped(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa
   if (!use_aux) {
     for (const Unit& g : groups)
       group(C.stream, C.batch, C.batch_bytes, g.e - g.s, go.data() + g.s, ga.data() + g.s, gb.data() + g.s,
-            lvl(idx[g.s]));
+            lvl(idx[g.s]), idx.data() + g.s);
     return;
   }
   if (!C.aux) {
@@ -511,7 +511,7 @@ static void run_grouped(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa
   for (const Unit& u : units) {
     const bool aux = u.stream == 1;
     group(aux ? C.aux : C.stream, aux ? C.batch2 : C.batch, aux ? C.batch2_bytes : C.batch_bytes, u.e - u.s,
-          go.data() + u.s, ga.data() + u.s, gb.data() + u.s, lvl(idx[u.s]));
+          go.data() + u.s, ga.data() + u.s, gb.data() + u.s, lvl(idx[u.s]), idx.data() + u.s);
   }
   AOA_CUDA(cudaEventRecord(C.ev_join, C.aux));
   AOA_CUDA(cudaStreamWaitEvent(C.stream, C.ev_join, 0));
@@ -541,7 +541,7 @@ void hmult_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* a, aoa_ct* co
   // group by level (the operands' common limb count), chunks of kMaxBatch
   run_grouped(C, n, out, a, b, [&](int z) { return std::min(a[z]->level, b[z]->level); },
               [&](cudaStream_t st, void*& ws, size_t& wb, int g, aoa_ct* const* go, aoa_ct* const* ga,
-                  aoa_ct* const* gb, int level) {
+                  aoa_ct* const* gb, int level, const int*) {
                 hmult_batch_group(C, st, ws, wb, g, go, ga, gb, evk, do_rescale, level);
               });
 }
@@ -556,7 +556,7 @@ static size_t galois_words(const Engine& E, int n) {
 }
 
 static void galois_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_bytes, int n, aoa_ct* const* out,
-                               aoa_ct* const* in, long galois, const aoa_swk* key, int level) {
+                               aoa_ct* const* in, const long* galois, const aoa_swk* const* keys, int level) {
   const Engine& E = *C.E;
   const long N = E.N;
   const int m = level + 1, k = E.k, kl = E.kl;
@@ -587,14 +587,26 @@ static void galois_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_by
     slots[z] = in[z]->slots;
     scale[z] = in[z]->scale;
   }
-  automorph_ntt_batch_op(E, ptr, half, R, n, galois, m, st);
+  GaloisList gl;
+  bool one_key = true;
+  for (int z = 0; z < n; z++) {
+    gl.g[z] = galois[z];
+    one_key = one_key && keys[z] == keys[0];
+  }
+  automorph_ntt_batch_op(E, ptr, half, R, n, gl, m, st);
   NttIo io;                                      // inverse of the permuted c1, out of place
   io.src = X;
   io.src_poly_stride = k;
   ntt_batch_io(E, T, n, 0, m, k, false, io, st);
   modup(E, T, half, UB, (long)kl * N, n, level, st);
   ntt_batch(E, UB, n, k, kl, kl, true, st);
-  keyswitch_mul_batch_op(E, X, half, UB, (long)kl * N, key->d, KS, ks, n, m, st);
+  if (one_key) {                                 // each key word read once for the group
+    keyswitch_mul_batch_op(E, X, half, UB, (long)kl * N, keys[0]->d, KS, ks, n, m, st);
+  } else {
+    KeyPtrs kp;
+    for (int z = 0; z < n; z++) kp.k[z] = keys[z]->d;
+    keyswitch_mul_keys_op(E, X, half, UB, (long)kl * N, kp, KS, ks, n, m, st);
+  }
   ntt_batch(E, KS + (long)m * N, 2 * n, k, kl, k + kl, false, st);
   moddown_conv(E, KS + (long)m * N, ks, Y, half, 2 * n, m, st);
   ntt_batch(E, Y, 2 * n, 0, m, k, true, st);
@@ -612,22 +624,43 @@ static void galois_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_by
   }
 }
 
-void galois_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* in, long galois, const aoa_swk* key) {
+// n automorphisms, op z by galois[z] with keys[z]: grouped by level only, so
+// ops of different steps and keys share every launch of a group.
+void galois_batch(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* in, const long* galois,
+                  const aoa_swk* const* keys) {
   const Engine& E = *C.E;
   if (C.transform != AOA_NTT) throw AoaError(AOA_ERR_BAD_PARAM, "batched rotations run on the NTT transform only");
   if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
   if (n == 0) return;
-  if (!out || !in) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
-  if (!key || !key->d) throw AoaError(AOA_ERR_NO_KEY, "missing switching key for this automorphism");
-  if (key->domain != AOA_NTT) throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
+  if (!out || !in || !galois || !keys) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
   if (E.kl == 0) throw AoaError(AOA_ERR_BAD_PARAM, "key switching needs special primes (kl > 0)");
   for (int z = 0; z < n; z++) {
     if (!out[z] || !in[z]) throw AoaError(AOA_ERR_BAD_PARAM, "null ciphertext in batch");
-    to_domain(C, in[z], AOA_NTT, in[z]->level + 1);
+    if (!keys[z] || !keys[z]->d) throw AoaError(AOA_ERR_NO_KEY, "missing switching key for this automorphism");
+    if (keys[z]->domain != AOA_NTT)
+      throw AoaError(AOA_ERR_BAD_PARAM, "the switching key is in another transform domain");
+    if (!(galois[z] & 1)) throw AoaError(AOA_ERR_BAD_PARAM, "the Galois element must be odd");
   }
+  for (int z = 0; z < n; z++) to_domain(C, in[z], AOA_NTT, in[z]->level + 1);
   run_grouped(C, n, out, in, nullptr, [&](int z) { return in[z]->level; },
               [&](cudaStream_t st, void*& ws, size_t& wb, int g, aoa_ct* const* go, aoa_ct* const* ga,
-                  aoa_ct* const*, int level) { galois_batch_group(C, st, ws, wb, g, go, ga, galois, key, level); });
+                  aoa_ct* const*, int level, const int* ids) {
+                std::vector<long> gg(g);
+                std::vector<const aoa_swk*> kk(g);
+                for (int t = 0; t < g; t++) {
+                  gg[t] = galois[ids[t]];
+                  kk[t] = keys[ids[t]];
+                }
+                galois_batch_group(C, st, ws, wb, g, go, ga, gg.data(), kk.data(), level);
+              });
+}
+
+static void galois_batch_uniform(Ctx& C, int n, aoa_ct* const* out, aoa_ct* const* in, long galois,
+                                 const aoa_swk* key) {
+  if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
+  std::vector<long> g(n, galois);
+  std::vector<const aoa_swk*> k(n, key);
+  galois_batch(C, n, out, in, g.data(), k.data());
 }
 
 // The reference's per-call HMult + relinearise + rescale, step for step
@@ -1005,13 +1038,30 @@ int aoa_rotate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, i
     const Engine& E = *c->c.E;
     long r = steps % (E.N / 2);
     if (r < 0) r += E.N / 2;
-    galois_batch(c->c, n, out, in, (long)h_powmod(5, (uint64_t)r, (uint64_t)(2 * E.N)), rtk);
+    galois_batch_uniform(c->c, n, out, in, (long)h_powmod(5, (uint64_t)r, (uint64_t)(2 * E.N)), rtk);
+  });
+}
+
+int aoa_rotate_batch_steps(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, const int* steps,
+                           const aoa_swk* const* rtks) {
+  if (!c) return fail(AOA_ERR_BAD_PARAM, "null argument");
+  return guarded([&] {
+    const Engine& E = *c->c.E;
+    if (n < 0) throw AoaError(AOA_ERR_BAD_PARAM, "negative batch size");
+    if (n > 0 && !steps) throw AoaError(AOA_ERR_BAD_PARAM, "null batch arrays");
+    std::vector<long> g(n);
+    for (int z = 0; z < n; z++) {
+      long r = steps[z] % (E.N / 2);
+      if (r < 0) r += E.N / 2;
+      g[z] = (long)h_powmod(5, (uint64_t)r, (uint64_t)(2 * E.N));
+    }
+    galois_batch(c->c, n, out, in, g.data(), rtks);
   });
 }
 
 int aoa_conjugate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, const aoa_swk* cjk) {
   if (!c) return fail(AOA_ERR_BAD_PARAM, "null argument");
-  return guarded([&] { galois_batch(c->c, n, out, in, 2 * c->c.E->N - 1, cjk); });
+  return guarded([&] { galois_batch_uniform(c->c, n, out, in, 2 * c->c.E->N - 1, cjk); });
 }
 
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk) {

@@ -181,12 +181,12 @@ __global__ void automorph_ntt(uint64_t* out, const uint64_t* in, long poly_strid
 // NTT-domain automorphism of both polys of ciphertext z = blockIdx.z / 2
 // (poly blockIdx.z % 2, stride half) into out: poly 0 of every op first
 // (op stride half), then poly 1 (block offset n*half).
-__global__ void automorph_ntt_batch(CtPtrs ptr, long half, uint64_t* out, int n, long galois, int log_n) {
+__global__ void automorph_ntt_batch(CtPtrs ptr, long half, uint64_t* out, int n, GaloisList gl, int log_n) {
   const long N = 1L << log_n;
   const long p = coef_index();
   const int z = blockIdx.z >> 1, poly = blockIdx.z & 1;
   const uint32_t br = __brev((uint32_t)p) >> (32 - log_n);
-  const long e = ((2L * br + 1) * galois) & (2 * N - 1);
+  const long e = ((2L * br + 1) * gl.g[z]) & (2 * N - 1);
   const long src = __brev((uint32_t)((e - 1) >> 1)) >> (32 - log_n);
   const long limb = (long)blockIdx.y * N;
   out[(long)poly * n * half + (long)z * half + limb + p] = ptr.a[z][(long)poly * half + limb + src];
@@ -230,6 +230,37 @@ __global__ void keyswitch_mul_batch(const uint64_t* xq, long xq_stride, const ui
     uint64_t v[kEwPer];
 #pragma unroll
     for (int u = 0; u < kEwPer; u++) v[u] = x[z * xs + coef_u(u)];
+#pragma unroll
+    for (int u = 0; u < kEwPer; u++) {
+      const long c = coef_u(u);
+      o[z * k_stride + c] = mul_mod(v[u], kb[u], P);
+      o[(n + z) * k_stride + c] = mul_mod(v[u], ka[u], P);
+    }
+  }
+}
+
+// key products with a key per op: op z's x limbs times keys.k[z] (the same
+// layout as keyswitch_mul_batch; each op's key words are read for that op)
+__global__ void keyswitch_mul_keys(const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                                   KeyPtrs keys, long key_half, uint64_t* k, long k_stride, int n, int nq, int K,
+                                   const PrimeConst* pc, int log_n) {
+  const long N = 1L << log_n;
+  const int l = blockIdx.y;
+  const int prime = l < nq ? l : K + (l - nq);
+  const uint64_t* x = l < nq ? xq + (long)l * N : xb + (long)(l - nq) * N;
+  const long xs = l < nq ? xq_stride : xb_stride;
+  const PrimeConst P = pc[prime];
+  uint64_t* o = k + (long)l * N;
+  for (int z = 0; z < n; z++) {
+    const uint64_t* kbp = keys.k[z] + (long)prime * N;
+    uint64_t v[kEwPer], kb[kEwPer], ka[kEwPer];
+#pragma unroll
+    for (int u = 0; u < kEwPer; u++) {
+      const long c = coef_u(u);
+      v[u] = x[z * xs + c];
+      kb[u] = kbp[c];
+      ka[u] = kbp[key_half + c];
+    }
 #pragma unroll
     for (int u = 0; u < kEwPer; u++) {
       const long c = coef_u(u);
@@ -304,9 +335,18 @@ void automorph_coef_op(const Engine& E, uint64_t* out, const uint64_t* in, long 
   AOA_CHECK_LAUNCH();
 }
 
-void automorph_ntt_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* out, int n, long galois,
-                            int nlimbs, cudaStream_t st) {
+void automorph_ntt_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* out, int n,
+                            const GaloisList& galois, int nlimbs, cudaStream_t st) {
   automorph_ntt_batch<<<ew_grid(E, nlimbs, 2 * n), 256, 0, st>>>(ptr, half, out, n, galois, E.log_n);
+  note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+void keyswitch_mul_keys_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                           const KeyPtrs& keys, uint64_t* k, long k_stride, int n, int nq, cudaStream_t st) {
+  const long half = (long)E.nprimes * E.N;
+  keyswitch_mul_keys<<<ew4_grid(E, nq + E.kl, 1), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, keys, half, k, k_stride,
+                                                                 n, nq, E.k, E.d_pc, E.log_n);
   note_launch();
   AOA_CHECK_LAUNCH();
 }

@@ -4,8 +4,8 @@ Batched uneven workload: many ciphertexts of different ring degree and live
 limb count with a mix of HMult + relinearise + rescale, rotations and
 additions.  The grouped schedule runs one context (stream) per ring degree,
 batches every HMult of a degree into grouped launches (aoa_hmult_batch groups
-by limb count) and every rotation by one step into one batched call
-(aoa_rotate_batch, grouped by limb count, one key per step), and is captured
+by limb count) and every rotation of the degree into one batched call
+(aoa_rotate_batch_steps, grouped by limb count, a step and key per op), and is captured
 once per context into a CUDA graph that is replayed; the plain schedule
 issues the reference's per-call operation sequence one op at a time.
 
@@ -25,8 +25,8 @@ import time
 import numpy as np
 
 from . import (AOA_COEF, AOA_NTT, Ciphertext, Context, Engine, Graph, SwitchKey, ckks_add, ckks_encode,
-               ckks_mul_batch, ckks_mul_plain, ckks_mul_pt, ckks_rescale, ckks_rotate_batch, ckks_rotate_plain,
-               ckks_sumslots, params)
+               ckks_mul_batch, ckks_mul_plain, ckks_mul_pt, ckks_rescale, ckks_rotate_batch, ckks_rotate_batch_steps,
+               ckks_rotate_plain, ckks_sumslots, params)
 
 
 def _rand_residues(rng, primes, n):
@@ -98,21 +98,19 @@ class UnevenBatch:
     def run_grouped(self, ln):
         """Every op of degree 2^ln on its context: the HMults in grouped batched
         launches (grouped by limb count inside the call), the rotations in one
-        batched call per step (grouped by limb count inside the call, each step
-        with its own key), then the additions."""
+        batched call (grouped by limb count inside the call, each op with its
+        own step and key), then the additions."""
         ctx = self.ctx[ln]
         muls = [z for z, op in enumerate(self.ops) if op["log_n"] == ln and op["kind"] == "mul"]
         if muls:
             pairs = [self._args(z) for z in muls]
             ckks_mul_batch(ctx, [self.outs[z] for z in muls], [p[0] for p in pairs], [p[1] for p in pairs],
                            self.evk[ln])
-        by_step = {}
-        for z, op in enumerate(self.ops):
-            if op["log_n"] == ln and op["kind"] == "rot":
-                by_step.setdefault(op["step"], []).append(z)
-        for step, zs in sorted(by_step.items()):
-            ckks_rotate_batch(ctx, [self.outs[z] for z in zs], [self._args(z)[0] for z in zs], step,
-                              self.rtk[ln][step])
+        rots = [z for z, op in enumerate(self.ops) if op["log_n"] == ln and op["kind"] == "rot"]
+        if rots:                    # one call: grouped by limb count, a step and key per op
+            ckks_rotate_batch_steps(ctx, [self.outs[z] for z in rots], [self._args(z)[0] for z in rots],
+                                    [self.ops[z]["step"] for z in rots],
+                                    [self.rtk[ln][self.ops[z]["step"]] for z in rots])
         for z, op in enumerate(self.ops):
             if op["log_n"] == ln and op["kind"] == "add":
                 args = self._args(z)

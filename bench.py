@@ -340,8 +340,9 @@ def systems_workloads(aoa, torch):
               "rotation_keys": "a distinct key per step 2^j and degree",
               "plain": "one op at a time in input order: HMult and rotations through the reference's per-call "
                        "sequences on this engine (aoa_hmult_plain, aoa_rotate_plain), additions as ckks_add",
-              "schedule": "one stream per N; HMults grouped by limb count (<=64 per launch), rotations batched "
-                          "per step (grouped by limb count), additions; one CUDA graph per stream"}
+              "schedule": "one stream per N; HMults grouped by limb count (<=64 per launch), rotations in one "
+                          "batched call per N (grouped by limb count, a step and key per op), additions; "
+                          "one CUDA graph per stream"}
     del wb
     n_req = 500
 

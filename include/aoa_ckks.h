@@ -305,6 +305,12 @@ int aoa_rotate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, int steps, const aoa_swk* rt
 /* n rotations by the same step with the same key (each op as aoa_rotate),
  * every stage one launch over the batch grouped by level; NTT contexts.    */
 int aoa_rotate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, int steps, const aoa_swk* rtk);
+/* n rotations with a step and key per op (out[i] = in[i] rotated by
+ * steps[i] with rtks[i], each as aoa_rotate): grouped by level only, so ops of
+ * different steps share every launch of a group; NTT contexts.  No reference
+ * counterpart as one call (the reference rotates one ciphertext per call). */
+int aoa_rotate_batch_steps(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, const int* steps,
+                           const aoa_swk* const* rtks);
 /* ckks_conjugate (ckks.cpp:1011-1040) */
 int aoa_conjugate(aoa_ctx* c, aoa_ct* out, aoa_ct* in, const aoa_swk* cjk);
 int aoa_conjugate_batch(aoa_ctx* c, int n, aoa_ct* const* out, aoa_ct* const* in, const aoa_swk* cjk);

@@ -464,6 +464,57 @@ def test_rotate_batch_equals_single_rotations(ref_table, count):
     assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
 
 
+@pytest.mark.parametrize("count", [7, 20])
+def test_rotate_batch_steps_equals_single_rotations(ref_table, count):
+    """Rotations with a step and key per op in one batched call (grouped by
+    level only: ops of different steps and keys share the launches; a right
+    rotation; an output aliasing its input; 20 ops take the two-stream split)
+    give the per-call residues, and the oracle's for two ops."""
+    require_gpu()
+    Q, B = _sets(ref_table)["p60"]
+    aoa, E, ctx, o = _setup(12, Q, B)
+    N, k = E.N, E.k
+    rots = (1, 2, 4, 64, N // 2 - 3)
+    keys = make_keys(o, seed=24, rotations=rots)
+    rtk = {r: aoa.SwitchKey(ctx, *keys["rtk"][r]) for r in rots}
+    rng = np.random.default_rng(25)
+    data = [_rand_ct(rng, Q, N, k) for _ in range(count)]
+    levels = [k - 1 - (z % 3) for z in range(count)]
+    steps = [rots[z % len(rots)] for z in range(count)]
+    steps[1] = -3                                          # right by 3 = left by N/2 - 3
+
+    def make():
+        cts = []
+        for x, lv in zip(data, levels):
+            c = aoa.Ciphertext.from_residues(ctx, *x, slots=N // 2, scale=1 << 40,
+                                             domain=aoa.AOA_NTT if lv % 2 else aoa.AOA_COEF)
+            c.set(lv, N // 2, 1 << 40, c.domain)
+            cts.append(c)
+        return cts
+
+    key_of = lambda s: rtk[s if s > 0 else N // 2 + s]
+    cts = make()
+    outs = [aoa.Ciphertext(ctx) for _ in cts]
+    outs[2] = cts[2]                                       # in place
+    aoa.ckks_rotate_batch_steps(ctx, outs, cts, steps, [key_of(s) for s in steps])
+    got = [x.download(nlimbs=x.level + 1, domain=aoa.AOA_COEF) for x in outs]
+    ref = make()
+    for z, (c, lv) in enumerate(zip(ref, levels)):
+        w = aoa.Ciphertext(ctx)
+        aoa.ckks_rotate_left(ctx, w, c, steps[z], key_of(steps[z]))
+        assert outs[z].level == lv == w.level
+        want = w.download(nlimbs=lv + 1, domain=aoa.AOA_COEF)
+        assert np.array_equal(got[z][0], want[0]) and np.array_equal(got[z][1], want[1]), z
+    for z in (0, 1):                                       # level k - 1 ops in coefficients
+        if levels[z] != k - 1 or z % 2:
+            continue
+        r = steps[z] if steps[z] > 0 else N // 2 + steps[z]
+        w0, w1 = o.rotate_left(data[z], r, keys["rtk"][r], k - 1, state=ST_COEF)
+        assert np.array_equal(got[z][0], w0) and np.array_equal(got[z][1], w1), z
+    with pytest.raises(aoa.capi.AoaError):                  # a missing key is refused
+        aoa.ckks_rotate_batch_steps(ctx, outs[:2], make()[:2], steps[:2], [rtk[1], None])
+
+
 def test_tensor_core_and_cuda_core_conversions_agree(ref_table):
     """The int8 tensor-core basis conversion and the CUDA-core kernel give the
     same residues (ModUp, ModDown and the merged ModDown + rescale of HMult)."""
