@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "../../include/aoa_ckks.h"
@@ -119,20 +120,20 @@ struct Engine {
   double2* d_ksi = nullptr;
   uint32_t* d_rot = nullptr;
   // DGT (folded Gaussian-integer transform of length N/2): cyclic merged
-  // tables per prime, constants with N/2 inverses, and the twist by powers of
-  // a root r of i (r^(N/2) = i) split as r^n = r^(n mod L) * r^(L floor(n/L)):
-  // GI entries {re, re', im, im'} (Shoup companions), [nprimes][L] and
-  // [nprimes][N/2/L], forward (r) and inverse (r^-1).
+  // tables per prime, constants with N/2 inverses, and the twist by the
+  // powers of a root r of i (r^(N/2) = i).  The twist tables hold r^n = c + di
+  // (forward) and r^-n (inverse) for every n < N/2 in the form of a
+  // three-product GI multiply, six planes [nprimes][6][N/2]: c, d - c, c + d
+  // with their Shoup companions; they are built on the first DGT use
+  // (dgt_twist_tables), so engines that never run a DGT do not hold them.
   std::vector<uint64_t> dgt_roots;   // 2 per prime (re, im of r)
   ShoupW* d_dtw = nullptr;
   ShoupW* d_ditw = nullptr;
   PrimeConst* d_dpc = nullptr;
-  uint64_t* d_twist_lo = nullptr;
-  uint64_t* d_twist_hi = nullptr;
-  uint64_t* d_untwist_lo = nullptr;
-  uint64_t* d_untwist_hi = nullptr;
-  int dgt_log_lo = 0;
-  std::vector<void*> allocations;
+  mutable std::mutex dgt_twist_mu;
+  mutable uint64_t* d_twist = nullptr;
+  mutable uint64_t* d_untwist = nullptr;
+  mutable std::vector<void*> allocations;
 };
 
 struct Ctx {

@@ -21,8 +21,6 @@ using namespace aoa;
 
 namespace {
 
-constexpr int kTwistLo = 256;            // r^n = r^(n mod 256) * r^(256 floor(n / 256))
-
 long bitrev_l(long x, int bits) {
   long r = 0;
   for (int i = 0; i < bits; i++) r |= ((x >> i) & 1L) << (bits - 1 - i);
@@ -30,7 +28,7 @@ long bitrev_l(long x, int bits) {
 }
 
 template <class T>
-T* upload(Engine& E, const std::vector<T>& h) {
+T* upload(const Engine& E, const std::vector<T>& h) {
   T* d = nullptr;
   AOA_CUDA(cudaMalloc(&d, std::max<size_t>(1, h.size()) * sizeof(T)));
   E.allocations.push_back(d);
@@ -59,30 +57,26 @@ GIh derived_root(uint64_t q, uint64_t g, long N) {
   return {x, y};
 }
 
-// (a + ib) * (c + id) for a twist-table entry {c, c', d, d'}.
-__device__ __forceinline__ void gi_mulc(uint64_t& a, uint64_t& b, const uint64_t* w, uint64_t q) {
-  const uint64_t ac = shoup(a, w[0], w[1], q), bd = shoup(b, w[2], w[3], q);
-  const uint64_t ad = shoup(a, w[2], w[3], q), bc = shoup(b, w[0], w[1], q);
-  a = sub_mod(ac, bd, q);
-  b = add_mod(ad, bc, q);
-}
-
 // Twist (forward) or untwist (inverse) of GI limbs in place: limb l of poly p
-// at data + p*poly_stride + l*N, planes [re | im] of H = N/2 words.
-__global__ void gi_twist(uint64_t* data, long poly_stride, int npolys, int first_prime, const uint64_t* __restrict__ lo,
-                         const uint64_t* __restrict__ hi, int log_lo, int H, const PrimeConst* __restrict__ pc) {
+// at data + p*poly_stride + l*N, planes [re | im] of H = N/2 words; entry n
+// of the prime's table is r^(+-n) = c + di, applied as the three-product
+// (a + ib)(c + id) = (k1 - k3) + i (k1 + k2), k1 = c (a + b), k2 = a (d - c),
+// k3 = b (c + d) (a + b < 2q, which a Shoup product takes).
+__global__ void gi_twist(uint64_t* data, long poly_stride, int npolys, int first_prime, const uint64_t* __restrict__ tab,
+                         int H, const PrimeConst* __restrict__ pc) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= H) return;
   const int item = blockIdx.y, limb = item / npolys, p = item % npolys;
   const int prime = first_prime + limb;
-  const int L = 1 << log_lo, NH = H >> log_lo;
   uint64_t* x = data + (long)p * poly_stride + (long)limb * 2 * H;
   const uint64_t q = pc[prime].q;
-  uint64_t a = x[n], b = x[H + n];
-  gi_mulc(a, b, lo + ((long)prime * L + (n & (L - 1))) * 4, q);
-  if (NH > 1) gi_mulc(a, b, hi + ((long)prime * NH + (n >> log_lo)) * 4, q);
-  x[n] = a;
-  x[H + n] = b;
+  const uint64_t* w = tab + (long)prime * 6 * H + n;
+  const uint64_t a = x[n], b = x[H + n];
+  const uint64_t k1 = shoup(a + b, w[0], w[H], q);
+  const uint64_t k2 = shoup(a, w[2 * H], w[3 * H], q);
+  const uint64_t k3 = shoup(b, w[4 * H], w[5 * H], q);
+  x[n] = sub_mod(k1, k3, q);
+  x[H + n] = add_mod(k1, k2, q);
 }
 
 // Karatsuba GI product of canonical operands (GIMul, aoa-dgt src/cuda/dgt.cu:530-553).
@@ -192,14 +186,8 @@ void dgt_init(Engine& E, const uint64_t* roots) {
   const long H = E.N / 2;
   const int lh = E.log_n - 1;
   const int np = E.nprimes;
-  const int L = (int)std::min<long>(kTwistLo, H);
-  const long NH = H / L;
-  E.dgt_log_lo = 0;
-  while ((1 << E.dgt_log_lo) < L) E.dgt_log_lo++;
   std::vector<ShoupW> tw((size_t)np * H), itw((size_t)np * H);
   std::vector<PrimeConst> pc(E.h_pc);
-  std::vector<uint64_t> tlo((size_t)np * L * 4), thi((size_t)np * NH * 4), ulo((size_t)np * L * 4),
-      uhi((size_t)np * NH * 4);
   E.dgt_roots.assign((size_t)2 * np, 0);
   bool bad = false;
 #pragma omp parallel for schedule(dynamic)
@@ -233,39 +221,52 @@ void dgt_init(Engine& E, const uint64_t* roots) {
       base = gi_mul_h(base, base, q);
     }
     if (chk.re != 0 || chk.im != 1) { bad = true; continue; }
-    const uint64_t norm = (uint64_t)(((unsigned __int128)r.re * r.re + (unsigned __int128)r.im * r.im) % q);
-    const uint64_t ni = h_invmod(norm, q);
-    const GIh ri = {h_mulmod(r.re, ni, q), h_mulmod(r.im ? q - r.im : 0, ni, q)};
     E.dgt_roots[2 * p] = r.re;
     E.dgt_roots[2 * p + 1] = r.im;
-    auto put = [q](std::vector<uint64_t>& t, size_t i, GIh v) {
-      t[4 * i] = v.re; t[4 * i + 1] = h_shoup_companion(v.re, q);
-      t[4 * i + 2] = v.im; t[4 * i + 3] = h_shoup_companion(v.im, q);
-    };
-    GIh a = {1, 0}, b = {1, 0};
-    for (int n = 0; n < L; n++) {
-      put(tlo, (size_t)p * L + n, a);
-      put(ulo, (size_t)p * L + n, b);
-      a = gi_mul_h(a, r, q);
-      b = gi_mul_h(b, ri, q);
-    }
-    const GIh aL = a, bL = b;                            // r^L, r^-L
-    a = {1, 0}; b = {1, 0};
-    for (long n = 0; n < NH; n++) {
-      put(thi, (size_t)p * NH + n, a);
-      put(uhi, (size_t)p * NH + n, b);
-      a = gi_mul_h(a, aL, q);
-      b = gi_mul_h(b, bL, q);
-    }
   }
   if (bad) throw AoaError(AOA_ERR_BAD_PARAM, "dgt_roots: a root r does not satisfy r^(N/2) = i");
   E.d_dtw = upload(E, tw);
   E.d_ditw = upload(E, itw);
   E.d_dpc = upload(E, pc);
-  E.d_twist_lo = upload(E, tlo);
-  E.d_twist_hi = upload(E, thi);
-  E.d_untwist_lo = upload(E, ulo);
-  E.d_untwist_hi = upload(E, uhi);
+}
+
+// The twist tables, on the first DGT of the engine (12 words per prime and
+// Gaussian integer: 190 MB for 61 primes at N = 2^16).
+static void dgt_twist_tables(const Engine& E) {
+  std::lock_guard<std::mutex> lock(E.dgt_twist_mu);
+  if (E.d_twist) return;
+  const long H = E.N / 2;
+  const int np = E.nprimes;
+  std::vector<uint64_t> tf((size_t)np * 6 * H), uf((size_t)np * 6 * H);
+#pragma omp parallel for schedule(dynamic)
+  for (int p = 0; p < np; p++) {
+    const uint64_t q = E.primes[p];
+    const GIh r = {E.dgt_roots[2 * p], E.dgt_roots[2 * p + 1]};
+    const uint64_t norm = (uint64_t)(((unsigned __int128)r.re * r.re + (unsigned __int128)r.im * r.im) % q);
+    const uint64_t ni = h_invmod(norm, q);
+    const GIh ri = {h_mulmod(r.re, ni, q), h_mulmod(r.im ? q - r.im : 0, ni, q)};
+    auto put = [&](std::vector<uint64_t>& t, long n, GIh v) {
+      uint64_t* base = t.data() + (size_t)p * 6 * H + n;
+      const uint64_t c = v.re, dc = (v.im + q - v.re) % q, cd = (v.re + v.im) % q;
+      base[0] = c;
+      base[H] = h_shoup_companion(c, q);
+      base[2 * H] = dc;
+      base[3 * H] = h_shoup_companion(dc, q);
+      base[4 * H] = cd;
+      base[5 * H] = h_shoup_companion(cd, q);
+    };
+    GIh a = {1, 0}, b = {1, 0};
+    for (long n = 0; n < H; n++) {
+      put(tf, n, a);
+      put(uf, n, b);
+      a = gi_mul_h(a, r, q);
+      b = gi_mul_h(b, ri, q);
+    }
+  }
+  uint64_t* t = upload(E, tf);
+  uint64_t* u = upload(E, uf);
+  E.d_untwist = u;
+  E.d_twist = t;
 }
 
 // DGT / inverse DGT of limbs 0..nlimbs-1 (primes first_prime..) of npolys GI
@@ -277,16 +278,17 @@ void dgt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
     throw AoaError(AOA_ERR_BAD_PARAM, "dgt: prime range out of bounds");
   const int H = (int)(E.N / 2);
   const NttTables T = dgt_tables(E);
+  dgt_twist_tables(E);
   if (forward) {
-    gi_twist<<<gi_grid(E, nlimbs * npolys), 256, 0, st>>>(data, poly_stride * E.N, npolys, first_prime,
-                                                            E.d_twist_lo, E.d_twist_hi, E.dgt_log_lo, H, E.d_pc);
+    gi_twist<<<gi_grid(E, nlimbs * npolys), 256, 0, st>>>(data, poly_stride * E.N, npolys, first_prime, E.d_twist,
+                                                            H, E.d_pc);
     note_launch();
     AOA_CHECK_LAUNCH();
     ntt_batch_tables(E, T, data, npolys, first_prime, 2 * nlimbs, 2 * poly_stride, true, st);
   } else {
     ntt_batch_tables(E, T, data, npolys, first_prime, 2 * nlimbs, 2 * poly_stride, false, st);
     gi_twist<<<gi_grid(E, nlimbs * npolys), 256, 0, st>>>(data, poly_stride * E.N, npolys, first_prime,
-                                                            E.d_untwist_lo, E.d_untwist_hi, E.dgt_log_lo, H, E.d_pc);
+                                                            E.d_untwist, H, E.d_pc);
     note_launch();
     AOA_CHECK_LAUNCH();
   }
@@ -384,8 +386,10 @@ int aoa_engine_dgt_roots(const aoa_engine* e, uint64_t* out) {
 // aoa-ntt library) or AOA_DGT (the aoa-dgt library).
 int aoa_ctx_set_transform(aoa_ctx* c, int domain) {
   if (!c || (domain != AOA_NTT && domain != AOA_DGT)) return fail(AOA_ERR_BAD_PARAM, "bad transform");
-  c->c.transform = domain;
-  return AOA_OK;
+  return guarded([&] {
+    if (domain == AOA_DGT) dgt_twist_tables(*c->c.E);    // allocated now, not inside later evaluations
+    c->c.transform = domain;
+  });
 }
 
 }  // extern "C"

@@ -191,7 +191,9 @@ int aoa_engine_dgt_roots(const aoa_engine* e, uint64_t* roots_out);
 /* Which library's transform the context's evaluations use: AOA_NTT (aoa-ntt,
  * default) or AOA_DGT (aoa-dgt: HMult tensor and key products as GIMul,
  * rotations through the coefficient domain).  Ciphertexts and keys carry
- * their domain; operands are converted on demand like poly_t states.       */
+ * their domain; operands are converted on demand like poly_t states.  The
+ * engine's DGT twist tables (12 words per prime and Gaussian integer) are
+ * allocated by the first AOA_DGT setting or the first DGT of the engine.   */
 int aoa_ctx_set_transform(aoa_ctx* c, int domain);
 
 /* --- RNS basis conversion and rescale on device buffers (coefficient domain).
