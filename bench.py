@@ -103,12 +103,19 @@ class ClockSampler:
 
 def issue_roofline(issue, clk, sms):
     """The transform against the instruction issue peak: sms x 4 warp
-    instructions per SM clock, at the median SM clock of the timed region."""
+    instructions per SM clock, at the median SM clock of the timed region;
+    and against its integer multiply pipe: the pipe cycles its instruction mix
+    needs over the cycles of the pipes of all SM sub-partitions in the
+    measured time."""
     if not issue:
         return None
     mhz = (clk or {}).get("sm_mhz") or 1965.0
     peak = sms * 4 * mhz * 1e6
-    return dict(issue, peak_per_s=peak, sm_mhz=mhz, frac=issue["achieved_per_s"] / peak)
+    out = dict(issue, peak_per_s=peak, sm_mhz=mhz, frac=issue["achieved_per_s"] / peak)
+    if "fma_pipe_cycles" in issue:
+        avail = sms * 4 * mhz * 1e6 * issue["seconds"]
+        out["fma_pipe_frac"] = issue["fma_pipe_cycles"] / avail
+    return out
 
 
 def dist_setup():
@@ -591,8 +598,10 @@ def main():
             # the SMs' instruction issue peak (4 schedulers x 1 warp instruction
             # per clock per SM), at the SM clock sampled during the timed region
             wi = tj["ntt_fwd_warp_instructions_per_limb"] * npolys * K
-            issue = {"warp_instructions": wi, "achieved_per_s": wi / (fwd_ms / 1000.0),
+            issue = {"warp_instructions": wi, "achieved_per_s": wi / (fwd_ms / 1000.0), "seconds": fwd_ms / 1000.0,
                      "source": "warp instructions per limb from an ncu capture of the same forward transform"}
+            if "ntt_fwd_fma_pipe_cycles_per_limb" in tj:
+                issue["fma_pipe_cycles"] = tj["ntt_fwd_fma_pipe_cycles_per_limb"] * npolys * K
     del buf
 
     # ---- DGT variant: transform rate and per-call HMult on a DGT context -----------
