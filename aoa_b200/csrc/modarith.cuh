@@ -71,7 +71,7 @@ __device__ __forceinline__ uint64_t shoup_lazy_mad3(uint64_t y, uint64_t w, uint
   uint64_t r;
 #ifdef __CUDA_ARCH__
   asm("{\n\t"
-      ".reg .u32 y0, y1, w0, w1, p0, p1, n0, n1, a1, b1, s0, s1, t0, t1, r0, r1;\n\t"
+      ".reg .u32 y0, y1, w0, w1, p0, p1, n0, n1, a1, b1, t0, t1, r0, r1;\n\t"
       ".reg .u64 S, T, R;\n\t"
       "mov.b64 {y0, y1}, %1;\n\t"
       "mov.b64 {w0, w1}, %2;\n\t"
@@ -79,11 +79,11 @@ __device__ __forceinline__ uint64_t shoup_lazy_mad3(uint64_t y, uint64_t w, uint
       "mov.b64 {n0, n1}, %4;\n\t"
       "mul.hi.u32 a1, y0, p1;\n\t"
       "mul.hi.u32 b1, y1, p0;\n\t"
-      "add.cc.u32 s0, a1, b1;\n\t"
-      "addc.u32 s1, 0, 0;\n\t"
-      "mov.b64 S, {s0, s1};\n\t"
+      "cvt.u64.u32 S, a1;\n\t"
       "mad.wide.u32 T, y1, p1, S;\n\t"
       "mov.b64 {t0, t1}, T;\n\t"
+      "add.cc.u32 t0, t0, b1;\n\t"
+      "addc.u32 t1, t1, 0;\n\t"
       "mul.wide.u32 R, y0, w0;\n\t"
       "mad.wide.u32 R, t0, n0, R;\n\t"
       "mov.b64 {r0, r1}, R;\n\t"
