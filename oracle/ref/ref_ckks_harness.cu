@@ -12,6 +12,7 @@
 //
 // usage: ref_ckks_harness <out file> <log2 N> <k> <kl> <prec>
 //        ref_ckks_harness --time <log2 N> <k> <kl> <prec> <reps>   (see time_hmult)
+//        ref_ckks_harness --digest <log2 N> <k> <kl> <prec>        (see digests)
 //
 // Part 1, seeded operands (the test regenerates them): every limb of every
 // polynomial is filled like ref_harness does (word j of limb i is output
@@ -271,7 +272,66 @@ static int time_hmult(int reps) {
   return 0;
 }
 
+// Digest mode, for shapes too large to keep as fixtures: the seeded ckks_mul
+// (HMult, relinearise, rescale) and ckks_rotate_left by 1 of part 1 at level
+// k - 1 (same seeds and scales), each output limb reduced to a position-
+// weighted digest sum_j c_j (2 j + 1) G mod 2^64, G = 0x9E3779B97F4A7C15.
+// Prints one JSON line: primes, then per op its level, scale and the digests
+// of c0's limbs followed by c1's.
+static uint64_t limb_digest(const uint64_t* c) {
+  uint64_t d = 0;
+  for (int j = 0; j < g_N; j++) d += c[j] * ((2 * (uint64_t)j + 1) * 0x9E3779B97F4A7C15ull);
+  return d;
+}
+
+static void print_digests(const char* name, Context* ctx, cipher_t* c, bool last) {
+  const int n = c->level + 1;
+  const std::vector<uint64_t> c0 = limbs(ctx, &c->c[0], n), c1 = limbs(ctx, &c->c[1], n);
+  printf("\"%s\": {\"level\": %d, \"scale\": %llu, \"digests\": [", name, c->level,
+         (unsigned long long)c->scale);
+  for (int i = 0; i < 2 * n; i++) {
+    const uint64_t* base = (i < n ? c0.data() : c1.data()) + (size_t)(i % n) * g_N;
+    printf("%s%llu", i ? ", " : "", (unsigned long long)limb_digest(base));
+  }
+  printf("]}%s", last ? "" : ", ");
+}
+
+static int digests() {
+  CKKSContext* ctx = new CKKSContext();
+  const int slots = g_N / 2, level = g_k - 1;
+  set_key(ctx, ctx->keys.evk, 111, 112);
+  RotationKey* rk = new RotationKey;
+  set_key(ctx, rk, 123, 124);                             // rotation key for r = 1: seeds 113 + 10 r, 114 + 10 r
+  ctx->keys.rtk_left[1] = rk;
+  cipher_t a, b, c, out;
+  set_ct(ctx, &a, 101, 102, level, kScaleA, slots);
+  set_ct(ctx, &b, 103, 104, level, kScaleB, slots);
+  cipher_init(ctx, &out);
+  ckks_mul(ctx, &out, &a, &b);
+  if (!check_cuda("ckks_mul")) return 1;
+  printf("{\"N\": %d, \"k\": %d, \"kl\": %d, \"primes\": [", g_N, g_k, g_kl);
+  for (size_t i = 0; i < g_primes.size(); i++) printf("%s%llu", i ? ", " : "", (unsigned long long)g_primes[i]);
+  printf("], ");
+  print_digests("hmult", ctx, &out, false);
+  set_ct(ctx, &c, 105, 106, level, kScaleA, slots);
+  ckks_rotate_left(ctx, &out, &c, 1);
+  if (!check_cuda("ckks_rotate_left")) return 1;
+  print_digests("rotate1", ctx, &out, true);
+  printf("}\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 6 && strcmp(argv[1], "--digest") == 0) {
+    g_N = 1 << atoi(argv[2]);
+    g_k = atoi(argv[3]);
+    g_kl = atoi(argv[4]);
+    CUDAManager::init(g_k, g_kl, g_N, atoi(argv[5]));
+    if (!check_cuda("init")) return 1;
+    g_primes = CUDAManager::RNSQPrimes;
+    g_primes.insert(g_primes.end(), CUDAManager::RNSBPrimes.begin(), CUDAManager::RNSBPrimes.end());
+    return digests();
+  }
   if (argc == 7 && strcmp(argv[1], "--time") == 0) {
     g_N = 1 << atoi(argv[2]);
     g_k = atoi(argv[3]);
@@ -284,7 +344,8 @@ int main(int argc, char** argv) {
   }
   if (argc != 6) {
     fprintf(stderr, "usage: ref_ckks_harness <out> <log2 N> <k> <kl> <prec>\n"
-                    "       ref_ckks_harness --time <log2 N> <k> <kl> <prec> <reps>\n");
+                    "       ref_ckks_harness --time <log2 N> <k> <kl> <prec> <reps>\n"
+                    "       ref_ckks_harness --digest <log2 N> <k> <kl> <prec>\n");
     return 2;
   }
   g_N = 1 << atoi(argv[2]);

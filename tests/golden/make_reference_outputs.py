@@ -25,9 +25,13 @@ aoa-dgt's CKKS layer with ref_ckks_harness's records for DGT_CKKS_CONFIGS
 Usage (on a machine with a GPU and the built harnesses):
     python tests/golden/make_reference_outputs.py OUT_DIR
 writes OUT_DIR/reference_outputs.npz, reference_ckks_outputs.npz,
-reference_dgt_outputs.npz and reference_dgt_ckks_outputs.npz (copy them into
-tests/golden/).
+reference_dgt_outputs.npz, reference_dgt_ckks_outputs.npz and
+reference_digests.json (copy them into tests/golden/).  The digests are the
+reference's ckks_mul and rotation at the headline shape (N = 2^16, 30 + 31
+primes) on the seeded operands of the CKKS records, each output limb reduced
+to a position-weighted sum (ref_ckks_harness --digest).
 """
+import json
 import os
 import subprocess
 import sys
@@ -57,6 +61,9 @@ DGT_TAGS = {1: "dgt_fwd", 2: "dgt_inv", 3: "mul", 4: "modup", 5: "moddown", 6: "
 # (log2 N, k, kl, prec) of the CKKS-layer records (aoa-ntt, then aoa-dgt)
 CKKS_CONFIGS = [(10, 4, 5, 55)]
 DGT_CKKS_CONFIGS = [(10, 4, 4, 48)]
+# (log2 N, k, kl, prec) of the full-shape digests (ckks_mul and a rotation at
+# the headline shape, too large to keep whole)
+DIGEST_CONFIGS = [(16, 30, 31, 55)]
 CKKS_TAGS = {20: "hmult_l%d", 21: "hmult_norescale_l%d", 23: "conjugate_l%d", 24: "add_l%d", 25: "sub_l%d",
              26: "encode_s%d", 40: "sk", 41: "evk", 42: "enc300", 43: "enc301", 44: "mul_keys", 45: "dec300",
              46: "dec_mul", 47: "rot1_keys", 48: "dec_rot1"}
@@ -155,6 +162,16 @@ def main():
     dst = os.path.join(out_dir, "reference_dgt_ckks_outputs.npz")
     np.savez_compressed(dst, **arrays)
     print("wrote", dst, sorted(arrays))
+    digests = []
+    for log_n, k, kl, prec in DIGEST_CONFIGS:
+        out = subprocess.run([CKKS_HARNESS, "--digest", str(log_n), str(k), str(kl), str(prec)], check=True,
+                             capture_output=True, text=True).stdout
+        digests.append(json.loads([l for l in out.splitlines() if l.startswith("{")][-1]))
+    dst = os.path.join(out_dir, "reference_digests.json")
+    with open(dst, "w") as f:
+        json.dump(digests, f)
+        f.write("\n")
+    print("wrote", dst)
 
 
 if __name__ == "__main__":
