@@ -15,6 +15,7 @@
 // runs it.
 //
 // usage: ref_dgt_ckks_harness <out file> <log2 nphi> <k> <kl> <prec>
+//        ref_dgt_ckks_harness --digest <log2 nphi> <k> <kl> <prec>   (see digests)
 // Records (little-endian u64): {tag, level, nwords, words}; a ciphertext
 // record holds [aux, scale, slots, c0 limbs 0..n-1, c1 limbs 0..n-1]:
 //   20 ckks_mul(a, b), 21 ckks_mul_without_rescale(a, b), 22 ckks_rotate_left
@@ -232,9 +233,64 @@ static void reference_keys(CKKSContext* ctx) {
   cudaStreamSynchronize(ctx->get_stream());
 }
 
+// Digest mode, as ref_ckks_harness --digest: ckks_mul and ckks_rotate_left
+// by 1 of the seeded operands at level k - 1, each output limb (coefficients)
+// reduced to sum_j c_j (2 j + 1) G mod 2^64, G = 0x9E3779B97F4A7C15.
+static uint64_t limb_digest(const uint64_t* c) {
+  uint64_t d = 0;
+  for (int j = 0; j < g_nphi; j++) d += c[j] * ((2 * (uint64_t)j + 1) * 0x9E3779B97F4A7C15ull);
+  return d;
+}
+
+static void print_digests(const char* name, Context* ctx, cipher_t* c, bool last) {
+  const int n = c->level + 1;
+  const std::vector<uint64_t> c0 = limbs(ctx, &c->c[0], n), c1 = limbs(ctx, &c->c[1], n);
+  printf("\"%s\": {\"level\": %d, \"scale\": %llu, \"digests\": [", name, c->level,
+         (unsigned long long)c->scale);
+  for (int i = 0; i < 2 * n; i++) {
+    const uint64_t* base = (i < n ? c0.data() : c1.data()) + (size_t)(i % n) * g_nphi;
+    printf("%s%llu", i ? ", " : "", (unsigned long long)limb_digest(base));
+  }
+  printf("]}%s", last ? "" : ", ");
+}
+
+static int digests() {
+  CKKSContext* ctx = new CKKSContext();
+  const int slots = g_nphi / 2, level = g_k - 1;
+  ctx->evk = new_key(ctx, 111, 112);
+  ctx->rtk_left[1] = new_key(ctx, 123, 124);
+  cipher_t a, b, c, out;
+  cipher_init(ctx, &out);
+  set_ct(ctx, &a, 101, 102, level, kScaleA, slots);
+  set_ct(ctx, &b, 103, 104, level, kScaleB, slots);
+  ckks_mul(ctx, &out, &a, &b);
+  if (!check_cuda("ckks_mul")) return 1;
+  printf("{\"N\": %d, \"k\": %d, \"kl\": %d, \"primes\": [", g_nphi, g_k, g_kl);
+  for (size_t i = 0; i < g_primes.size(); i++) printf("%s%llu", i ? ", " : "", (unsigned long long)g_primes[i]);
+  printf("], ");
+  print_digests("hmult", ctx, &out, false);
+  set_ct(ctx, &c, 105, 106, level, kScaleA, slots);
+  ckks_rotate_left(ctx, &out, &c, 1);
+  if (!check_cuda("ckks_rotate_left")) return 1;
+  print_digests("rotate1", ctx, &out, true);
+  printf("}\n");
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 6 && strcmp(argv[1], "--digest") == 0) {
+    g_nphi = 1 << atoi(argv[2]);
+    g_k = atoi(argv[3]);
+    g_kl = atoi(argv[4]);
+    CUDAEngine::init(g_k, g_kl, g_nphi, atoi(argv[5]));
+    if (!check_cuda("init")) return 1;
+    g_primes = CUDAEngine::RNSPrimes;
+    g_primes.insert(g_primes.end(), CUDAEngine::RNSBPrimes.begin(), CUDAEngine::RNSBPrimes.end());
+    return digests();
+  }
   if (argc != 6) {
-    fprintf(stderr, "usage: ref_dgt_ckks_harness <out> <log2 nphi> <k> <kl> <prec>\n");
+    fprintf(stderr, "usage: ref_dgt_ckks_harness <out> <log2 nphi> <k> <kl> <prec>\n"
+                    "       ref_dgt_ckks_harness --digest <log2 nphi> <k> <kl> <prec>\n");
     return 2;
   }
   g_nphi = 1 << atoi(argv[2]);

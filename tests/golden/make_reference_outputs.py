@@ -29,7 +29,8 @@ reference_dgt_outputs.npz, reference_dgt_ckks_outputs.npz and
 reference_digests.json (copy them into tests/golden/).  The digests are the
 reference's ckks_mul and rotation at the headline shape (N = 2^16, 30 + 31
 primes) on the seeded operands of the CKKS records, each output limb reduced
-to a position-weighted sum (ref_ckks_harness --digest).
+to a position-weighted sum, from both variants (ref_ckks_harness and
+ref_dgt_ckks_harness --digest).
 """
 import json
 import os
@@ -164,9 +165,12 @@ def main():
     print("wrote", dst, sorted(arrays))
     digests = []
     for log_n, k, kl, prec in DIGEST_CONFIGS:
-        out = subprocess.run([CKKS_HARNESS, "--digest", str(log_n), str(k), str(kl), str(prec)], check=True,
-                             capture_output=True, text=True).stdout
-        digests.append(json.loads([l for l in out.splitlines() if l.startswith("{")][-1]))
+        for variant, harness in (("aoa-ntt", CKKS_HARNESS), ("aoa-dgt", DGT_CKKS_HARNESS)):
+            out = subprocess.run([harness, "--digest", str(log_n), str(k), str(kl), str(prec)], check=True,
+                                 capture_output=True, text=True).stdout
+            rec = json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+            rec["variant"] = variant
+            digests.append(rec)
     dst = os.path.join(out_dir, "reference_digests.json")
     with open(dst, "w") as f:
         json.dump(digests, f)

@@ -4,7 +4,8 @@ The digests of pdroalves/aoa's own ckks_mul and rotation at N = 2^16, 30 Q +
 31 special primes (its 55-bit set, 63-bit q0; tests/test_oracle_reference_digests.py)
 are compared with this engine's per-call and batched HMult + relinearise +
 rescale and its per-call and batched rotation of the same seeded operands,
-through the C ABI (63-bit q0 limbs on strict butterflies, the others lazy)."""
+through the C ABI (63-bit q0 limbs on strict butterflies, the others lazy),
+on an NTT context and on a DGT context (aoa-dgt's digests are the same)."""
 import numpy as np
 import pytest
 
@@ -15,14 +16,18 @@ from tests.test_oracle_reference_digests import digests, load
 pytestmark = pytest.mark.gpu
 
 
-def test_engine_digests_equal_reference():
+@pytest.mark.parametrize("variant", ["aoa-ntt", "aoa-dgt"])
+def test_engine_digests_equal_reference(variant):
     require_gpu()
     import aoa_b200 as aoa
-    d = load()
+    d = load(variant)
     N, k = d["N"], d["k"]
     primes = d["primes"]
     E = aoa.Engine(16, primes[:k], primes[k:], scale_bits=55)
     ctx = aoa.Context(E)
+    dgt = variant == "aoa-dgt"
+    if dgt:                                     # roots derived from the primes' generators
+        ctx.set_transform(aoa.AOA_DGT)
     evk = aoa.SwitchKey(ctx, *seeded_key(111, 112, primes, N), domain=aoa.AOA_COEF)
     rtk = aoa.SwitchKey(ctx, *seeded_key(123, 124, primes, N), domain=aoa.AOA_COEF)
     a_in, b_in, c_in = (seeded_ct(101, 102, primes[:k], N), seeded_ct(103, 104, primes[:k], N),
@@ -41,8 +46,10 @@ def test_engine_digests_equal_reference():
         assert digests(g0, g1, k - 1) == d["hmult"]["digests"]
     r = aoa.Ciphertext(ctx)
     aoa.ckks_rotate_left(ctx, r, ct(c_in, SCALE_A), 1, rtk)
-    rs = [aoa.Ciphertext(ctx) for _ in range(2)]
-    aoa.ckks_rotate_batch(ctx, rs, [ct(c_in, SCALE_A), ct(c_in, SCALE_A)], 1, rtk)
+    rs = []
+    if not dgt:                                 # batched rotations run on NTT contexts
+        rs = [aoa.Ciphertext(ctx) for _ in range(2)]
+        aoa.ckks_rotate_batch(ctx, rs, [ct(c_in, SCALE_A), ct(c_in, SCALE_A)], 1, rtk)
     for o in [r] + rs:
         assert o.level == d["rotate1"]["level"] and o.scale == d["rotate1"]["scale"]
         g0, g1 = o.download(nlimbs=k)

@@ -1,8 +1,9 @@
 """The oracle at the headline shape against the reference itself.
 
 tests/golden/reference_digests.json holds digests of what pdroalves/aoa's
-aoa-ntt computed on a B200 at N = 2^16 with 30 Q and 31 special primes (its
-own 55-bit prime set, 63-bit q0; oracle/ref/ref_ckks_harness.cu --digest):
+aoa-ntt and aoa-dgt computed on a B200 at N = 2^16 with 30 Q and 31 special
+primes (their own 55-bit prime set, 63-bit q0; oracle/ref/ref_ckks_harness.cu
+and ref_dgt_ckks_harness.cu --digest):
 ckks_mul (HMult, relinearise, rescale; src/ckks/ckks.cpp:273-347) and
 ckks_rotate_left by one slot (ckks.cpp:982-1009) of the seeded operands and
 keys of the CKKS records (tests/test_oracle_reference_ckks.py) at level 29.
@@ -22,9 +23,9 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref
 G = np.uint64(0x9E3779B97F4A7C15)
 
 
-def load():
+def load(variant="aoa-ntt"):
     with open(GOLDEN) as f:
-        return json.load(f)[0]
+        return [d for d in json.load(f) if d["variant"] == variant][0]
 
 
 def digests(c0, c1, n):
@@ -33,6 +34,14 @@ def digests(c0, c1, n):
     with np.errstate(over="ignore"):
         w = (2 * np.arange(N, dtype=np.uint64) + np.uint64(1)) * G
         return [int(np.sum(x[i] * w, dtype=np.uint64)) for x in (c0, c1) for i in range(n)]
+
+
+def test_both_reference_variants_agree():
+    """aoa-ntt and aoa-dgt give the same residues at the headline shape (the
+    transform only changes the domain of exact products)."""
+    a, b = load("aoa-ntt"), load("aoa-dgt")
+    assert a["primes"] == b["primes"]
+    assert a["hmult"] == b["hmult"] and a["rotate1"] == b["rotate1"]
 
 
 def test_fixture_is_the_headline_shape():
