@@ -283,6 +283,12 @@ void gi_tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_
                   uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st);
 void gi_keyswitch_mul_op(const Engine& E, const uint64_t* xq, const uint64_t* xb, const uint64_t* key, uint64_t* k0,
                          uint64_t* k1, int nq, cudaStream_t st);
+// the same over a batch of n ops (one launch each)
+void gi_tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D, int n, int nlimbs,
+                        cudaStream_t st);
+void gi_keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb,
+                               long xb_stride, const uint64_t* key, uint64_t* k, long k_stride, int n, int nq,
+                               cudaStream_t st);
 // ckks.cu: limb transforms of a kind (AOA_NTT / AOA_DGT) and domain changes
 void xform(const Engine& E, int kind, uint64_t* d, int npolys, int first_prime, int nlimbs, long stride, bool fwd,
            cudaStream_t st);

@@ -364,8 +364,7 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
   const int tk = C.transform;
   uint64_t* D2 = D + 2L * n * half;
   if (tk == AOA_DGT) {
-    for (int z = 0; z < n; z++)
-      gi_tensor_op(E, a[z]->d, half, b[z]->d, half, D + z * half, D + (n + z) * half, D2 + z * half, m, st);
+    gi_tensor_batch_op(E, ptr, half, D, n, m, st);
   } else {
     tensor_batch_op(E, ptr, half, D, n, m, st);
   }
@@ -382,8 +381,7 @@ static void hmult_batch_group(Ctx& C, cudaStream_t st, void*& ws, size_t& ws_byt
   modup(E, T, half, UB, (long)kl * N, n, level, st);
   if (tk == AOA_DGT) {
     xform(E, tk, UB, n, k, kl, kl, true, st);
-    for (int z = 0; z < n; z++)
-      gi_keyswitch_mul_op(E, D2 + z * half, UB + (long)z * kl * N, evk->d, KS + z * ks, KS + (n + z) * ks, m, st);
+    gi_keyswitch_mul_batch_op(E, D2, half, UB, (long)kl * N, evk->d, KS, ks, n, m, st);
   } else if (fuse & kFuseKeyProduct) {
     NttIo io;                                  // special-limb transform with the key products fused
     io.epi.mode = kEpiKeyProduct;

@@ -109,11 +109,9 @@ __global__ void gi_mul(uint64_t* c, long cs, const uint64_t* a, long as, const u
 // HMult tensor on GI limbs (dr2_dgt, dgt.cu:1252-1283, with the middle term
 // as (a0 + a1)(b0 + b1) - d0 - d2 as ckks_mul_without_rescale forms it,
 // aoa-dgt src/ckks.cpp:299-306).
-__global__ void gi_tensor(const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0, uint64_t* d1,
-                          uint64_t* d2, int H, const PrimeConst* __restrict__ pc) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= H) return;
-  const int limb = blockIdx.y;
+__device__ __forceinline__ void gi_tensor_at(const uint64_t* a, long a_half, const uint64_t* b, long b_half,
+                                             uint64_t* d0, uint64_t* d1, uint64_t* d2, int H,
+                                             const PrimeConst* __restrict__ pc, int n, int limb) {
   const long off = (long)limb * 2 * H + n;
   const PrimeConst& P = pc[limb];
   const uint64_t q = P.q;
@@ -129,13 +127,30 @@ __global__ void gi_tensor(const uint64_t* a, long a_half, const uint64_t* b, lon
   d1[off + H] = sub_mod(si, add_mod(e0i, e2i, q), q);
 }
 
-// Key-switch products on GI limbs: k0 = x * key_b, k1 = x * key_a over the QB
-// limbs of the extended input (Q limbs < nq at xq, the B limbs at xb).
-__global__ void gi_keyswitch_mul(const uint64_t* xq, const uint64_t* xb, const uint64_t* key, long key_half,
-                                 uint64_t* k0, uint64_t* k1, int nq, int K, int H, const PrimeConst* __restrict__ pc) {
+__global__ void gi_tensor(const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0, uint64_t* d1,
+                          uint64_t* d2, int H, const PrimeConst* __restrict__ pc) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= H) return;
-  const int l = blockIdx.y;
+  gi_tensor_at(a, a_half, b, b_half, d0, d1, d2, H, pc, n, blockIdx.y);
+}
+
+// the tensor of op z = blockIdx.z of a batch: operands ptr.a[z] / ptr.b[z]
+// ([c0 | c1], stride half), outputs D0 = D, D1 = D + n half, D2 = D + 2n half
+// at op stride half
+__global__ void gi_tensor_batch(CtPtrs ptr, long half, uint64_t* D, int nops, int H, const PrimeConst* __restrict__ pc) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= H) return;
+  const int z = blockIdx.z;
+  uint64_t* d = D + (long)z * half;
+  const long nh = (long)nops * half;
+  gi_tensor_at(ptr.a[z], half, ptr.b[z], half, d, d + nh, d + 2 * nh, H, pc, n, blockIdx.y);
+}
+
+// Key-switch products on GI limbs: k0 = x * key_b, k1 = x * key_a over the QB
+// limbs of the extended input (Q limbs < nq at xq, the B limbs at xb).
+__device__ __forceinline__ void gi_keyswitch_at(const uint64_t* xq, const uint64_t* xb, const uint64_t* key,
+                                                long key_half, uint64_t* k0, uint64_t* k1, int nq, int K, int H,
+                                                const PrimeConst* __restrict__ pc, int n, int l) {
   const int prime = l < nq ? l : K + (l - nq);
   const long N = 2L * H;
   const uint64_t* x = (l < nq ? xq + (long)l * N : xb + (long)(l - nq) * N) + n;
@@ -149,6 +164,25 @@ __global__ void gi_keyswitch_mul(const uint64_t* xq, const uint64_t* xb, const u
   gi_mul_dev(x[0], x[H], ka[0], ka[H], r, i, P);
   k1[(long)l * N + n] = r;
   k1[(long)l * N + n + H] = i;
+}
+
+__global__ void gi_keyswitch_mul(const uint64_t* xq, const uint64_t* xb, const uint64_t* key, long key_half,
+                                 uint64_t* k0, uint64_t* k1, int nq, int K, int H, const PrimeConst* __restrict__ pc) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= H) return;
+  gi_keyswitch_at(xq, xb, key, key_half, k0, k1, nq, K, H, pc, n, blockIdx.y);
+}
+
+// the key products of op z = blockIdx.z: x at xq + z xq_stride (Q limbs) and
+// xb + z xb_stride (B limbs), k0 at k + z k_stride, k1 at k + (n + z) k_stride
+__global__ void gi_keyswitch_mul_batch(const uint64_t* xq, long xq_stride, const uint64_t* xb, long xb_stride,
+                                       const uint64_t* key, long key_half, uint64_t* k, long k_stride, int nops,
+                                       int nq, int K, int H, const PrimeConst* __restrict__ pc) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= H) return;
+  const int z = blockIdx.z;
+  gi_keyswitch_at(xq + z * xq_stride, xb + z * xb_stride, key, key_half, k + z * k_stride, k + (nops + z) * k_stride,
+                  nq, K, H, pc, n, blockIdx.y);
 }
 
 // Reference GaussianInteger layout <-> planar GI limbs.
@@ -305,6 +339,25 @@ void gi_mul_op(const Engine& E, uint64_t* c, long cs, const uint64_t* a, long as
 void gi_tensor_op(const Engine& E, const uint64_t* a, long a_half, const uint64_t* b, long b_half, uint64_t* d0,
                   uint64_t* d1, uint64_t* d2, int nlimbs, cudaStream_t st) {
   gi_tensor<<<gi_grid(E, nlimbs), 256, 0, st>>>(a, a_half, b, b_half, d0, d1, d2, (int)(E.N / 2), E.d_pc);
+  note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+void gi_tensor_batch_op(const Engine& E, const CtPtrs& ptr, long half, uint64_t* D, int n, int nlimbs,
+                        cudaStream_t st) {
+  const dim3 g = gi_grid(E, nlimbs);
+  gi_tensor_batch<<<dim3(g.x, g.y, n), 256, 0, st>>>(ptr, half, D, n, (int)(E.N / 2), E.d_pc);
+  note_launch();
+  AOA_CHECK_LAUNCH();
+}
+
+void gi_keyswitch_mul_batch_op(const Engine& E, const uint64_t* xq, long xq_stride, const uint64_t* xb,
+                               long xb_stride, const uint64_t* key, uint64_t* k, long k_stride, int n, int nq,
+                               cudaStream_t st) {
+  const dim3 g = gi_grid(E, nq + E.kl);
+  gi_keyswitch_mul_batch<<<dim3(g.x, g.y, n), 256, 0, st>>>(xq, xq_stride, xb, xb_stride, key,
+                                                              (long)(E.k + E.kl) * E.N, k, k_stride, n, nq, E.k,
+                                                              (int)(E.N / 2), E.d_pc);
   note_launch();
   AOA_CHECK_LAUNCH();
 }
