@@ -61,9 +61,13 @@ GIh derived_root(uint64_t q, uint64_t g, long N) {
 // at data + p*poly_stride + l*N, planes [re | im] of H = N/2 words; entry n
 // of the prime's table is r^(+-n) = c + di, applied as the three-product
 // (a + ib)(c + id) = (k1 - k3) + i (k1 + k2), k1 = c (a + b), k2 = a (d - c),
-// k3 = b (c + d) (a + b < 2q, which a Shoup product takes).
+// k3 = b (c + d) (a + b < 2q, which a Shoup product takes).  For primes below
+// 2^kLazyPrimeBits the products use the three-product quotient of the limb
+// transforms (each in [0, 4q)); with lazy_out (a forward twist whose limb
+// transform takes inputs below 16q) the results stay in [0, 8q), otherwise
+// they are reduced to [0, q).
 __global__ void gi_twist(uint64_t* data, long poly_stride, int npolys, int first_prime, const uint64_t* __restrict__ tab,
-                         int H, const PrimeConst* __restrict__ pc) {
+                         int H, const PrimeConst* __restrict__ pc, bool lazy_out) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= H) return;
   const int item = blockIdx.y, limb = item / npolys, p = item % npolys;
@@ -72,6 +76,26 @@ __global__ void gi_twist(uint64_t* data, long poly_stride, int npolys, int first
   const uint64_t q = pc[prime].q;
   const uint64_t* w = tab + (long)prime * 6 * H + n;
   const uint64_t a = x[n], b = x[H + n];
+  if (q < (1ull << kLazyPrimeBits)) {
+    const uint64_t nq = 0 - q, q2 = q << 1, q4 = q << 2;
+    uint64_t k1 = shoup_lazy_mad3(a + b, w[0], w[H], nq);
+    uint64_t k2 = shoup_lazy_mad3(a, w[2 * H], w[3 * H], nq);
+    uint64_t k3 = shoup_lazy_mad3(b, w[4 * H], w[5 * H], nq);
+    if (lazy_out) {
+      x[n] = k1 - k3 + q4;
+      x[H + n] = k1 + k2;
+      return;
+    }
+    k1 = k1 >= q2 ? k1 - q2 : k1;
+    k1 = k1 >= q ? k1 - q : k1;
+    k2 = k2 >= q2 ? k2 - q2 : k2;
+    k2 = k2 >= q ? k2 - q : k2;
+    k3 = k3 >= q2 ? k3 - q2 : k3;
+    k3 = k3 >= q ? k3 - q : k3;
+    x[n] = sub_mod(k1, k3, q);
+    x[H + n] = add_mod(k1, k2, q);
+    return;
+  }
   const uint64_t k1 = shoup(a + b, w[0], w[H], q);
   const uint64_t k2 = shoup(a, w[2 * H], w[3 * H], q);
   const uint64_t k3 = shoup(b, w[4 * H], w[5 * H], q);
@@ -314,15 +338,17 @@ void dgt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
   const NttTables T = dgt_tables(E);
   dgt_twist_tables(E);
   if (forward) {
+    // the limb transforms of rings of 2^11 and more take forward inputs below
+    // 16q on their lazy limbs (the smaller ones run canonical butterflies)
     gi_twist<<<gi_grid(E, nlimbs * npolys), 256, 0, st>>>(data, poly_stride * E.N, npolys, first_prime, E.d_twist,
-                                                            H, E.d_pc);
+                                                            H, E.d_pc, T.log_n >= 10);
     note_launch();
     AOA_CHECK_LAUNCH();
     ntt_batch_tables(E, T, data, npolys, first_prime, 2 * nlimbs, 2 * poly_stride, true, st);
   } else {
     ntt_batch_tables(E, T, data, npolys, first_prime, 2 * nlimbs, 2 * poly_stride, false, st);
     gi_twist<<<gi_grid(E, nlimbs * npolys), 256, 0, st>>>(data, poly_stride * E.N, npolys, first_prime,
-                                                            E.d_untwist, H, E.d_pc);
+                                                            E.d_untwist, H, E.d_pc, false);
     note_launch();
     AOA_CHECK_LAUNCH();
   }

@@ -167,11 +167,24 @@ def run_reference(args, world, rank):
 
 
 def profile_case(args, aoa, ctx, rr, ps):
-    """Small fixed cases for ncu: `ntt` = forward + inverse over args.polys
-    polys of 30 limbs (args.polys * 15 MiB); `hmult` = 2 HMult+relin+rescale;
-    `batch` = 2 batched calls of args.batch HMult+relin+rescale."""
+    """Small fixed cases for ncu: `ntt` / `dgt` = forward + inverse NTT / DGT
+    over args.polys polys of 30 limbs (args.polys * 15 MiB); `hmult` = 2
+    HMult+relin+rescale; `batch` = 2 batched calls of args.batch
+    HMult+relin+rescale."""
     N = 1 << LOG_N
-    if args.profile_case == "ntt":
+    if args.profile_case == "dgt":
+        ctx.set_transform(aoa.AOA_DGT)
+        buf = ctx.alloc((args.polys, K, N))
+        xs = rr(ps[:K])
+        for p in range(args.polys):
+            aoa.capi.check(aoa.capi.load().aoa_memcpy_h2d(ctx.handle, buf.offset(p * K * N), aoa.capi.ptr(xs),
+                                                          xs.nbytes))
+        for _ in range(2):
+            ctx.dgt_fwd(buf, args.polys, 0, K)
+            ctx.dgt_inv(buf, args.polys, 0, K)
+        ctx.sync()
+        assert np.array_equal(buf.numpy()[0], xs), "inverse(forward(x)) != x"
+    elif args.profile_case == "ntt":
         buf = ctx.alloc((args.polys, K, N))
         xs = rr(ps[:K])
         for p in range(args.polys):
@@ -402,9 +415,9 @@ def main():
     ap.add_argument("--impl", default="aoa", choices=["aoa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-systems", action="store_true", help="skip the uneven-batch and serving measurements")
-    ap.add_argument("--profile-case", choices=["ntt", "hmult", "batch"],
+    ap.add_argument("--profile-case", choices=["ntt", "dgt", "hmult", "batch"],
                     help="run a small fixed case for ncu captures (no timing, no JSON)")
-    ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt")
+    ap.add_argument("--polys", type=int, default=16, help="polys of 30 limbs for --profile-case ntt / dgt")
     ap.add_argument("--autotune", action="store_true",
                     help="run the transform autotuner first (default: the engine's measured-best shapes)")
     ap.add_argument("--no-autotune", action="store_true", help="(default) keep the engine's transform shapes")
