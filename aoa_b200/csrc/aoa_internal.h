@@ -40,6 +40,7 @@ constexpr unsigned kErrWaitTimeout = 1u;   // an mbarrier wait hit its iteration
 #define AOA_LAZY_PRIME_BITS 60
 #endif
 constexpr int kLazyPrimeBits = AOA_LAZY_PRIME_BITS;
+constexpr int kButterflyCanonical = 0, kButterflyLazy = 1, kButterflyLazyQ1 = 2;
 constexpr int kLargeItems = 1536;           // limb-transform launches this large use ntt_waves_large
 
 struct Tune {
@@ -103,8 +104,10 @@ struct Engine {
   long N = 0;
   int k = 0, kl = 0, nprimes = 0;
   int scale_bits = 0;
-  bool lazy = false;          // every prime < 2^kLazyPrimeBits: Harvey lazy butterflies
-  std::vector<char> lazy_prime;   // per prime: q < 2^kLazyPrimeBits
+  // butterfly kind per prime (kButterfly*): canonical, Harvey lazy (q <
+  // 2^kLazyPrimeBits), or lazy with the remainder for q = 1 mod 2^32
+  std::vector<char> prime_kind;
+  int ntt_kind = kButterflyCanonical;   // the kind every prime shares, -1 when they differ
   std::vector<uint64_t> primes, gens;
   std::vector<PrimeConst> h_pc;
   PrimeConst* d_pc = nullptr;
@@ -205,10 +208,10 @@ struct NttTables {
   const PrimeConst* pc = nullptr;
   int log_n = 0;
   int prime_shift = 0;     // limb l uses prime first + (l >> prime_shift)
-  bool lazy = false;
-  // per prime (q < 2^kLazyPrimeBits), when only some primes allow lazy
-  // butterflies: the limbs run in runs of one kind
-  const char* lazy_prime = nullptr;
+  int kind = kButterflyCanonical;   // butterfly kind of every limb
+  // per prime butterfly kind, when the primes' kinds differ: the limbs run in
+  // runs of one kind
+  const char* prime_kind = nullptr;
 };
 // Fused ends of a limb transform.  NttIo::src: the first pass reads item
 // (p, l) from src + p * src_poly_stride + l * N instead of the data (an

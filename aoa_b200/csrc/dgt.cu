@@ -63,9 +63,35 @@ GIh derived_root(uint64_t q, uint64_t g, long N) {
 // (a + ib)(c + id) = (k1 - k3) + i (k1 + k2), k1 = c (a + b), k2 = a (d - c),
 // k3 = b (c + d) (a + b < 2q, which a Shoup product takes).  For primes below
 // 2^kLazyPrimeBits the products use the three-product quotient of the limb
-// transforms (each in [0, 4q)); with lazy_out (a forward twist whose limb
-// transform takes inputs below 16q) the results stay in [0, 8q), otherwise
-// they are reduced to [0, q).
+// transforms (each in [0, 4q); the shorter remainder where q = 1 mod 2^32);
+// with lazy_out (a forward twist whose limb transform takes inputs below 16q)
+// the results stay in [0, 8q), otherwise they are reduced to [0, q).
+template <bool Q1>
+__device__ __forceinline__ void gi_twist_lazy(uint64_t* x, int n, int H, const uint64_t* w, uint64_t a, uint64_t b,
+                                              uint64_t q, bool lazy_out) {
+  auto mul = [&](uint64_t y, uint64_t wv, uint64_t wp) {
+    if constexpr (Q1) return shoup_lazy_mad3_q1(y, wv, wp, q);
+    else return shoup_lazy_mad3(y, wv, wp, 0 - q);
+  };
+  const uint64_t q2 = q << 1, q4 = q << 2;
+  uint64_t k1 = mul(a + b, w[0], w[H]);
+  uint64_t k2 = mul(a, w[2 * H], w[3 * H]);
+  uint64_t k3 = mul(b, w[4 * H], w[5 * H]);
+  if (lazy_out) {
+    x[n] = k1 - k3 + q4;
+    x[H + n] = k1 + k2;
+    return;
+  }
+  k1 = k1 >= q2 ? k1 - q2 : k1;
+  k1 = k1 >= q ? k1 - q : k1;
+  k2 = k2 >= q2 ? k2 - q2 : k2;
+  k2 = k2 >= q ? k2 - q : k2;
+  k3 = k3 >= q2 ? k3 - q2 : k3;
+  k3 = k3 >= q ? k3 - q : k3;
+  x[n] = sub_mod(k1, k3, q);
+  x[H + n] = add_mod(k1, k2, q);
+}
+
 __global__ void gi_twist(uint64_t* data, long poly_stride, int npolys, int first_prime, const uint64_t* __restrict__ tab,
                          int H, const PrimeConst* __restrict__ pc, bool lazy_out) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -76,24 +102,9 @@ __global__ void gi_twist(uint64_t* data, long poly_stride, int npolys, int first
   const uint64_t q = pc[prime].q;
   const uint64_t* w = tab + (long)prime * 6 * H + n;
   const uint64_t a = x[n], b = x[H + n];
-  if (q < (1ull << kLazyPrimeBits)) {
-    const uint64_t nq = 0 - q, q2 = q << 1, q4 = q << 2;
-    uint64_t k1 = shoup_lazy_mad3(a + b, w[0], w[H], nq);
-    uint64_t k2 = shoup_lazy_mad3(a, w[2 * H], w[3 * H], nq);
-    uint64_t k3 = shoup_lazy_mad3(b, w[4 * H], w[5 * H], nq);
-    if (lazy_out) {
-      x[n] = k1 - k3 + q4;
-      x[H + n] = k1 + k2;
-      return;
-    }
-    k1 = k1 >= q2 ? k1 - q2 : k1;
-    k1 = k1 >= q ? k1 - q : k1;
-    k2 = k2 >= q2 ? k2 - q2 : k2;
-    k2 = k2 >= q ? k2 - q : k2;
-    k3 = k3 >= q2 ? k3 - q2 : k3;
-    k3 = k3 >= q ? k3 - q : k3;
-    x[n] = sub_mod(k1, k3, q);
-    x[H + n] = add_mod(k1, k2, q);
+  if (q < (1ull << kLazyPrimeBits)) {      // the prime is the same for the whole block
+    if ((q & 0xffffffffull) == 1) gi_twist_lazy<true>(x, n, H, w, a, b, q, lazy_out);
+    else gi_twist_lazy<false>(x, n, H, w, a, b, q, lazy_out);
     return;
   }
   const uint64_t k1 = shoup(a + b, w[0], w[H], q);
@@ -226,8 +237,8 @@ __global__ void gi_layout(uint64_t* dst, const uint64_t* src, int H, bool to_pla
 NttTables dgt_tables(const Engine& E) {
   NttTables T;
   T.tw = E.d_dtw; T.itw = E.d_ditw; T.pc = E.d_dpc;
-  T.log_n = E.log_n - 1; T.prime_shift = 1; T.lazy = E.lazy;
-  if (!E.lazy) T.lazy_prime = E.lazy_prime.data();
+  T.log_n = E.log_n - 1; T.prime_shift = 1; T.kind = std::max(E.ntt_kind, 0);
+  if (E.ntt_kind < 0) T.prime_kind = E.prime_kind.data();
   return T;
 }
 

@@ -282,12 +282,15 @@ int aoa_engine_create(const aoa_params* p, aoa_engine** out) {
     for (int i = 0; i < E.nprimes; i++)
       for (int j = 0; j < i; j++)
         if (E.primes[i] == E.primes[j]) throw AoaError(AOA_ERR_BAD_PARAM, "primes must be distinct");
-    E.lazy = true;
-    E.lazy_prime.clear();
+    E.prime_kind.clear();
     for (uint64_t q : E.primes) {
-      E.lazy = E.lazy && q < (1ull << kLazyPrimeBits);
-      E.lazy_prime.push_back(q < (1ull << kLazyPrimeBits) ? 1 : 0);
+      const int kind = q >= (1ull << kLazyPrimeBits) ? kButterflyCanonical
+                       : (q & 0xffffffffull) == 1 ? kButterflyLazyQ1 : kButterflyLazy;
+      E.prime_kind.push_back((char)kind);
     }
+    E.ntt_kind = E.prime_kind[0];
+    for (char kind : E.prime_kind)
+      if (kind != E.ntt_kind) E.ntt_kind = -1;
     E.gens.resize(E.nprimes);
     for (int i = 0; i < E.nprimes; i++)
       E.gens[i] = p->generators ? p->generators[i] : h_smallest_primitive_root(E.primes[i]);

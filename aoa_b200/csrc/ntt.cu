@@ -44,16 +44,17 @@ struct Sub {
 };
 
 // ---- butterflies ------------------------------------------------------------
-// Strict mode keeps every value canonical in [0, q) (any q < 2^63); lazy mode
-// (all primes < 2^60) lets values grow between reductions (Harvey's lazy
-// butterflies; bounds below).  The last stage of each transform reduces to
-// [0, q).
+// The canonical kind keeps every value in [0, q) (any q < 2^63); the lazy
+// kinds (primes < 2^60) let values grow between reductions (Harvey's lazy
+// butterflies; bounds below), kButterflyLazyQ1 with the shorter Shoup
+// remainder of primes q = 1 mod 2^32.  The last stage of each transform
+// reduces to [0, q).
 
-template <bool LAZY>
+template <int KIND>
 struct Bf;
 
 template <>
-struct Bf<false> {
+struct Bf<kButterflyCanonical> {
   static __device__ __forceinline__ void ct(uint64_t& x, uint64_t& y, ShoupW w, uint64_t q, bool) {
     uint64_t U = x, V = shoup(y, w, q);
     x = add_mod(U, V, q);
@@ -83,10 +84,11 @@ struct Bf<false> {
 // (< 2^64): a reducing stage (even stage index within its pass) maps [0, 16q)
 // to [0, 12q) (U reduced by 8q), the stage after it maps [0, 12q) to
 // [0, 16q).  Inverse values stay in [0, 4q), reduced at every stage.
-template <>
-struct Bf<true> {
-  static __device__ __forceinline__ uint64_t mulw(uint64_t y, ShoupW w, uint64_t q) {
-    return shoup_lazy_mad3(y, w.w, w.wp, 0 - q);   // [0, 4q)
+template <int KIND>
+struct Bf {
+  static __device__ __forceinline__ uint64_t mulw(uint64_t y, ShoupW w, uint64_t q) {   // [0, 4q)
+    if constexpr (KIND == kButterflyLazyQ1) return shoup_lazy_mad3_q1(y, w.w, w.wp, q);
+    else return shoup_lazy_mad3(y, w.w, w.wp, 0 - q);
   }
   // x - b if x >= b else x, for x < 2^63 + b, b < 2^63 (sign of the difference)
   static __device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t b) {
@@ -147,7 +149,7 @@ __device__ __forceinline__ ShoupW ldsw(uint32_t a) {
 // twiddle index for local half-span 2^j and local group g: K * S/2^(j+1) + g;
 // here K = 1 and the twiddles 0..S-1 of the prime sit in shared memory at tw.
 
-template <int LOG_S, bool LAZY>
+template <int LOG_S, int LAZY>
 __device__ __forceinline__ void fwd_high_s(uint64_t (&v)[Sub<LOG_S>::E], uint32_t tw, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
@@ -182,7 +184,7 @@ __device__ __forceinline__ int low_tw_perm(int e) {
   return (1 << lvl) + ((off & ((1 << sh) - 1)) << D::HI) + (off >> sh);
 }
 
-template <int LOG_S, bool LAZY, bool PERM = false>
+template <int LOG_S, int LAZY, bool PERM = false>
 __device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t tw, uint32_t hi, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
@@ -199,7 +201,7 @@ __device__ __forceinline__ void fwd_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t
 
 // ---- inverse (Gentleman-Sande) -------------------------------------------
 
-template <int LOG_S, bool LAZY, bool PERM = false>
+template <int LOG_S, int LAZY, bool PERM = false>
 __device__ __forceinline__ void inv_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t itw, uint32_t hi, uint64_t q) {
   using D = Sub<LOG_S>;
 #pragma unroll
@@ -216,7 +218,7 @@ __device__ __forceinline__ void inv_low_s(uint64_t (&u)[Sub<LOG_S>::L], uint32_t
 
 // the column pass's high digit holds the transform's final stage (half-span
 // N/2): scale by N^-1 there
-template <int LOG_S, bool LAZY>
+template <int LOG_S, int LAZY>
 __device__ __forceinline__ void inv_high_s(uint64_t (&v)[Sub<LOG_S>::E], uint32_t itw, uint64_t q, ShoupW ninv,
                                            ShoupW ninv_w1) {
   using D = Sub<LOG_S>;
@@ -256,7 +258,7 @@ __device__ __forceinline__ void load_low_tw(ShoupW (&w)[Sub<LOG_S>::G][Sub<LOG_S
   }
 }
 
-template <int LOG_S, bool LAZY>
+template <int LOG_S, int LAZY>
 __device__ __forceinline__ void fwd_low_r(uint64_t (&u)[Sub<LOG_S>::L], const ShoupW (&w)[Sub<LOG_S>::L - 1],
                                           uint64_t q) {
   using D = Sub<LOG_S>;
@@ -272,7 +274,7 @@ __device__ __forceinline__ void fwd_low_r(uint64_t (&u)[Sub<LOG_S>::L], const Sh
   }
 }
 
-template <int LOG_S, bool LAZY>
+template <int LOG_S, int LAZY>
 __device__ __forceinline__ void inv_low_r(uint64_t (&u)[Sub<LOG_S>::L], const ShoupW (&w)[Sub<LOG_S>::L - 1],
                                           uint64_t q) {
   using D = Sub<LOG_S>;
@@ -390,7 +392,7 @@ struct RowTile {
 // between two buffers, so a new limb's twiddles can be written before the
 // first barrier: the buffer's previous users finished at least one item
 // earlier.
-template <int LOG_R, int DIV, bool LAZY, bool FWD>
+template <int LOG_R, int DIV, int LAZY, bool FWD>
 __global__ void __launch_bounds__(ColTile<LOG_R, DIV>::THREADS, ColTile<LOG_R, DIV>::MIN_BLOCKS)
 ntt_cols(NttBatch b, const __grid_constant__ CUtensorMap tmap) {
   using D = Sub<LOG_R>;
@@ -623,7 +625,7 @@ ntt_cols_wo(NttBatch b) {
       uint64_t v[D::E];
 #pragma unroll
       for (int h = 0; h < D::E; h++) v[h] = lds64(sm + Tl::row((h << D::LO) + t) * 8);
-      fwd_high_s<LOG_R, true>(v, stw, q);
+      fwd_high_s<LOG_R, kButterflyLazy>(v, stw, q);
 #pragma unroll
       for (int h = 0; h < D::E; h++) sts64(sm + Tl::row((h << D::LO) + t) * 8, v[h]);
       __syncwarp();
@@ -633,7 +635,7 @@ ntt_cols_wo(NttBatch b) {
         uint64_t u[D::L];
 #pragma unroll
         for (int l = 0; l < D::L; l++) u[l] = lds64(sm + Tl::row((hi << D::LO) + l) * 8);
-        fwd_low_s<LOG_R, true, true>(u, stw, hi, q);
+        fwd_low_s<LOG_R, kButterflyLazy, true>(u, stw, hi, q);
 #pragma unroll
         for (int l = 0; l < D::L; l++) x[(long)((hi << D::LO) + l) * C] = u[l];
       }
@@ -645,7 +647,7 @@ ntt_cols_wo(NttBatch b) {
         uint64_t u[D::L];
 #pragma unroll
         for (int l = 0; l < D::L; l++) u[l] = lds64(sm + Tl::row((hi << D::LO) + l) * 8);
-        inv_low_s<LOG_R, true, true>(u, stw, hi, q);
+        inv_low_s<LOG_R, kButterflyLazy, true>(u, stw, hi, q);
 #pragma unroll
         for (int l = 0; l < D::L; l++) sts64(sm + Tl::row((hi << D::LO) + l) * 8, u[l]);
       }
@@ -653,7 +655,7 @@ ntt_cols_wo(NttBatch b) {
       uint64_t v[D::E];
 #pragma unroll
       for (int h = 0; h < D::E; h++) v[h] = lds64(sm + Tl::row((h << D::LO) + t) * 8);
-      inv_high_s<LOG_R, true>(v, stw, q, ninv, ninv_w1);
+      inv_high_s<LOG_R, kButterflyLazy>(v, stw, q, ninv, ninv_w1);
 #pragma unroll
       for (int h = 0; h < D::E; h++) x[(long)((h << D::LO) + t) * C] = v[h];
     }
@@ -676,7 +678,7 @@ __device__ __forceinline__ int swz(int hi, int lo) {
 // barrier per item (after the tile's mbarrier) also frees the previous
 // item's buffer for the next copy, and the high-digit twiddles alternate
 // between two buffers per limb, as in the column pass.
-template <int LOG_C, int DIV, bool LAZY, bool FWD>
+template <int LOG_C, int DIV, int LAZY, bool FWD>
 __global__ void __launch_bounds__(RowTile<LOG_C, DIV>::THREADS, RowTile<LOG_C, DIV>::MIN_BLOCKS)
 ntt_rows(NttBatch b, const __grid_constant__ NttEpi epi) {
   using D = Sub<LOG_C>;
@@ -867,7 +869,7 @@ static bool col_tensor_map(const NttBatch& b, int W, CUtensorMap* map) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int LOG_R, int DIV, bool LAZY>
+template <int LOG_R, int DIV, int LAZY>
 static void launch_cols(const Engine& E, const NttBatch& b0, bool fwd, cudaStream_t st) {
   using Tl = ColTile<LOG_R, DIV>;
   const int C = 1 << b0.log_c;
@@ -893,7 +895,7 @@ static void launch_cols_wo(const Engine& E, const NttBatch& b, bool fwd, cudaStr
   note_launch();
 }
 
-template <int LOG_C, int DIV, bool LAZY>
+template <int LOG_C, int DIV, int LAZY>
 static void launch_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st, const NttEpi& epi) {
   using Tl = RowTile<LOG_C, DIV>;
   const int R = 1 << b.log_r;
@@ -908,10 +910,10 @@ static void launch_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream
 
 // Tile width choice (DIV) for a launch: the engine's tuning for lazy
 // transforms; strict transforms (primes of 62 bits or more) use the widest.
-template <bool LAZY>
+template <int LAZY>
 static int tile_div(int knob) { return LAZY ? std::max(0, std::min(2, knob)) : 0; }
 
-template <bool LAZY>
+template <int LAZY>
 static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st) {
   const int div = tile_div<LAZY>(E.tune.ntt_cols_div);
   if (LAZY && E.tune.ntt_cols_kind == 1 && b.log_r >= 6 && b.log_r <= 9) {
@@ -929,10 +931,10 @@ static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t 
   switch (b.log_r) {
 #define AOA_CASE(s)                                                \
   case s:                                                          \
-    if constexpr (!LAZY) launch_cols<s, 0, false>(E, b, fwd, st);    \
-    else if (div == 0) launch_cols<s, 0, true>(E, b, fwd, st);      \
-    else if (div == 1) launch_cols<s, 1, true>(E, b, fwd, st);      \
-    else launch_cols<s, 2, true>(E, b, fwd, st);                    \
+    if constexpr (!LAZY) launch_cols<s, 0, LAZY>(E, b, fwd, st);     \
+    else if (div == 0) launch_cols<s, 0, LAZY>(E, b, fwd, st);      \
+    else if (div == 1) launch_cols<s, 1, LAZY>(E, b, fwd, st);      \
+    else launch_cols<s, 2, LAZY>(E, b, fwd, st);                    \
     break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
@@ -940,16 +942,16 @@ static void run_cols(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t 
   }
 }
 
-template <bool LAZY>
+template <int LAZY>
 static void run_rows(const Engine& E, const NttBatch& b, bool fwd, cudaStream_t st, const NttEpi& epi) {
   const int div = tile_div<LAZY>(E.tune.ntt_rows_div);
   switch (b.log_c) {
 #define AOA_CASE(s)                                                \
   case s:                                                          \
-    if constexpr (!LAZY) launch_rows<s, 0, false>(E, b, fwd, st, epi);    \
-    else if (div == 0) launch_rows<s, 0, true>(E, b, fwd, st, epi);      \
-    else if (div == 1) launch_rows<s, 1, true>(E, b, fwd, st, epi);      \
-    else launch_rows<s, 2, true>(E, b, fwd, st, epi);                    \
+    if constexpr (!LAZY) launch_rows<s, 0, LAZY>(E, b, fwd, st, epi);     \
+    else if (div == 0) launch_rows<s, 0, LAZY>(E, b, fwd, st, epi);      \
+    else if (div == 1) launch_rows<s, 1, LAZY>(E, b, fwd, st, epi);      \
+    else launch_rows<s, 2, LAZY>(E, b, fwd, st, epi);                    \
     break;
     AOA_NTT_SIZES(AOA_CASE)
 #undef AOA_CASE
@@ -962,18 +964,19 @@ static void allow_smem(K kernel, size_t bytes) {
   AOA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
+template <int S, int DIV, int KIND>
+static void allow_kind() {
+  allow_smem(ntt_cols<S, DIV, KIND, true>, ColTile<S, DIV>::SMEM);
+  allow_smem(ntt_cols<S, DIV, KIND, false>, ColTile<S, DIV>::SMEM);
+  allow_smem(ntt_rows<S, DIV, KIND, true>, RowTile<S, DIV>::SMEM);
+  allow_smem(ntt_rows<S, DIV, KIND, false>, RowTile<S, DIV>::SMEM);
+}
+
 template <int S, int DIV>
 static void allow_size() {
-  allow_smem(ntt_cols<S, DIV, true, true>, ColTile<S, DIV>::SMEM);
-  allow_smem(ntt_cols<S, DIV, true, false>, ColTile<S, DIV>::SMEM);
-  allow_smem(ntt_rows<S, DIV, true, true>, RowTile<S, DIV>::SMEM);
-  allow_smem(ntt_rows<S, DIV, true, false>, RowTile<S, DIV>::SMEM);
-  if (DIV == 0) {
-    allow_smem(ntt_cols<S, 0, false, true>, ColTile<S, 0>::SMEM);
-    allow_smem(ntt_cols<S, 0, false, false>, ColTile<S, 0>::SMEM);
-    allow_smem(ntt_rows<S, 0, false, true>, RowTile<S, 0>::SMEM);
-    allow_smem(ntt_rows<S, 0, false, false>, RowTile<S, 0>::SMEM);
-  }
+  allow_kind<S, DIV, kButterflyLazy>();
+  allow_kind<S, DIV, kButterflyLazyQ1>();
+  if (DIV == 0) allow_kind<S, 0, kButterflyCanonical>();
 }
 
 // Once per engine: opt every transform kernel in to its dynamic shared memory.
@@ -1048,21 +1051,22 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   if (npolys <= 0 || nlimbs <= 0) return;
   if (first_prime < 0 || first_prime + ((nlimbs - 1) >> T.prime_shift) >= E.nprimes)
     throw AoaError(AOA_ERR_BAD_PARAM, "ntt: prime range out of bounds");
-  if (T.lazy_prime && T.log_n >= 10) {
-    // Mixed prime sizes (the reference's prime sets put a 63-bit q0 before
-    // its 45..55-bit buckets): the limbs run in maximal runs of one kind, the
-    // lazy kernels for primes below 2^kLazyPrimeBits, the strict ones for the
+  if (T.prime_kind && T.log_n >= 10) {
+    // Primes of different butterfly kinds (the reference's prime sets put a
+    // 63-bit q0 before its 45..55-bit buckets): the limbs run in maximal runs
+    // of one kind, the lazy kernels for primes below 2^kLazyPrimeBits (with
+    // the shorter remainder where q = 1 mod 2^32), the canonical ones for the
     // rest.  Runs start at prime boundaries; each run's data, source and
     // epilogue limbs are offset by its first limb.
     const long n = 1L << T.log_n;
-    auto lazy_at = [&](int l) { return T.lazy_prime[first_prime + (l >> T.prime_shift)] != 0; };
+    auto kind_at = [&](int l) { return (int)T.prime_kind[first_prime + (l >> T.prime_shift)]; };
     for (int l0 = 0; l0 < nlimbs;) {
-      const bool lz = lazy_at(l0);
+      const int kind = kind_at(l0);
       int l1 = l0 + 1;
-      while (l1 < nlimbs && lazy_at(l1) == lz) l1++;
+      while (l1 < nlimbs && kind_at(l1) == kind) l1++;
       NttTables T2 = T;
-      T2.lazy = lz;
-      T2.lazy_prime = nullptr;
+      T2.kind = kind;
+      T2.prime_kind = nullptr;
       if (l0 == 0 && l1 == nlimbs) {
         ntt_batch_tables(E, T2, data, npolys, first_prime, nlimbs, poly_stride, forward, st, io);
         return;
@@ -1127,12 +1131,15 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
       first.src = io->src + c0 * io->src_poly_stride * n;
       first.src_poly_stride = io->src_poly_stride;
     }
-    if (T.lazy) {
-      if (forward) { run_cols<true>(E, first, true, st); run_rows<true>(E, b, true, st, epi); }
-      else { run_rows<true>(E, first, false, st, no_epi); run_cols<true>(E, b, false, st); }
-    } else {
-      if (forward) { run_cols<false>(E, first, true, st); run_rows<false>(E, b, true, st, epi); }
-      else { run_rows<false>(E, first, false, st, no_epi); run_cols<false>(E, b, false, st); }
+    switch (T.kind) {
+#define AOA_KIND(K)                                                                   \
+  case K:                                                                             \
+    if (forward) { run_cols<K>(E, first, true, st); run_rows<K>(E, b, true, st, epi); }  \
+    else { run_rows<K>(E, first, false, st, no_epi); run_cols<K>(E, b, false, st); }     \
+    break;
+      AOA_KIND(kButterflyCanonical) AOA_KIND(kButterflyLazy) AOA_KIND(kButterflyLazyQ1)
+#undef AOA_KIND
+      default: throw AoaError(AOA_ERR_BAD_PARAM, "ntt: unknown butterfly kind");
     }
   }
   AOA_CHECK_LAUNCH();
@@ -1143,8 +1150,8 @@ void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
                long poly_stride, bool forward, cudaStream_t st) {
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
-  T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
-  if (!E.lazy) T.lazy_prime = E.lazy_prime.data();
+  T.log_n = E.log_n; T.prime_shift = 0; T.kind = std::max(E.ntt_kind, 0);
+  if (E.ntt_kind < 0) T.prime_kind = E.prime_kind.data();
   ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, nullptr);
 }
 
@@ -1153,8 +1160,8 @@ void ntt_batch_io(const Engine& E, uint64_t* data, int npolys, int first_prime, 
                   bool forward, const NttIo& io, cudaStream_t st) {
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
-  T.log_n = E.log_n; T.prime_shift = 0; T.lazy = E.lazy;
-  if (!E.lazy) T.lazy_prime = E.lazy_prime.data();
+  T.log_n = E.log_n; T.prime_shift = 0; T.kind = std::max(E.ntt_kind, 0);
+  if (E.ntt_kind < 0) T.prime_kind = E.prime_kind.data();
   ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, &io);
 }
 

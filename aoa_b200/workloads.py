@@ -42,6 +42,12 @@ def hbm_bytes(op, m, kl, n):
     return 6 * m * n * 8
 
 
+
+# 60-bit primes q = 1 mod 2^32 (q = 1 mod 2N for every degree used): their
+# limb transforms take the shorter Shoup remainder
+PRIME_MODULUS = 1 << 32
+
+
 class UnevenBatch:
     """The batched uneven workload: n_ops ops over ring degrees 2^log_ns, live
     limbs uniform in [min_limbs, k], op mix mul / rot / add."""
@@ -50,7 +56,7 @@ class UnevenBatch:
                  inputs_per_n=4, scale_bits=50, autotune=False):
         rng = np.random.default_rng(seed)
         self.k, self.kl = k, kl
-        primes = params.ntt_primes(60, 2 << max(log_ns), k + kl)
+        primes = params.ntt_primes(60, PRIME_MODULUS, k + kl)
         self.engines, self.ctx, self.evk, self.rtk, self.inputs = {}, {}, {}, {}, {}
         for ln in log_ns:
             E = Engine(ln, primes[:k], primes[k:], scale_bits=scale_bits)
@@ -161,7 +167,7 @@ class Server:
                  scale_bits=50, n_slots_used=None, autotune=False):
         rng = np.random.default_rng(seed)
         self.k, self.kl, self.log_ns = k, kl, log_ns
-        primes = params.ntt_primes(60, 2 << max(log_ns), k + kl)
+        primes = params.ntt_primes(60, PRIME_MODULUS, k + kl)
         self.engines, self.pool, self.keys, self.weights = {}, {}, {}, {}
         self.hbm_budget, self.hbm_used = hbm_budget, 0
         self.stats = {}

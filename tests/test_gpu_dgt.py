@@ -11,6 +11,7 @@ from types import SimpleNamespace
 import numpy as np
 import pytest
 
+import oracle
 from oracle import DgtOracle, Oracle, dgt_prime_set, dgt_roots, fold, unfold
 from tests.ckks_inputs import make_keys, uniform_residues
 from tests.gpu_util import require_gpu
@@ -122,6 +123,41 @@ def test_engine_reports_roots_and_derives_its_own(dgt_table):
         c.dgt_inv(da, 1, 0, 3)
         res.append(da.numpy())
     assert np.array_equal(res[0], res[1])
+
+
+@pytest.mark.parametrize("log_n", [11, 16])
+def test_dgt_on_primes_one_mod_2_32(log_n):
+    """The twist (three Shoup products per Gaussian integer) and the cyclic
+    limb transforms on primes q = 1 mod 2^32, which take the shorter Shoup
+    remainder, next to another prime below 2^60 and one above it, with the
+    roots the engine derives: the forward DGT equals the oracle's on the same
+    generators and roots, and the inverse undoes it."""
+    require_gpu()
+    import aoa_b200 as aoa
+    from aoa_b200 import params
+    n = 1 << log_n
+    q1 = oracle.gen_ntt_primes(60, 1 << 32, 2)
+    other = [q for q in oracle.gen_ntt_primes(59, 2 * n, 8) if q % (1 << 32) != 1][:1]
+    big = oracle.gen_ntt_primes(62, 2 * n, 1)
+    Q, B = [q1[0], other[0], big[0]], [q1[1]]
+    primes = Q + B
+    E = aoa.Engine(log_n, Q, B)
+    ctx = aoa.Context(E)
+    out = np.zeros(2 * len(primes), dtype=np.uint64)
+    aoa.capi.check(aoa.capi.load().aoa_engine_dgt_roots(E.handle, out.ctypes.data))
+    r = [tuple(int(v) for v in out[2 * i:2 * i + 2]) for i in range(len(primes))]
+    g = [params.primitive_root(q) for q in primes]
+    D = DgtOracle(n // 2, primes, g, r)
+    rng = np.random.default_rng(log_n + 60)
+    xs = np.stack([uniform_residues(rng, primes, n) for _ in range(2)])
+    xs[1] = np.array([[q - 1] * n for q in primes], dtype=np.uint64)
+    d = ctx.upload(xs)
+    ctx.dgt_fwd(d, 2, 0, len(primes))
+    got = d.numpy()
+    for p in range(2):
+        assert np.array_equal(got[p], unfold(D.fwd(fold(xs[p])))), p
+    ctx.dgt_inv(d, 2, 0, len(primes))
+    assert np.array_equal(d.numpy(), xs)
 
 
 @pytest.mark.parametrize("log_n,prec,in_domain", [(12, 55, "coef"), (13, 52, "dgt"), (11, 45, "coef")])

@@ -1,7 +1,8 @@
 """Bit-exact parity at the benchmarked configuration, through the C ABI.
 
 The benchmark runs HMult + relinearise + rescale at N = 2^16 with 30 Q primes
-and 31 special primes of 60 bits (q = 1 mod 2^17), dnum = 1 (the reference's
+and 31 special primes of 60 bits (q = 1 mod 2^32, a subset of the primes
+q = 1 mod 2N; the tests also run the largest primes q = 1 mod 2^17), dnum = 1 (the reference's
 ckks_mul, aoa-ntt src/ckks/ckks.cpp:273-347, with the conversions of
 src/cuda/manager.cu:180-223 and 312-341).  There the tensor-core basis
 conversion runs its full shapes: ModUp 30 -> 31 (8 K-steps of the int8 GEMM),
@@ -23,17 +24,21 @@ from tests.gpu_util import require_gpu
 pytestmark = pytest.mark.gpu
 
 LOG_N, K, KL = 16, 30, 31
+# the two 60-bit prime families: the largest q = 1 mod 2^17, and the largest
+# q = 1 mod 2^32 (the benchmark's set), whose transforms take the shorter Shoup
+# remainder
+FAMILIES = (1 << 17, 1 << 32)
 
 
-def _primes(count=K + KL):
-    return oracle.gen_ntt_primes(60, 1 << 17, count)
+def _primes(count=K + KL, modulus=1 << 17):
+    return oracle.gen_ntt_primes(60, modulus, count)
 
 
-@pytest.fixture(scope="module")
-def full():
+@pytest.fixture(scope="module", params=FAMILIES, ids=["q=1 mod 2^17", "q=1 mod 2^32"])
+def full(request):
     require_gpu()
     import aoa_b200 as aoa
-    ps = _primes()
+    ps = _primes(modulus=request.param)
     Q, B = ps[:K], ps[K:]
     E = aoa.Engine(LOG_N, Q, B, scale_bits=50)
     ctx = aoa.Context(E)

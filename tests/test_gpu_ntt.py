@@ -219,6 +219,53 @@ def test_misaligned_device_pointer_is_rejected():
     assert np.array_equal(d2.numpy()[0], o.ntt_fwd(x[0]))
 
 
+@pytest.mark.parametrize("log_n", [11, 13, 16])
+@pytest.mark.parametrize("shape", [(0, 0, 0), (0, 1, 1), (1, 2, 2), (-1, 2, 0), (0, 0, 1, 1)])
+def test_primes_one_mod_2_32_take_the_short_remainder(log_n, shape):
+    """Primes q = 1 mod 2^32 below 2^60 run the lazy butterflies with the
+    shorter Shoup remainder (t q = t + (t_0 q_1) 2^32 mod 2^64).  Interleaved
+    with other lazy primes and with primes above 2^60, the limbs run in runs of
+    all three butterfly kinds; with all-(q-1) and random inputs, for every
+    column / row tile width and the warp-owned column pass, the transforms
+    equal the oracle's."""
+    require_gpu()
+    split, cdiv, rdiv = shape[:3]
+    cols_kind = shape[3] if len(shape) > 3 else 0
+    n = 1 << log_n
+    q1 = oracle.gen_ntt_primes(60, 1 << 32, 3)
+    lazy = [q for q in oracle.gen_ntt_primes(59, 2 * n, 8) if q % (1 << 32) != 1][:2]
+    big = oracle.gen_ntt_primes(62, 2 * n, 2)
+    assert all(q % (1 << 32) == 1 and q < 1 << 60 for q in q1) and len(lazy) == 2
+    ps = [q1[0], lazy[0], q1[1], big[0], q1[2], lazy[1], big[1]]
+    E, ctx, o = _engine_and_oracle(log_n, ps[:5], ps[5:])
+    E.tune("ntt_split", split)
+    E.tune("ntt_cols_div", cdiv)
+    E.tune("ntt_rows_div", rdiv)
+    E.tune("ntt_cols_kind", cols_kind)
+    rng = np.random.default_rng(log_n + 17 * (split + 2) + 3 * cdiv + rdiv)
+    x = _rand(rng, ps, n, npolys=3)
+    x[1] = np.array([[p - 1] * n for p in ps], dtype=np.uint64)
+    d = ctx.upload(x)
+    ctx.ntt_fwd(d, 3, 0, 7)
+    X = d.numpy()
+    for p in range(3):
+        assert np.array_equal(X[p], o.ntt_fwd(x[p])), p
+    ctx.ntt_inv(d, 3, 0, 7)
+    assert np.array_equal(d.numpy(), x)
+    y = _rand(rng, ps, n)
+    dy = ctx.upload(y)
+    ctx.ntt_inv(dy, 1, 0, 7)
+    assert np.array_equal(dy.numpy()[0], o.ntt_inv(y[0]))
+    # a set of such primes only (one run per pass, as in the benchmark)
+    E1, ctx1, o1 = _engine_and_oracle(log_n, q1[:2], q1[2:])
+    x1 = _rand(rng, q1, n, npolys=2)
+    d1 = ctx1.upload(x1)
+    ctx1.ntt_fwd(d1, 2, 0, 3)
+    assert np.array_equal(d1.numpy()[1], o1.ntt_fwd(x1[1]))
+    ctx1.ntt_inv(d1, 2, 0, 3)
+    assert np.array_equal(d1.numpy(), x1)
+
+
 @pytest.mark.parametrize("log_n", [11, 16])
 def test_mixed_prime_sizes_run_lazy_and_strict_limbs(log_n):
     """Primes above and below 2^60 interleaved: the limbs run in alternating
