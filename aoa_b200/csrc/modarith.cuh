@@ -147,6 +147,18 @@ AOA_HD uint64_t shoup(uint64_t a, uint64_t w, uint64_t wp, uint64_t q) {
 
 AOA_HD uint64_t shoup(uint64_t a, ShoupW w, uint64_t q) { return shoup(a, w.w, w.wp, q); }
 
+// t q mod 2^64 for q = q1 2^32 + 1 (q = 1 mod 2^32): t + (t_0 q1) 2^32, one
+// 32-bit multiply instead of a wide one and two 32-bit ones.
+AOA_HD uint64_t mul_q1(uint64_t t, uint64_t q) {
+  return t + ((uint64_t)((uint32_t)t * (uint32_t)(q >> 32)) << 32);
+}
+
+// Exact Shoup product a w mod q in [0, q) for any a < 2^64 and q = 1 mod 2^32.
+AOA_HD uint64_t shoup_q1(uint64_t a, uint64_t w, uint64_t wp, uint64_t q) {
+  const uint64_t r = a * w - mul_q1(mulhi64(a, wp), q);
+  return r >= q ? r - q : r;
+}
+
 // Montgomery REDC of x = hi*2^64 + lo with x < q*2^64: x * 2^-64 mod q.
 AOA_HD uint64_t redc(uint64_t lo, uint64_t hi, uint64_t q, uint64_t qinv_neg) {
   uint64_t m = lo * qinv_neg;
@@ -175,6 +187,17 @@ AOA_HD uint64_t barrett_wide(uint64_t lo, uint64_t hi, uint64_t q, uint64_t mu, 
   const uint32_t x1hi = funnel_r32((uint32_t)hi, (uint32_t)(hi >> 32), t);
   const uint64_t x1 = ((uint64_t)x1hi << 32) | x1lo;
   uint64_t r = lo - mulhi64(x1, mu) * q;
+  r = r >= q ? r - q : r;
+  return r >= q ? r - q : r;
+}
+
+// barrett_wide for q = 1 mod 2^32 (the quotient times q through mul_q1).
+AOA_HD uint64_t barrett_wide_q1(uint64_t lo, uint64_t hi, uint64_t q, uint64_t mu, uint32_t s) {
+  const uint32_t t = s - 32;
+  const uint32_t x1lo = funnel_r32((uint32_t)(lo >> 32), (uint32_t)hi, t);
+  const uint32_t x1hi = funnel_r32((uint32_t)hi, (uint32_t)(hi >> 32), t);
+  const uint64_t x1 = ((uint64_t)x1hi << 32) | x1lo;
+  uint64_t r = lo - mul_q1(mulhi64(x1, mu), q);
   r = r >= q ? r - q : r;
   return r >= q ? r - q : r;
 }

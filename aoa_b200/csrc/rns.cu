@@ -211,6 +211,10 @@ struct TcOut {
   uint64_t q, mu, sh, one_sh;
 };
 
+// Q1: every input and output prime of the launch is q = 1 mod 2^32 below
+// 2^60 (the engine's butterfly kind kButterflyLazyQ1): the quotient times q
+// in the reductions and Shoup products takes one 32-bit multiply (mul_q1).
+template <bool Q1>
 __device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const TcOut& c, const PrimeConst* P) {
   uint64_t W0 = v[0], W1 = v[4];
   asm("mad.wide.u32 %0, %1, 256, %0;" : "+l"(W0) : "r"(v[1]));
@@ -225,14 +229,35 @@ __device__ __forceinline__ uint64_t tc_combine(const uint32_t* v, const TcOut& c
       : "=r"(r1), "=r"(r2)
       : "r"((uint32_t)(W0 >> 32)), "r"((uint32_t)W1), "r"((uint32_t)(W1 >> 32)));
   const uint64_t lo = ((uint64_t)r1 << 32) | (uint32_t)W0;
-  if (c.sh) return barrett_wide(lo, r2, c.q, c.mu, (uint32_t)c.sh);
+  if (c.sh) return Q1 ? barrett_wide_q1(lo, r2, c.q, c.mu, (uint32_t)c.sh) : barrett_wide(lo, r2, c.q, c.mu, (uint32_t)c.sh);
   return reduce128(lo, r2, *P);
 }
 
+// exact Shoup product of the conversion kernel's epilogue
+template <bool Q1>
+__device__ __forceinline__ uint64_t tc_shoup(uint64_t a, uint64_t w, uint64_t wp, uint64_t q) {
+  return Q1 ? shoup_q1(a, w, wp, q) : shoup(a, w, wp, q);
+}
+
+// an input scaled by its CRT constant, z = [x w]_q in [0, q): for Q1 primes
+// the transforms' three-product quotient with the short remainder ([0, 4q))
+// and two conditional subtractions
+template <bool Q1>
+__device__ __forceinline__ uint64_t tc_scale(uint64_t x, ShoupW w, uint64_t q) {
+  if constexpr (Q1) {
+    uint64_t r = shoup_lazy_mad3_q1(x, w.w, w.wp, q);
+    r = r >= 2 * q ? r - 2 * q : r;
+    return r >= q ? r - q : r;
+  } else {
+    return shoup(x, w, q);
+  }
+}
+
 // x mod q_out for x < p (another prime): one subtraction when p < 2 q_out
+template <bool Q1>
 __device__ __forceinline__ uint64_t tc_cross(uint64_t x, uint64_t p, const TcOut& c) {
   if (p < 2 * c.q) return x >= c.q ? x - c.q : x;
-  return shoup(x, 1, c.one_sh, c.q);
+  return tc_shoup<Q1>(x, 1, c.one_sh, c.q);
 }
 
 // Persistent: CTA b handles tiles b, b + grid, ...  Per tile: the inputs (loaded
@@ -242,7 +267,7 @@ __device__ __forceinline__ uint64_t tc_cross(uint64_t x, uint64_t p, const TcOut
 // (tile rows) and every fourth output starting at w / 4.
 constexpr int kTcPairs = 32 / 2 / (kTcThreads / kTcRows);   // input pairs per thread (nin <= 32)
 
-template <int MODE>
+template <int MODE, bool Q1>
 __global__ void __launch_bounds__(kTcThreads, 1)
 basis_convert_tc(ConvArgs a, int j_first, int j_end) {
   extern __shared__ __align__(1024) uint8_t tcs[];
@@ -324,8 +349,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       const int p = ap + m * (kTcThreads / kTcRows);
       if (p < npairs) {
         const int i0 = 2 * p, i1 = 2 * p + 1;
-        const uint64_t z0 = shoup(xa[m], s_zc[i0], s_qin[i0]);
-        const uint64_t z1 = i1 < a.nin ? shoup(xb[m], s_zc[i1], s_qin[i1]) : 0;
+        const uint64_t z0 = tc_scale<Q1>(xa[m], s_zc[i0], s_qin[i0]);
+        const uint64_t z1 = i1 < a.nin ? tc_scale<Q1>(xb[m], s_zc[i1], s_qin[i1]) : 0;
         *(uint4*)(As + (size_t)p * (kTcRows * 16) + ar * 16) =
             make_uint4((uint32_t)z0, (uint32_t)(z0 >> 32), (uint32_t)z1, (uint32_t)(z1 >> 32));
       }
@@ -363,7 +388,7 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
       const TcOut cpl = s_out[l];
       const PrimeConst* Pl = a.pc + a.out_prime0 + l;
       // the rescale modes read the table with B^-1 folded in: sums are conv * B^-1
-      const uint64_t sl = (l & 1) ? tc_combine(v + 8, cpl, Pl) : tc_combine(v, cpl, Pl);
+      const uint64_t sl = (l & 1) ? tc_combine<Q1>(v + 8, cpl, Pl) : tc_combine<Q1>(v, cpl, Pl);
       const uint64_t cl = sub_mod(dv, sl, cpl.q);
       const int per = (((l + 3) / 4) + 1) & ~1;
       const int jb = par * per, je = min(l, jb + per);
@@ -374,7 +399,8 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
           if (j + u < je) {
             const TcOut cp = s_out[j + u];
             out[(long)(j + u - a.out_shift) * N] =
-                add_mod(tc_combine(v + 8 * u, cp, a.pc + a.out_prime0 + j + u), tc_cross(cl, cpl.q, cp), cp.q);
+                add_mod(tc_combine<Q1>(v + 8 * u, cp, a.pc + a.out_prime0 + j + u), tc_cross<Q1>(cl, cpl.q, cp),
+                        cp.q);
           }
         }
       }
@@ -389,14 +415,14 @@ basis_convert_tc(ConvArgs a, int j_first, int j_end) {
           const int o = jj + u;
           if (o >= jb && o < je) {
             const TcOut cp = s_out[o];
-            uint64_t r = tc_combine(v + 8 * u, cp, a.pc + a.out_prime0 + o);
+            uint64_t r = tc_combine<Q1>(v + 8 * u, cp, a.pc + a.out_prime0 + o);
             if (MODE == kModDown) {
               const uint64_t x = a.x[poly * a.x_poly_stride + (long)(o - a.x_shift) * N + c];
-              r = shoup(sub_mod(x, r, cp.q), a.binv[o], cp.q);
+              r = tc_shoup<Q1>(sub_mod(x, r, cp.q), a.binv[o].w, a.binv[o].wp, cp.q);
             } else if (MODE == kRescaleTop) {
               r = sub_mod(dv, r, cp.q);                            // folded table: r = conv * B^-1
             } else if (MODE == kRescaleY) {
-              r = add_mod(r, shoup(dv, 1, cp.one_sh, cp.q), cp.q); // folded table: r = conv * B^-1
+              r = add_mod(r, tc_shoup<Q1>(dv, 1, cp.one_sh, cp.q), cp.q); // folded table: r = conv * B^-1
             }
             out[(long)(o - a.out_shift) * N] = r;
           }
@@ -430,13 +456,20 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
     t.npolys = npolys;
     const long tiles = (N / kTcRows) * npolys;
     const unsigned grid_tc = (unsigned)std::min<long>(tiles, E.num_sms);
+    bool q1 = true;                               // every input and output prime q = 1 mod 2^32 below 2^60
+    for (int i = 0; i < a.nin; i++) q1 = q1 && E.prime_kind[a.in_prime0 + i] == kButterflyLazyQ1;
+    for (int j = 0; j < j_end; j++) q1 = q1 && E.prime_kind[a.out_prime0 + j] == kButterflyLazyQ1;
+#define AOA_TC(M)                                                                                   \
+  if (q1) basis_convert_tc<M, true><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end);     \
+  else basis_convert_tc<M, false><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end);
     switch (a.mode) {
-      case kRaw: basis_convert_tc<kRaw><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
-      case kModDown: basis_convert_tc<kModDown><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
-      case kRescaleTop: basis_convert_tc<kRescaleTop><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
-      case kRescaleY: basis_convert_tc<kRescaleY><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
-      default: basis_convert_tc<kRescaleFused><<<grid_tc, kTcThreads, kTcSmem, st>>>(t, j_begin, j_end); break;
+      case kRaw: AOA_TC(kRaw) break;
+      case kModDown: AOA_TC(kModDown) break;
+      case kRescaleTop: AOA_TC(kRescaleTop) break;
+      case kRescaleY: AOA_TC(kRescaleY) break;
+      default: AOA_TC(kRescaleFused) break;
     }
+#undef AOA_TC
     note_launch();
     AOA_CHECK_LAUNCH();
     return;
@@ -452,14 +485,11 @@ static void run_convert(const Engine& E, const ConvArgs& a, int npolys, int j_be
 // conversion kernel needs, and check the 128-bit accumulation bound.
 void rns_init(Engine& E) {
   AOA_CUDA(cudaFuncSetAttribute(basis_convert, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRaw>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kModDown>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRescaleTop>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kTcSmem));
-  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRescaleY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kTcSmem));
-  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<kRescaleFused>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kTcSmem));
+#define AOA_TC_SMEM(M)                                                                                       \
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem)); \
+  AOA_CUDA(cudaFuncSetAttribute(basis_convert_tc<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  AOA_TC_SMEM(kRaw) AOA_TC_SMEM(kModDown) AOA_TC_SMEM(kRescaleTop) AOA_TC_SMEM(kRescaleY) AOA_TC_SMEM(kRescaleFused)
+#undef AOA_TC_SMEM
   auto bits = [](uint64_t x) { int b = 0; while (x) { b++; x >>= 1; } return b; };
   uint64_t mq = 0, mb = 0;
   for (int i = 0; i < E.k; i++) mq = std::max(mq, E.primes[i]);

@@ -175,14 +175,15 @@ def test_rotate_full_size_bit_exact(full, r):
     assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
 
 
+@pytest.mark.parametrize("modulus", FAMILIES, ids=["q=1 mod 2^17", "q=1 mod 2^32"])
 @pytest.mark.parametrize("kind", ["all_q_minus_1", "max_z"])
-def test_conversion_32_inputs(kind):
+def test_conversion_32_inputs(kind, modulus):
     """The tensor-core conversion at its own maximum of 32 inputs and 32
     outputs (32 Q + 32 special primes at N = 2^12): ModUp at level 31 and
     ModDown, against the oracle and against the CUDA-core kernel."""
     require_gpu()
     import aoa_b200 as aoa
-    ps = _primes(64)
+    ps = _primes(64, modulus)
     Q, B = ps[:32], ps[32:]
     E = aoa.Engine(12, Q, B)
     ctx = aoa.Context(E)
@@ -204,15 +205,16 @@ def test_conversion_32_inputs(kind):
         assert np.array_equal(down.numpy(), want_down), tc
 
 
+@pytest.mark.parametrize("modulus", FAMILIES, ids=["q=1 mod 2^17", "q=1 mod 2^32"])
 @pytest.mark.parametrize("level", [29, 17, 8, 2])
-def test_conversion_kernels_agree_at_benchmark_shapes(level):
+def test_conversion_kernels_agree_at_benchmark_shapes(level, modulus):
     """30 Q + 31 special 60-bit primes at N = 2^12 (the benchmark's conversion
     shapes on a small ring): ModUp, ModDown and HMult with its merged ModDown +
     rescale, tensor-core kernel vs CUDA-core kernel vs oracle, with all-(q-1)
     inputs (ciphertexts and conversion inputs) and max-z conversion inputs."""
     require_gpu()
     import aoa_b200 as aoa
-    ps = _primes()
+    ps = _primes(modulus=modulus)
     Q, B = ps[:K], ps[K:]
     E = aoa.Engine(12, Q, B)
     ctx = aoa.Context(E)
