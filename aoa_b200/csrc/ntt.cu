@@ -879,8 +879,12 @@ static void launch_cols(const Engine& E, const NttBatch& b0, bool fwd, cudaStrea
   // a tensor-map tile load needs the rows of the tile in order (no row swizzle: W = 16)
   b.use_tma = E.tune.ntt_cols_tma && Tl::W == 16 && col_tensor_map(b, Tl::W, &map) ? 1 : 0;
   dim3 grid(C / Tl::W, ctas_per_tile(E, C / Tl::W, b.nitems, Tl::MIN_BLOCKS));
+  // the inverse column pass keeps the general remainder on primes
+  // q = 1 mod 2^32: with the short one it measured 3% slower (more carries on
+  // the multiply pipe in its Gentleman-Sande butterflies)
+  constexpr int INV = LAZY == kButterflyLazyQ1 ? kButterflyLazy : LAZY;
   if (fwd) ntt_cols<LOG_R, DIV, LAZY, true><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, map);
-  else ntt_cols<LOG_R, DIV, LAZY, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, map);
+  else ntt_cols<LOG_R, DIV, INV, false><<<grid, Tl::THREADS, Tl::SMEM, st>>>(b, map);
   note_launch();
 }
 
@@ -967,7 +971,7 @@ static void allow_smem(K kernel, size_t bytes) {
 template <int S, int DIV, int KIND>
 static void allow_kind() {
   allow_smem(ntt_cols<S, DIV, KIND, true>, ColTile<S, DIV>::SMEM);
-  allow_smem(ntt_cols<S, DIV, KIND, false>, ColTile<S, DIV>::SMEM);
+  if constexpr (KIND != kButterflyLazyQ1) allow_smem(ntt_cols<S, DIV, KIND, false>, ColTile<S, DIV>::SMEM);
   allow_smem(ntt_rows<S, DIV, KIND, true>, RowTile<S, DIV>::SMEM);
   allow_smem(ntt_rows<S, DIV, KIND, false>, RowTile<S, DIV>::SMEM);
 }
