@@ -419,7 +419,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="aoa", choices=["aoa", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-systems", action="store_true", help="skip the uneven-batch and serving measurements")
@@ -857,7 +857,7 @@ def main():
                     "hmult_per_call_ops_per_s": world * B / (dgt_hmult_ms / 1000.0),
                     "hmult_batched_ops_per_s": world * B / (dgt_batch_ms / 1000.0),
                     "path": "aoa-dgt ckks_mul on a DGT context (GI tensor and key products), inputs in the DGT domain; "
-                            "batched: ckks_mul_batch of the same 16 pairs on the DGT context"},
+                            "batched: ckks_mul_batch of the same %d pairs on the DGT context" % B},
             "encoder": {"slots": N // 2, "limbs": K, "encode_ms_host_to_device": enc_ms,
                         "decode_ms_device_to_host": dec_ms},
             "uneven_batch": uneven,
