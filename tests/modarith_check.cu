@@ -2,7 +2,9 @@
 // compiled by nvcc as host code: Barrett products for every modulus bit length
 // 34..62 (extreme and random operands below 2^n), the fused two-product
 // reduction for 34..61 bits, the Montgomery products used outside that range
-// (3..33 and 63 bits), against exact 128-bit arithmetic.  Prints "ok <count>".
+// (3..33 and 63 bits), and for moduli q = 1 mod 2^32 (34..60 bits) the Barrett
+// reduction and exact Shoup product whose quotient times q takes one 32-bit
+// multiply, against exact 128-bit arithmetic.  Prints "ok <count>".
 #include <cstdio>
 #include <random>
 
@@ -55,6 +57,27 @@ int main() {
         a %= q;                                                             // the entry point: a, b < q
         b %= q;
         check(mul_mod(a, b, P), (uint64_t)(((unsigned __int128)a * b) % q));
+      }
+    }
+  }
+  for (int n = 34; n <= 60; n++) {                                      // q = q1 2^32 + 1
+    for (int t = 0; t < 100; t++) {
+      const uint64_t hi = t == 0 ? (1ull << (n - 33)) : t == 1 ? (1ull << (n - 32)) - 1
+                                                       : (1ull << (n - 33)) | (rng() & ((1ull << (n - 33)) - 1));
+      const uint64_t q = (hi << 32) | 1;
+      const PrimeConst P = constants(q);
+      const uint64_t lim = (1ull << n) - 1;
+      for (int r = 0; r < 100; r++) {
+        const uint64_t a = r == 0 ? lim : rng() & lim, b = r == 0 ? lim : rng() & lim;
+        const uint64_t t64 = rng();
+        check(mul_q1(t64, q), t64 * q);
+        const unsigned __int128 ab = (unsigned __int128)a * b;
+        check(barrett_wide_q1((uint64_t)ab, (uint64_t)(ab >> 64), q, P.bar_mu, (uint32_t)P.bar_sh),
+              (uint64_t)(ab % q));
+        const uint64_t w = r == 1 ? q - 1 : rng() % q;
+        const uint64_t wp = (uint64_t)(((unsigned __int128)w << 64) / q);
+        const uint64_t x = r == 2 ? ~0ull : rng();                        // any 64-bit operand
+        check(shoup_q1(x, w, wp, q), (uint64_t)(((unsigned __int128)x * w) % q));
       }
     }
   }
