@@ -694,8 +694,8 @@ def main():
         uneven, serving = systems_workloads(aoa, torch)
 
     # ---- end to end through the C ABI with host buffers -----------------------------
-    # Every step uploads its 16 input pairs from pinned host memory, runs the
-    # batched HMult + relinearise + rescale and queues the 16 results' copy
+    # Every step uploads its B input pairs from pinned host memory, runs the
+    # batched HMult + relinearise + rescale and queues the B results' copy
     # back (coefficient domain); steps alternate between two contexts
     # (streams), so one step's copies overlap the other's arithmetic, as a
     # serving loop would (three contexts measured slower: 668 vs ~700/s, the
