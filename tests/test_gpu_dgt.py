@@ -160,6 +160,44 @@ def test_dgt_on_primes_one_mod_2_32(log_n):
     assert np.array_equal(d.numpy(), xs)
 
 
+def test_dgt_hmult_on_primes_one_mod_2_32():
+    """ckks_mul and ckks_mul_batch on a DGT context over primes q = 1 mod 2^32
+    (the benchmark's kind: short Shoup remainders in the twist, the limb
+    transforms and the basis conversion), roots derived by the engine: the
+    oracle's HMult residues in coefficients."""
+    require_gpu()
+    import aoa_b200 as aoa
+    log_n, k, kl = 12, 4, 4
+    ps = oracle.gen_ntt_primes(60, 1 << 32, k + kl)
+    Q, B = ps[:k], ps[k:]
+    E = aoa.Engine(log_n, Q, B)
+    ctx = aoa.Context(E)
+    ctx.set_transform(aoa.AOA_DGT)
+    o = Oracle(1 << log_n, Q, B)
+    keys = make_keys(o, seed=33)
+    evk = aoa.SwitchKey(ctx, o.ntt_inv(keys["evk"][0]), o.ntt_inv(keys["evk"][1]), domain=aoa.AOA_COEF)
+    rng = np.random.default_rng(77)
+    N = 1 << log_n
+    pairs = [tuple(uniform_residues(rng, Q, N) for _ in range(4)) for _ in range(3)]
+    sa, sb = 1 << 40, (1 << 40) + 77
+    level = k - 1
+    w = [o.hmult((a0, a1), (b0, b1), keys["evk"], level, sa, sb) for a0, a1, b0, b1 in pairs]
+    cts = [(aoa.Ciphertext.from_residues(ctx, a0, a1, slots=N // 2, scale=sa),
+            aoa.Ciphertext.from_residues(ctx, b0, b1, slots=N // 2, scale=sb)) for a0, a1, b0, b1 in pairs]
+    out = aoa.Ciphertext(ctx)
+    aoa.ckks_mul(ctx, out, cts[0][0], cts[0][1], evk)
+    g0, g1 = out.download(nlimbs=level, domain=aoa.AOA_COEF)
+    assert out.scale == w[0][2]
+    assert np.array_equal(g0, w[0][0][:level]) and np.array_equal(g1, w[0][1][:level])
+    cts = [(aoa.Ciphertext.from_residues(ctx, a0, a1, slots=N // 2, scale=sa),
+            aoa.Ciphertext.from_residues(ctx, b0, b1, slots=N // 2, scale=sb)) for a0, a1, b0, b1 in pairs]
+    outs = [aoa.Ciphertext(ctx) for _ in pairs]
+    aoa.ckks_mul_batch(ctx, outs, [c[0] for c in cts], [c[1] for c in cts], evk)
+    for ob, (w0, w1, _) in zip(outs, w):
+        g0, g1 = ob.download(nlimbs=level, domain=aoa.AOA_COEF)
+        assert np.array_equal(g0, w0[:level]) and np.array_equal(g1, w1[:level])
+
+
 @pytest.mark.parametrize("log_n,prec,in_domain", [(12, 55, "coef"), (13, 52, "dgt"), (11, 45, "coef")])
 def test_dgt_hmult_matches_oracle(dgt_table, log_n, prec, in_domain):
     """ckks_mul of the DGT library (aoa-dgt src/ckks.cpp:275-358): the same
