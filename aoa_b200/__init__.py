@@ -45,7 +45,7 @@ class Engine:
         self.handle = h
 
     def tune(self, knob, value):
-        """Set a launch-shape knob ("ntt_split", "ntt_cols_div", "ntt_cols_kind",
+        """Set a launch-shape knob ("ntt_split", "dgt_split", "ntt_cols_div", "ntt_cols_kind",
         "ntt_rows_div", "ntt_waves", "ntt_waves_large", "ntt_chunk_bytes",
         "ntt_cols_tma", "conv_tensor_cores", "fuse", "batch_streams", "spin_limit")."""
         capi.check(capi.load().aoa_engine_tune(self.handle, knob.encode(), float(value)))

@@ -53,6 +53,10 @@ struct Tune {
   double ntt_waves_large = 8.0;       // the same for launches of at least kLargeItems limbs
   bool conv_tensor_cores = true;      // basis conversion on the int8 tensor cores where it applies
   int ntt_split = 0;                  // log2(C) - floor(log2(N) / 2) of the R x C transform split
+  // the same for the DGT's cyclic limb transforms (N/2 points): at N = 2^16
+  // the 2^15-point transforms ran 2-3% faster with 256-point rows than with
+  // the 128-point rows of split 0
+  int dgt_split = 1;
   int ntt_cols_div = 0;               // column-pass tile width: widest >> div (0..2)
   int ntt_cols_kind = 0;              // column pass: 0 CTA-wide exchange, 1 warp-owned columns
   int ntt_rows_div = 1;               // row-pass tile height: tallest >> div (0..2)
@@ -209,6 +213,7 @@ struct NttTables {
   int log_n = 0;
   int prime_shift = 0;     // limb l uses prime first + (l >> prime_shift)
   int kind = kButterflyCanonical;   // butterfly kind of every limb
+  int split = 0;                     // log2(C) - floor(log2(n) / 2) of the R x C split
   // per prime butterfly kind, when the primes' kinds differ: the limbs run in
   // runs of one kind
   const char* prime_kind = nullptr;

@@ -238,6 +238,7 @@ NttTables dgt_tables(const Engine& E) {
   NttTables T;
   T.tw = E.d_dtw; T.itw = E.d_ditw; T.pc = E.d_dpc;
   T.log_n = E.log_n - 1; T.prime_shift = 1; T.kind = std::max(E.ntt_kind, 0);
+  T.split = E.tune.dgt_split;
   if (E.ntt_kind < 0) T.prime_kind = E.prime_kind.data();
   return T;
 }

@@ -332,6 +332,7 @@ int aoa_engine_tune(aoa_engine* h, const char* knob, double value) {
   else if (k == "ntt_waves_large" && value > 0 && value <= 64) h->e.tune.ntt_waves_large = value;
   else if (k == "conv_tensor_cores" && (value == 0 || value == 1)) h->e.tune.conv_tensor_cores = value != 0;
   else if (k == "ntt_split" && value >= -2 && value <= 2 && value == (int)value) h->e.tune.ntt_split = (int)value;
+  else if (k == "dgt_split" && value >= -2 && value <= 2 && value == (int)value) h->e.tune.dgt_split = (int)value;
   else if (k == "ntt_cols_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_cols_div = (int)value;
   else if (k == "ntt_rows_div" && value >= 0 && value <= 2 && value == (int)value) h->e.tune.ntt_rows_div = (int)value;
   else if (k == "ntt_cols_kind" && (value == 0 || value == 1)) h->e.tune.ntt_cols_kind = (int)value;
@@ -353,6 +354,7 @@ int aoa_engine_tune_get(const aoa_engine* h, const char* knob, double* value) {
   else if (k == "ntt_waves_large") *value = t.ntt_waves_large;
   else if (k == "conv_tensor_cores") *value = t.conv_tensor_cores ? 1 : 0;
   else if (k == "ntt_split") *value = t.ntt_split;
+  else if (k == "dgt_split") *value = t.dgt_split;
   else if (k == "ntt_cols_div") *value = t.ntt_cols_div;
   else if (k == "ntt_rows_div") *value = t.ntt_rows_div;
   else if (k == "ntt_cols_kind") *value = t.ntt_cols_kind;

@@ -1096,7 +1096,7 @@ void ntt_batch_tables(const Engine& E, const NttTables& T, uint64_t* data, int n
   b.tw = T.tw; b.itw = T.itw; b.pc = T.pc; b.err = E.d_err;
   b.spin = E.tune.spin_limit;
   b.log_n = T.log_n;
-  b.log_c = T.log_n / 2 + E.tune.ntt_split;
+  b.log_c = T.log_n / 2 + T.split;
   b.log_c = std::max(std::max(5, T.log_n - 10), std::min(std::min(10, T.log_n - 5), b.log_c));
   b.log_r = T.log_n - b.log_c;
   b.first_prime = first_prime; b.prime_shift = T.prime_shift; b.poly_stride = poly_stride;
@@ -1155,6 +1155,7 @@ void ntt_batch(const Engine& E, uint64_t* data, int npolys, int first_prime, int
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
   T.log_n = E.log_n; T.prime_shift = 0; T.kind = std::max(E.ntt_kind, 0);
+  T.split = E.tune.ntt_split;
   if (E.ntt_kind < 0) T.prime_kind = E.prime_kind.data();
   ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, nullptr);
 }
@@ -1165,6 +1166,7 @@ void ntt_batch_io(const Engine& E, uint64_t* data, int npolys, int first_prime, 
   NttTables T;
   T.tw = E.d_tw; T.itw = E.d_itw; T.pc = E.d_pc;
   T.log_n = E.log_n; T.prime_shift = 0; T.kind = std::max(E.ntt_kind, 0);
+  T.split = E.tune.ntt_split;
   if (E.ntt_kind < 0) T.prime_kind = E.prime_kind.data();
   ntt_batch_tables(E, T, data, npolys, first_prime, nlimbs, poly_stride, forward, st, &io);
 }

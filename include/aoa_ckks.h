@@ -96,7 +96,8 @@ int aoa_engine_destroy(aoa_engine* e);
  * "ntt_waves" (transform CTAs per pass in resident waves, default 1),
  * "ntt_waves_large" (the same for launches of at least 1536 limbs, default 8),
  * "ntt_split" (log2 C - floor(log2 N / 2) of the R x C transform split,
- * -2..2, default 0), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width
+ * -2..2, default 0), "dgt_split" (the same for the DGT's N/2-point cyclic
+ * limb transforms, default 1), "ntt_cols_div" / "ntt_rows_div" (column-pass tile width
  * and row-pass tile height = widest >> div, 0..2, defaults 0 / 1),
  * "ntt_cols_kind" (0 CTA-wide exchange, 1 warp-owned columns; default 0),
  * "ntt_cols_tma" (1: the column pass loads 16-column tiles with one

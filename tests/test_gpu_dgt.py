@@ -62,6 +62,26 @@ def test_dgt_bit_exact(dgt_table, log_n, prec):
         assert np.array_equal(got[p, 0], xs[p, 0]) and np.array_equal(got[p, 4], xs[p, 4])
 
 
+@pytest.mark.parametrize("log_n", [12, 16])
+def test_dgt_split_knob_keeps_results(dgt_table, log_n):
+    """The DGT's cyclic limb transforms take their own R x C split (knob
+    dgt_split, default 1); every split gives the oracle's DGT."""
+    require_gpu()
+    aoa, E, ctx, D, _ = _setup(dgt_table, log_n, 3, 2, 55)
+    assert E.tune_get("dgt_split") == 1
+    rng = np.random.default_rng(log_n + 3)
+    x = uniform_residues(rng, E.primes, E.N)
+    want = unfold(D.fwd(fold(x)))
+    for split in (-1, 0, 1, 2):
+        E.tune("dgt_split", split)
+        d = ctx.upload(x)
+        ctx.dgt_fwd(d, 1, 0, E.k + E.kl)
+        assert np.array_equal(d.numpy(), want), split
+        ctx.dgt_inv(d, 1, 0, E.k + E.kl)
+        assert np.array_equal(d.numpy(), x), split
+    E.tune("dgt_split", 1)
+
+
 def test_gi_layout_and_mul(dgt_table):
     require_gpu()
     aoa, E, ctx, D, _ = _setup(dgt_table, 12, 2, 2, 55)
