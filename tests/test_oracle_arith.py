@@ -62,3 +62,18 @@ def test_prime_search_rule():
     for hi, lo in zip(ps[:5], ps[1:6]):
         for c in range(lo + (1 << 17), hi, 1 << 17):
             assert not L.oc_is_prime(c)
+
+
+def test_prime_search_rule_one_mod_2_32():
+    """The benchmark's prime set: the 61 largest 60-bit primes q = 1 mod 2^32,
+    the same from the library's search and the oracle's, none skipped."""
+    from aoa_b200 import params
+    ps = oracle.gen_ntt_primes(60, 1 << 32, 61)
+    assert ps == params.ntt_primes(60, 1 << 32, 61)
+    assert len(ps) == 61 and ps == sorted(ps, reverse=True)
+    L = oracle.lib()
+    for q in ps:
+        assert q.bit_length() == 60 and q % (1 << 32) == 1 and L.oc_is_prime(q)
+    for hi, lo in zip(ps[:5], ps[1:6]):
+        for c in range(lo + (1 << 32), hi, 1 << 32):
+            assert not L.oc_is_prime(c)
